@@ -1,0 +1,143 @@
+/*
+ * lionbolt_b200.h -- C ABI of the B200 (sm_100a) transport-solve library.
+ *
+ * Drop-in boundary for Lionbolt's within-group transport solve.  The reference exposes this path
+ * as Fortran type-bound procedures re-exported by src/LionboltAPI.f90:1-12; every entry point
+ * below names the reference procedure it replaces.  A Fortran iso_c_binding interface for these
+ * functions is given in INTEGRATION.md.
+ *
+ * Conventions
+ *   - Plain pointers and sizes only; all host arrays are C-contiguous, 0-based.
+ *   - Angular vectors use the reference layout of SpaceAngleVector%v
+ *     (src/operators/LinearOperatorClass.f90:30-41): v[i * NENK + 4 * e + k] for direction i,
+ *     element e, local node k, NENK = 4 * NE (linear tetrahedra).
+ *   - Moment vectors: m[j * NENK + 4 * e + k], j = l*l + l + m the real spherical-harmonic index.
+ *   - Every call returns an LB_* status.  The reference terminates through stophere(msg) on the
+ *     same conditions; lb_last_error() returns the message.
+ *   - One handle = one CUDA device + one stream.  A handle is not safe for concurrent use from
+ *     several host threads (the reference GMRES driver is not re-entrant either,
+ *     src/solvers/SPARSKIT.f90:32, third_party/SPARSKIT/iters.f:1942).
+ */
+#ifndef LIONBOLT_B200_H
+#define LIONBOLT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct lb_handle lb_handle;
+
+enum lb_status {
+    LB_OK = 0,
+    LB_ERR_ARG = 1,      /* invalid argument / size                                           */
+    LB_ERR_CUDA = 2,     /* CUDA runtime error                                                */
+    LB_ERR_OOM = 3,      /* device allocation failed                                          */
+    LB_ERR_CYCLE = 4,    /* sweep ordering stagnated: cyclic dependency (SweepOrder.f90:178)  */
+    LB_ERR_TIMEOUT = 5,  /* a bounded device-side dependency wait gave up                     */
+    LB_ERR_NOCONV = 6,   /* Krylov iteration limit reached (SPARSKIT.f90:241-244, ipar(1)=-1) */
+    LB_ERR_NAN = 7,      /* residual norm is NaN (SPARSKIT.f90:205-207)                       */
+    LB_ERR_STATE = 8,    /* operator not ready (TransportOperator.f90:87-88)                  */
+    LB_ERR_BREAKDOWN = 9 /* Krylov breakdown (SPARSKIT.f90:248-251, ipar(1)=-3)               */
+};
+
+enum lb_solver {
+    LB_SOLVER_SI = 0,          /* source iteration, src/solvers/SourceIteration.f90           */
+    LB_SOLVER_GMRES = 1,       /* restarted GMRES(m), third_party/SPARSKIT/iters.f:1901        */
+    LB_SOLVER_FGMRES_ML = 2    /* FGMRES(m) with the learned right preconditioner             */
+};
+
+/* phase timers reported by lb_get_timers (milliseconds of device time, CUDA events) */
+enum lb_timer { LB_T_SWEEP = 0, LB_T_M2D = 1, LB_T_D2M = 2, LB_T_KRYLOV = 3, LB_T_COPY = 4, LB_T_PRECOND = 5, LB_NTIMERS = 6 };
+
+int lb_version(void);
+const char* lb_status_string(int status);
+
+/* Create / destroy a handle on CUDA device `device`.  Replaces the construction and %Destroy of
+ * TransportOp / ScatteringOp / BoltzmannOp (TransportOperator.f90:431-445,
+ * ScatteringOperator.f90:279-289, BoltzmannOperator.f90:328-338). */
+int lb_create(int device, lb_handle** out);
+int lb_destroy(lb_handle* h);
+/* Copies the last error message (NUL-terminated, truncated to len) into buf. */
+int lb_last_error(const lb_handle* h, char* buf, int len);
+
+/* Mesh: replaces MeshClass + mesh%PostProcess (src/geometry/PostProcess.f90:3-461) and the space
+ * part of the operators, TransportOp%Space (TransportOperator.f90:172-255) and ScatteringOp%Space
+ * (ScatteringOperator.f90:100-152).  Linear tetrahedra with gmsh local node order.
+ *   rg[NN][3]          node coordinates
+ *   node[NE][4]        0-based node ids, gmsh tetrahedron order, positively oriented
+ *   neighbors[NE][4]   element across local face f (gmsh faces {0,1,2},{0,1,3},{0,2,3},{1,2,3}),
+ *                      -1 on the boundary (gmshprocessing.py:32-42,258-288)
+ *   mat[NE]            0-based material index < Nm (Nm <= 256)
+ * Outward normals follow PostProcess.f90:45-102 bit for bit (sorted face nodes, centroid sign). */
+int lb_set_mesh(lb_handle* h, int NE, int NN, const double* rg, const int* node, const int* neighbors,
+                const int* mat, int Nm);
+
+/* Angular quadrature: replaces AngularClass (src/angular/SNPrep.f90:39-86) as consumed by
+ * TransportOp%SpaceAngle (TransportOperator.f90:257-388) -> BuildSpaceAngle (SweepOrder.f90,
+ * SweepArrays.f90).  k[NI][3] unit directions, w[NI] weights (sum 4 pi).  Builds the per-direction
+ * wavefront schedule on the host; returns LB_ERR_CYCLE when a level adds no element. */
+int lb_set_quadrature(lb_handle* h, int NI, const double* k, const double* w);
+
+/* Fills the GL x Chebyshev product quadrature of SNPrep.f90:39-76 (Ng polar, Nc azimuthal;
+ * the reference uses Nc = 2 Ng).  k[Ng*Nc][3], w[Ng*Nc]. */
+int lb_sn_quadrature(int Ng, int Nc, double* k, double* w);
+
+/* Within-group cross sections: replaces TransportOp%Physics (TransportOperator.f90:390-429) and
+ * ScatteringOp%Physics (ScatteringOperator.f90:215-277).  sigt[Nm] = XS%t, sigs[Nm][Ls+1] =
+ * XS%s(0:Ls, m) (Legendre moments of the within-group scattering cross section). */
+int lb_set_xs(lb_handle* h, int Ls, const double* sigt, const double* sigs);
+
+/* Sweep schedule for bit-exact checks against SweepOrder.f90:105-207 / SweepArrays.f90:34-92.
+ *   sl[NI][NE]        element visited at sweep position es of direction i (sl(es,i), 0-based)
+ *   upmask[NI][NE]    bit f set when local face f of sl[i][es] is upstream (IsUpstream)
+ *   nlevels[NI]       number of wavefront levels per direction
+ *   level_start[NI][NE+1]  start position of each level (entries past nlevels[i] undefined)
+ * Any pointer may be NULL. */
+int lb_get_schedule(lb_handle* h, int* sl, unsigned char* upmask, int* nlevels, int* level_start);
+
+/* T^{-1} in place: replaces TransportOp%MatInv ('SWEEP', TransportOperator.f90:72-151), i.e.
+ * EncodeSweep + Sweep (TransportAlgebra.f90:29-246) + decode.  s[NI*NENK] enters as source,
+ * leaves as solution (FP64 host buffer; the sweep runs in FP32 on the device). */
+int lb_transport_inv(lb_handle* h, double* s);
+
+/* K x in place: replaces ScatteringOp%MatVec (ScatteringOperator.f90:39-70 ->
+ * ScatteringAlgebra.f90:13-55).  Evaluated as moment-to-discrete (discrete-to-moment (x)). */
+int lb_scatter_apply(lb_handle* h, double* x);
+
+/* x <- x - T^{-1} K x: replaces BoltzmannOp%MatVec with Tprecond (BoltzmannOperator.f90:59-104). */
+int lb_boltzmann_matvec(lb_handle* h, double* x);
+
+/* L^{-1} s in place: replaces BoltzmannOp%MatInv (BoltzmannOperator.f90:106-151).  The Krylov
+ * iteration runs in flux-moment space (n = nm*NENK) with the SPARSKIT stopping test
+ * ||b - A phi|| <= rtol ||b|| + atol on the moment residual; maxit <= 0 means unlimited.
+ * iters = number of operator applications, resid = final residual norm. */
+int lb_boltzmann_solve(lb_handle* h, double* s, int solver, int m, double rtol, double atol, int maxit,
+                       int* iters, double* resid);
+
+/* Multigroup downscatter solve with dose tally: replaces the group loop of src/main/Main.f90:326-476
+ * (PIEISource :544-747, OpL%MatInv :434, tapes, CalculateDeposition :750-824,
+ * TallyDeposition.f90:19) with device-resident flux moments instead of disk tapes.
+ *   sigt[G][Nm]; sigs[G][G][Nm][Ls+1] transfer g'->g Legendre moments (sigs[g][g] within-group);
+ *   dd[G][Nm] dose cross sections (XS%DD); unc[NENK] uncollided scalar flux of the beam in group 0
+ *   at every DG node; beam_dir[3] its direction (monodirectional first-collision source). */
+int lb_mg_set_problem(lb_handle* h, int G, int Ls, const double* sigt, const double* sigs, const double* dd,
+                      const double* unc, const double* beam_dir);
+/* Runs every group to the stopping test; iters[G] receives operator applications per group. */
+int lb_mg_solve(lb_handle* h, int solver, int m, double rtol, double atol, int maxit, int* iters);
+/* flux[G][NENK] scalar fluence (collided + uncollided), dose[NENK]; either may be NULL. */
+int lb_mg_get_results(lb_handle* h, double* flux, double* dose);
+
+/* Device-time phase timers (ms) accumulated since the last reset, and kernel launch counts. */
+int lb_get_timers(lb_handle* h, double* ms, long long* launches);
+int lb_reset_timers(lb_handle* h);
+/* Algorithmic traffic of one full sweep (bytes) and its update count (NE*NI). */
+int lb_sweep_stats(lb_handle* h, double* bytes_per_sweep, double* updates_per_sweep, long long* upstream_faces);
+int lb_synchronize(lb_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LIONBOLT_B200_H */

@@ -1,0 +1,594 @@
+// Host side of the B200 transport-solve library: handle management, mesh post-processing,
+// quadrature, real spherical harmonics, the per-direction wavefront schedule, and the simple
+// C-ABI entry points.  Compiled with -ffp-contract=off: the FP64 face-orientation tests must
+// round exactly like the reference's DOT_PRODUCT so that the sweep levels are bit-identical.
+#include "lb_internal.h"
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <omp.h>
+
+namespace lb {
+
+constexpr double PI = 3.14159265358979323846264338327950288;
+constexpr double EPS64 = 2.220446049250313080847263336181640625e-16;   // EPSILON(1d0)
+constexpr int F2K[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};  // gmsh tet faces
+
+int fail(Handle* h, int code, const std::string& msg) {
+    if (h) h->err = msg;
+    return code;
+}
+
+int cuda_fail(Handle* h, cudaError_t e, const char* what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    return fail(h, e == cudaErrorMemoryAllocation ? LB_ERR_OOM : LB_ERR_CUDA, m);
+}
+
+static double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+static void cross3(const double* a, const double* b, double* c) {
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// Euclidean norm with the overflow-safe scaling gfortran applies to NORM2.
+static double norm3(const double* x) {
+    double scale = 0.0, ssq = 1.0;
+    for (int i = 0; i < 3; ++i) {
+        if (x[i] == 0.0) continue;
+        double a = std::fabs(x[i]);
+        if (scale < a) { double r = scale / a; ssq = 1.0 + ssq * r * r; scale = a; }
+        else { double r = a / scale; ssq += r * r; }
+    }
+    return scale * std::sqrt(ssq);
+}
+
+// Real orthonormal spherical harmonics up to degree Ls at unit direction dir.
+// Index j = l*l + l + m, m = -l..l; cos(m phi) for m > 0, sin(|m| phi) for m < 0.
+void real_sh(int Ls, const double* dir, double* Y) {
+    const double ct = dir[2];
+    const double st = std::sqrt(std::max(0.0, 1.0 - ct * ct));
+    const double phi = std::atan2(dir[1], dir[0]);
+    std::vector<double> P((size_t)(Ls + 1) * (Ls + 1), 0.0);
+    auto at = [&](int l, int m) -> double& { return P[(size_t)l * (Ls + 1) + m]; };
+    at(0, 0) = 1.0;
+    for (int m = 1; m <= Ls; ++m) at(m, m) = at(m - 1, m - 1) * (2.0 * m - 1.0) * st;
+    for (int m = 0; m < Ls; ++m) at(m + 1, m) = (2.0 * m + 1.0) * ct * at(m, m);
+    for (int m = 0; m <= Ls; ++m)
+        for (int l = m + 2; l <= Ls; ++l)
+            at(l, m) = ((2.0 * l - 1.0) * ct * at(l - 1, m) - (l + m - 1.0) * at(l - 2, m)) / (l - m);
+    for (int l = 0; l <= Ls; ++l)
+        for (int m = -l; m <= l; ++m) {
+            int am = m < 0 ? -m : m;
+            double ratio = 1.0;
+            for (int q = l - am + 1; q <= l + am; ++q) ratio /= q;
+            double nrm = std::sqrt((2.0 * l + 1.0) / (4.0 * PI) * ratio);
+            double v = nrm * at(l, am);
+            if (m > 0) v *= std::sqrt(2.0) * std::cos(am * phi);
+            if (m < 0) v *= std::sqrt(2.0) * std::sin(am * phi);
+            Y[l * l + l + m] = v;
+        }
+}
+
+void timer_begin(Handle* h, int kind, Timer& t) {
+    if (!h->free_timers.empty()) { t = h->free_timers.back(); h->free_timers.pop_back(); }
+    else { cudaEventCreate(&t.a); cudaEventCreate(&t.b); }
+    t.kind = kind;
+    cudaEventRecord(t.a, h->stream);
+}
+
+void timer_end(Handle* h, Timer& t) {
+    cudaEventRecord(t.b, h->stream);
+    h->timers.push_back(t);
+    h->launches[t.kind] += 1;
+}
+
+void timers_flush(Handle* h) {
+    if (h->timers.empty()) return;
+    cudaStreamSynchronize(h->stream);
+    for (auto& t : h->timers) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, t.a, t.b) == cudaSuccess) h->acc_ms[t.kind] += ms;
+        h->free_timers.push_back(t);
+    }
+    h->timers.clear();
+}
+
+template <class T>
+static int dev_alloc(Handle* h, T** p, size_t count, const char* what) {
+    if (h->device < 0) return LB_OK;   // host-only handle: schedule and geometry are built, nothing is uploaded
+    if (*p) { cudaFree(*p); *p = nullptr; }
+    if (count == 0) return LB_OK;
+    cudaError_t e = cudaMalloc((void**)p, sizeof(T) * count);
+    if (e != cudaSuccess) { *p = nullptr; return cuda_fail(h, e, what); }
+    return LB_OK;
+}
+
+template <class T>
+static int dev_upload(Handle* h, T** p, const T* src, size_t count, const char* what) {
+    if (h->device < 0) return LB_OK;
+    int rc = dev_alloc(h, p, count, what);
+    if (rc) return rc;
+    if (count == 0) return LB_OK;
+    cudaError_t e = cudaMemcpyAsync(*p, src, sizeof(T) * count, cudaMemcpyHostToDevice, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, what);
+    e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, what);
+    return LB_OK;
+}
+
+static void free_all(Handle* h) {
+    void* ptrs[] = {h->d_geom, h->d_mat, h->d_items, h->d_chunks, h->d_done, h->d_status, h->d_dirs, h->d_sigt,
+                    h->d_psi, h->d_qext, h->d_Ym2d, h->d_Yd2m, h->d_sigl, h->d_lofj, h->d_V, h->d_Z, h->d_x,
+                    h->d_b, h->d_t, h->d_red, h->d_unc, h->d_phi_all, h->d_src, h->d_dose, h->d_flux,
+                    h->d_sigl_mg};
+    for (void* p : ptrs) if (p) cudaFree(p);
+    if (h->h_red) cudaFreeHost(h->h_red);
+    for (auto& t : h->timers) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
+    for (auto& t : h->free_timers) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
+}
+
+// ----------------------------------------------------------------------------------------------
+//  Wavefront levels of one direction: the ascending list of elements whose pending upstream
+//  faces are all released, level by level.  Each level equals the set the reference's rescanning
+//  loop (SweepOrder.f90:137-185) collects, because an element becomes ready exactly when its last
+//  upstream neighbour is released, and the reference releases neighbours only after a level is
+//  complete.  Cost O(NE log NE) instead of O(levels * NE).
+// ----------------------------------------------------------------------------------------------
+static bool build_direction(const Handle* h, int i, int* items, std::vector<int>& starts, long long& nz) {
+    const int NE = h->NE;
+    const double* kv = &h->k[(size_t)i * 3];
+    std::vector<uint8_t> upm(NE, 0), outm(NE, 0), cnt(NE, 0);
+    std::vector<int> cur, nxt;
+    cur.reserve(1024); nxt.reserve(1024);
+    nz = 0;
+    for (int e = 0; e < NE; ++e) {
+        uint8_t u = 0, o = 0;
+        for (int f = 0; f < 4; ++f) {
+            double kdotn = dot3(kv, &h->nrm[(size_t)e * 12 + f * 3]);
+            if (h->nbr[(size_t)e * 4 + f] >= 0 && kdotn < -EPS64) u |= (uint8_t)(1u << f);   // IsUpstream
+            if (!(kdotn < 0.0)) o |= (uint8_t)(1u << f);   // outflow term, TransportAlgebra.f90:148-152
+        }
+        upm[e] = u; outm[e] = o;
+        cnt[e] = (uint8_t)__builtin_popcount(u);
+        nz += cnt[e];
+        if (cnt[e] == 0) cur.push_back(e);
+    }
+    starts.clear();
+    int es = 0;
+    while (!cur.empty()) {
+        starts.push_back(es);
+        for (int e : cur) items[es++] = e | ((int)upm[e] << 24) | ((int)outm[e] << 28);
+        nxt.clear();
+        for (int e : cur)
+            for (int f = 0; f < 4; ++f) {
+                int ep = h->nbr[(size_t)e * 4 + f];
+                if (ep < 0) continue;
+                // local face of ep that faces e (first match, as FINDLOC in SweepOrder.f90:169)
+                for (int q = 0; q < 4; ++q)
+                    if (h->nbr[(size_t)ep * 4 + q] == e) {
+                        if ((upm[ep] >> q) & 1u) { if (--cnt[ep] == 0) nxt.push_back(ep); }
+                        break;
+                    }
+            }
+        std::sort(nxt.begin(), nxt.end());
+        cur.swap(nxt);
+    }
+    starts.push_back(es);
+    return es == NE;
+}
+
+}  // namespace lb
+
+using namespace lb;
+
+struct lb_handle : public lb::Handle {};
+
+extern "C" {
+
+int lb_version(void) { return 10000; }
+
+const char* lb_status_string(int s) {
+    switch (s) {
+        case LB_OK: return "ok";
+        case LB_ERR_ARG: return "invalid argument";
+        case LB_ERR_CUDA: return "CUDA error";
+        case LB_ERR_OOM: return "out of device memory";
+        case LB_ERR_CYCLE: return "sweep is stagnant (cyclic dependency)";
+        case LB_ERR_TIMEOUT: return "device dependency wait timed out";
+        case LB_ERR_NOCONV: return "iteration did not converge in the iteration limit";
+        case LB_ERR_NAN: return "residual norm is NaN";
+        case LB_ERR_STATE: return "operator not ready";
+        case LB_ERR_BREAKDOWN: return "Krylov breakdown";
+        default: return "unknown status";
+    }
+}
+
+int lb_create(int device, lb_handle** out) {
+    if (!out) return LB_ERR_ARG;
+    *out = nullptr;
+    if (device == -1) {
+        // host-only handle: mesh post-processing and sweep scheduling without a GPU
+        lb_handle* h = new lb_handle();
+        h->device = -1;
+        *out = h;
+        return LB_OK;
+    }
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) return LB_ERR_CUDA;
+    if (device < 0 || device >= ndev) return LB_ERR_ARG;
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) return LB_ERR_CUDA;
+    lb_handle* h = new lb_handle();
+    h->device = device;
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) { delete h; return LB_ERR_CUDA; }
+    cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (cudaMalloc(&h->d_status, sizeof(SweepStatus)) != cudaSuccess) { delete h; return LB_ERR_OOM; }
+    if (cudaMallocHost(&h->h_red, sizeof(double) * 65536) != cudaSuccess) { delete h; return LB_ERR_OOM; }
+    if (cudaMalloc(&h->d_red, sizeof(double) * 65536) != cudaSuccess) { delete h; return LB_ERR_OOM; }
+    *out = h;
+    return LB_OK;
+}
+
+int lb_destroy(lb_handle* h) {
+    if (!h) return LB_OK;
+    if (h->device < 0) { delete h; return LB_OK; }
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream);
+    free_all(h);
+    if (h->mlp) mlp_destroy(h);
+    cudaStreamDestroy(h->stream);
+    delete h;
+    return LB_OK;
+}
+
+int lb_last_error(const lb_handle* h, char* buf, int len) {
+    if (!buf || len <= 0) return LB_ERR_ARG;
+    const char* m = h ? h->err.c_str() : "";
+    std::strncpy(buf, m, (size_t)len - 1);
+    buf[len - 1] = '\0';
+    return LB_OK;
+}
+
+int lb_sn_quadrature(int Ng, int Nc, double* k, double* w) {
+    if (Ng < 1 || Nc < 1 || !k || !w) return LB_ERR_ARG;
+    // Gauss-Legendre by Newton iteration on P_Ng, ascending nodes
+    std::vector<double> mu(Ng), wg(Ng);
+    for (int i = 0; i < Ng; ++i) {
+        double z = std::cos(PI * (i + 0.75) / (Ng + 0.5)), p0 = 1, p1 = z, dp = 1;
+        for (int it = 0; it < 100; ++it) {
+            p0 = 1.0; p1 = z;
+            for (int l = 2; l <= Ng; ++l) { double p2 = ((2.0 * l - 1.0) * z * p1 - (l - 1.0) * p0) / l; p0 = p1; p1 = p2; }
+            dp = Ng * (z * p1 - p0) / (z * z - 1.0);
+            double dz = p1 / dp;
+            z -= dz;
+            if (std::fabs(dz) < 1e-16) break;
+        }
+        p0 = 1.0; p1 = z;
+        for (int l = 2; l <= Ng; ++l) { double p2 = ((2.0 * l - 1.0) * z * p1 - (l - 1.0) * p0) / l; p0 = p1; p1 = p2; }
+        dp = Ng * (z * p1 - p0) / (z * z - 1.0);
+        mu[Ng - 1 - i] = z;
+        wg[Ng - 1 - i] = 2.0 / ((1.0 - z * z) * dp * dp);
+    }
+    for (int i = 0; i < Ng / 2; ++i) {
+        double a = 0.5 * (mu[Ng - 1 - i] - mu[i]); mu[i] = -a; mu[Ng - 1 - i] = a;
+        double b = 0.5 * (wg[i] + wg[Ng - 1 - i]); wg[i] = b; wg[Ng - 1 - i] = b;
+    }
+    if (Ng % 2) mu[Ng / 2] = 0.0;
+    // SNPrep.f90:49-76: phi_j = (2j-1) pi / Nc, j outer, i inner, w = wG * 2 pi / Nc
+    int ii = 0;
+    for (int j = 1; j <= Nc; ++j) {
+        double phi = (2 * j - 1) * PI / Nc;
+        for (int i = 0; i < Ng; ++i, ++ii) {
+            double st = std::sqrt(1.0 - mu[i] * mu[i]);
+            k[ii * 3 + 0] = std::cos(phi) * st;
+            k[ii * 3 + 1] = std::sin(phi) * st;
+            k[ii * 3 + 2] = mu[i];
+            w[ii] = wg[i] * (2.0 * PI / Nc);
+        }
+    }
+    return LB_OK;
+}
+
+int lb_set_mesh(lb_handle* h, int NE, int NN, const double* rg, const int* node, const int* neighbors, const int* mat,
+                int Nm) {
+    if (!h) return LB_ERR_ARG;
+    if (NE <= 0 || NN <= 0 || !rg || !node || !neighbors || !mat) return fail(h, LB_ERR_ARG, "lb_set_mesh: null or empty input");
+    if (NE >= kMaxElems - 1) return fail(h, LB_ERR_ARG, "lb_set_mesh: at most 16777214 elements are supported");
+    if (Nm < 1 || Nm > 256) return fail(h, LB_ERR_ARG, "lb_set_mesh: Nm must be in 1..256");
+    if (h->device >= 0) cudaSetDevice(h->device);
+    for (long long q = 0; q < 4LL * NE; ++q) {
+        if (node[q] < 0 || node[q] >= NN) return fail(h, LB_ERR_ARG, "lb_set_mesh: node index out of range");
+        if (neighbors[q] < -1 || neighbors[q] >= NE) return fail(h, LB_ERR_ARG, "lb_set_mesh: neighbour index out of range");
+    }
+    for (int e = 0; e < NE; ++e)
+        if (mat[e] < 0 || mat[e] >= Nm) return fail(h, LB_ERR_ARG, "lb_set_mesh: material index out of range");
+    h->NE = NE; h->NN = NN; h->Nm = Nm; h->NENK = 4LL * NE;
+    h->rg.assign(rg, rg + (size_t)NN * 3);
+    h->node.assign(node, node + (size_t)NE * 4);
+    h->nbr.assign(neighbors, neighbors + (size_t)NE * 4);
+    h->mat.assign(mat, mat + NE);
+    h->nrm.assign((size_t)NE * 12, 0.0);
+    h->svec.assign((size_t)NE * 12, 0.0);
+    h->nbrpack.assign((size_t)NE * 4, 0u);
+    int bad = 0;
+#pragma omp parallel for schedule(static) reduction(+ : bad)
+    for (int e = 0; e < NE; ++e) {
+        const int* nd = &h->node[(size_t)e * 4];
+        double com[3] = {0, 0, 0};
+        for (int q = 0; q < 4; ++q) for (int d = 0; d < 3; ++d) com[d] += h->rg[(size_t)nd[q] * 3 + d];
+        for (int d = 0; d < 3; ++d) com[d] /= 4.0;
+        // volume = |triple product| / 6
+        double a1[3], a2[3], a3[3], cx[3];
+        for (int d = 0; d < 3; ++d) {
+            a1[d] = h->rg[(size_t)nd[1] * 3 + d] - h->rg[(size_t)nd[0] * 3 + d];
+            a2[d] = h->rg[(size_t)nd[2] * 3 + d] - h->rg[(size_t)nd[0] * 3 + d];
+            a3[d] = h->rg[(size_t)nd[3] * 3 + d] - h->rg[(size_t)nd[0] * 3 + d];
+        }
+        cross3(a2, a1, cx);
+        double vol = std::fabs(dot3(a3, cx)) / 6.0;
+        if (!(vol > 0.0)) { ++bad; continue; }
+        for (int f = 0; f < 4; ++f) {
+            // outward unit normal from the sorted face nodes, sign from the centroid
+            // (PostProcess.f90:64-83): n = (r3-r1) x (r2-r1), r_a sorted by global id
+            int fn[3] = {nd[F2K[f][0]], nd[F2K[f][1]], nd[F2K[f][2]]};
+            std::sort(fn, fn + 3);
+            const double* p1 = &h->rg[(size_t)fn[0] * 3];
+            const double* p2 = &h->rg[(size_t)fn[1] * 3];
+            const double* p3 = &h->rg[(size_t)fn[2] * 3];
+            double r1[3], r2[3], n[3], c[3];
+            for (int d = 0; d < 3; ++d) { r1[d] = p2[d] - p1[d]; r2[d] = p3[d] - p1[d]; c[d] = p1[d] - com[d]; }
+            cross3(r2, r1, n);
+            double nn = norm3(n);
+            double normfac = std::copysign(1.0, dot3(n, c)) / nn;
+            double area = 0.5 * nn;
+            for (int d = 0; d < 3; ++d) {
+                h->nrm[(size_t)e * 12 + f * 3 + d] = normfac * n[d];
+                h->svec[(size_t)e * 12 + f * 3 + d] = normfac * n[d] * area / vol;
+            }
+            // neighbour word: element, local indices (in the neighbour) of this face's nodes
+            int ep = h->nbr[(size_t)e * 4 + f];
+            uint32_t word = kNoNeighbour;
+            if (ep >= 0) {
+                const int* ndp = &h->node[(size_t)ep * 4];
+                uint32_t perm = 0;
+                int found = 0;
+                for (int j = 0; j < 3; ++j) {
+                    int gnode = nd[F2K[f][j]];
+                    for (int q = 0; q < 4; ++q) if (ndp[q] == gnode) { perm |= (uint32_t)q << (2 * j); ++found; break; }
+                }
+                bool back = false;
+                for (int q = 0; q < 4; ++q) back |= (h->nbr[(size_t)ep * 4 + q] == e);
+                if (found != 3 || !back) ++bad;
+                word = (uint32_t)ep | (perm << 24);
+            }
+            word |= (uint32_t)((h->mat[e] >> (2 * f)) & 3) << 30;
+            h->nbrpack[(size_t)e * 4 + f] = word;
+        }
+    }
+    if (bad) return fail(h, LB_ERR_ARG, "lb_set_mesh: degenerate element or non-conforming neighbour table");
+    // device geometry: per element {snx[4], sny[4], snz[4], nbrpack[4]} (64 bytes)
+    std::vector<float4> geom((size_t)NE * 4);
+    for (int e = 0; e < NE; ++e) {
+        float4 gx, gy, gz, gw;
+        float* px = &gx.x; float* py = &gy.x; float* pz = &gz.x;
+        for (int f = 0; f < 4; ++f) {
+            px[f] = (float)h->svec[(size_t)e * 12 + f * 3 + 0];
+            py[f] = (float)h->svec[(size_t)e * 12 + f * 3 + 1];
+            pz[f] = (float)h->svec[(size_t)e * 12 + f * 3 + 2];
+        }
+        uint32_t* pw = reinterpret_cast<uint32_t*>(&gw.x);
+        for (int f = 0; f < 4; ++f) pw[f] = h->nbrpack[(size_t)e * 4 + f];
+        geom[(size_t)e * 4 + 0] = gx; geom[(size_t)e * 4 + 1] = gy;
+        geom[(size_t)e * 4 + 2] = gz; geom[(size_t)e * 4 + 3] = gw;
+    }
+    int rc = dev_upload(h, &h->d_geom, geom.data(), geom.size(), "upload geometry");
+    if (rc) return rc;
+    rc = dev_upload(h, &h->d_mat, h->mat.data(), h->mat.size(), "upload materials");
+    if (rc) return rc;
+    h->mesh_ready = true;
+    h->angle_ready = false;
+    h->phys_ready = false;
+    return LB_OK;
+}
+
+int lb_set_quadrature(lb_handle* h, int NI, const double* k, const double* w) {
+    if (!h) return LB_ERR_ARG;
+    if (!h->mesh_ready) return fail(h, LB_ERR_STATE, "lb_set_quadrature: mesh not set");
+    if (NI <= 0 || NI >= (1 << 24) || !k || !w) return fail(h, LB_ERR_ARG, "lb_set_quadrature: bad NI or null input");
+    if (h->device >= 0) cudaSetDevice(h->device);
+    const int NE = h->NE;
+    h->NI = NI;
+    h->NIpad = (NI + 15) / 16 * 16;
+    h->k.assign(k, k + (size_t)NI * 3);
+    h->w.assign(w, w + NI);
+    h->items.assign((size_t)NI * NE, 0);
+    std::vector<std::vector<int>> starts(NI);
+    std::vector<long long> nz(NI, 0);
+    int cyc = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : cyc)
+    for (int i = 0; i < NI; ++i)
+        if (!build_direction(h, i, &h->items[(size_t)i * NE], starts[i], nz[i])) ++cyc;
+    if (cyc) {
+        h->angle_ready = false;
+        return fail(h, LB_ERR_CYCLE, "SweepOrder: Sweep is stagnant. Check the mesh for errors, as this may imply "
+                                     "discontinuity in face/element indexing.");
+    }
+    h->nlev.assign(NI, 0);
+    h->lvl_base.assign(NI + 1, 0);
+    h->lvl_start.clear();
+    h->nz_upstream = 0;
+    int maxlev = 0;
+    for (int i = 0; i < NI; ++i) {
+        h->nlev[i] = (int)starts[i].size() - 1;
+        h->lvl_base[i] = (int)h->lvl_start.size();
+        h->lvl_start.insert(h->lvl_start.end(), starts[i].begin(), starts[i].end());
+        h->nz_upstream += nz[i];
+        maxlev = std::max(maxlev, h->nlev[i]);
+    }
+    h->lvl_base[NI] = (int)h->lvl_start.size();
+    // global level ids: gid(i, L) = sum_{i'<i} nlev[i'] + L
+    std::vector<int> gbase(NI + 1, 0);
+    for (int i = 0; i < NI; ++i) gbase[i + 1] = gbase[i] + h->nlev[i];
+    h->total_levels = gbase[NI];
+    // chunk list, level-major across directions: every chunk's dependencies (the previous level
+    // of its own direction) precede it, so claiming chunks in order can never deadlock.
+    std::vector<int4> chunks;
+    chunks.reserve((size_t)NI * NE / 24 + 16);
+    for (int L = 0; L < maxlev; ++L)
+        for (int i = 0; i < NI; ++i) {
+            if (L >= h->nlev[i]) continue;
+            const int* st = &h->lvl_start[h->lvl_base[i]];
+            int a = st[L], b = st[L + 1];
+            int prev = (L > 0) ? (st[L] - st[L - 1]) : 0;
+            for (int s = a; s < b; s += 32) {
+                int n = std::min(32, b - s);
+                chunks.push_back(make_int4(i | ((n - 1) << 24), s, gbase[i] + L, prev));
+            }
+        }
+    if (chunks.size() >= (size_t)INT32_MAX) return fail(h, LB_ERR_ARG, "lb_set_quadrature: problem too large");
+    h->nchunks = (int)chunks.size();
+    int rc = dev_upload(h, &h->d_items, h->items.data(), h->items.size(), "upload sweep items");
+    if (rc) return rc;
+    rc = dev_upload(h, &h->d_chunks, chunks.data(), chunks.size(), "upload sweep chunks");
+    if (rc) return rc;
+    rc = dev_alloc(h, &h->d_done, (size_t)h->total_levels, "level counters");
+    if (rc) return rc;
+    std::vector<float4> dirs(NI);
+    for (int i = 0; i < NI; ++i)
+        dirs[i] = make_float4((float)k[i * 3], (float)k[i * 3 + 1], (float)k[i * 3 + 2], (float)w[i]);
+    rc = dev_upload(h, &h->d_dirs, dirs.data(), dirs.size(), "upload directions");
+    if (rc) return rc;
+    size_t pe = (size_t)NI * (size_t)h->NENK;
+    if (h->device >= 0 && h->psi_elems != pe) {
+        rc = dev_alloc(h, &h->d_psi, pe, "angular work vector");
+        if (rc) return rc;
+        if (h->d_qext) { cudaFree(h->d_qext); h->d_qext = nullptr; }
+        h->psi_elems = pe;
+    }
+    h->angle_ready = true;
+    h->phys_ready = false;
+    return LB_OK;
+}
+
+int lb_get_schedule(lb_handle* h, int* sl, unsigned char* upmask, int* nlevels, int* level_start) {
+    if (!h) return LB_ERR_ARG;
+    if (!h->angle_ready) return fail(h, LB_ERR_STATE, "lb_get_schedule: quadrature not set");
+    const int NE = h->NE, NI = h->NI;
+    for (size_t q = 0; q < (size_t)NI * NE; ++q) {
+        int it = h->items[q];
+        if (sl) sl[q] = it & (kMaxElems - 1);
+        if (upmask) upmask[q] = (unsigned char)((it >> 24) & 0xF);
+    }
+    for (int i = 0; i < NI; ++i) {
+        if (nlevels) nlevels[i] = h->nlev[i];
+        if (level_start)
+            for (int L = 0; L <= h->nlev[i]; ++L) level_start[(size_t)i * (NE + 1) + L] = h->lvl_start[h->lvl_base[i] + L];
+    }
+    return LB_OK;
+}
+
+int lb_set_xs(lb_handle* h, int Ls, const double* sigt, const double* sigs) {
+    if (!h) return LB_ERR_ARG;
+    if (!h->angle_ready) return fail(h, LB_ERR_STATE, "lb_set_xs: quadrature not set");
+    if (Ls < 0 || Ls > 15 || !sigt || !sigs) return fail(h, LB_ERR_ARG, "lb_set_xs: Ls must be in 0..15");
+    if (h->device >= 0) cudaSetDevice(h->device);
+    const int Nm = h->Nm, NI = h->NI, NIpad = h->NIpad;
+    for (int m = 0; m < Nm; ++m)
+        if (!(sigt[m] >= 0.0) || !std::isfinite(sigt[m])) return fail(h, LB_ERR_NAN, "lb_set_xs: invalid total cross section");
+    h->sigt.assign(sigt, sigt + Nm);
+    h->sigs.assign(sigs, sigs + (size_t)Nm * (Ls + 1));
+    int nm = (Ls + 1) * (Ls + 1);
+    int nmpad = (nm + 15) / 16 * 16;
+    bool rebuild = (Ls != h->Ls) || (h->ybuilt_NI != NI);
+    h->Ls = Ls; h->nm = nm; h->nmpad = nmpad;
+    int rc;
+    std::vector<float> st(Nm);
+    for (int m = 0; m < Nm; ++m) st[m] = (float)sigt[m];
+    rc = dev_upload(h, &h->d_sigt, st.data(), st.size(), "upload sigt");
+    if (rc) return rc;
+    std::vector<float> sl((size_t)Nm * nmpad, 0.f);
+    for (int m = 0; m < Nm; ++m)
+        for (int l = 0; l <= Ls; ++l)
+            for (int j = l * l; j < (l + 1) * (l + 1); ++j) sl[(size_t)m * nmpad + j] = (float)sigs[(size_t)m * (Ls + 1) + l];
+    rc = dev_upload(h, &h->d_sigl, sl.data(), sl.size(), "upload sigma_l");
+    if (rc) return rc;
+    if (rebuild || !h->d_Ym2d) {
+        // split Y into three BF16 planes (hi + mid + lo carries 24 significant bits)
+        std::vector<__nv_bfloat16> ym((size_t)3 * NIpad * nmpad), yd((size_t)3 * nmpad * NIpad);
+        std::vector<double> Y(nm);
+        auto split3 = [](double v, __nv_bfloat16* o3) {
+            float f = (float)v;
+            __nv_bfloat16 a = __float2bfloat16_rn(f);
+            float r1 = f - __bfloat162float(a);
+            __nv_bfloat16 b = __float2bfloat16_rn(r1);
+            float r2 = r1 - __bfloat162float(b);
+            o3[0] = a; o3[1] = b; o3[2] = __float2bfloat16_rn(r2);
+        };
+        for (auto& v : ym) v = __float2bfloat16_rn(0.f);
+        for (auto& v : yd) v = __float2bfloat16_rn(0.f);
+        for (int i = 0; i < NI; ++i) {
+            real_sh(Ls, &h->k[(size_t)i * 3], Y.data());
+            for (int j = 0; j < nm; ++j) {
+                __nv_bfloat16 o3[3];
+                split3(Y[j], o3);
+                for (int p = 0; p < 3; ++p) ym[((size_t)p * NIpad + i) * nmpad + j] = o3[p];
+                split3(h->w[i] * Y[j], o3);
+                for (int p = 0; p < 3; ++p) yd[((size_t)p * nmpad + j) * NIpad + i] = o3[p];
+            }
+        }
+        rc = dev_upload(h, &h->d_Ym2d, ym.data(), ym.size(), "upload M2D operator");
+        if (rc) return rc;
+        rc = dev_upload(h, &h->d_Yd2m, yd.data(), yd.size(), "upload D2M operator");
+        if (rc) return rc;
+        h->ybuilt_NI = NI;
+    }
+    h->phys_ready = true;
+    return LB_OK;
+}
+
+int lb_get_timers(lb_handle* h, double* ms, long long* launches) {
+    if (!h) return LB_ERR_ARG;
+    if (h->device < 0) return fail(h, LB_ERR_STATE, "host-only handle");
+    cudaSetDevice(h->device);
+    timers_flush(h);
+    for (int q = 0; q < LB_NTIMERS; ++q) {
+        if (ms) ms[q] = h->acc_ms[q];
+        if (launches) launches[q] = h->launches[q];
+    }
+    return LB_OK;
+}
+
+int lb_reset_timers(lb_handle* h) {
+    if (!h) return LB_ERR_ARG;
+    if (h->device < 0) return fail(h, LB_ERR_STATE, "host-only handle");
+    cudaSetDevice(h->device);
+    timers_flush(h);
+    for (int q = 0; q < LB_NTIMERS; ++q) { h->acc_ms[q] = 0; h->launches[q] = 0; }
+    return LB_OK;
+}
+
+int lb_sweep_stats(lb_handle* h, double* bytes, double* updates, long long* upfaces) {
+    if (!h || !h->angle_ready) return LB_ERR_STATE;
+    double upd = (double)h->NE * h->NI;
+    // algorithmic bytes: q read (16 B) + psi write (16 B) + 3 FP32 face values per upstream face
+    // (12 B) per update, plus the packed schedule item (4 B) and one 64-B element record per pass
+    double b = upd * (16.0 + 16.0 + 4.0) + 12.0 * (double)h->nz_upstream + 64.0 * h->NE;
+    if (bytes) *bytes = b;
+    if (updates) *updates = upd;
+    if (upfaces) *upfaces = h->nz_upstream;
+    return LB_OK;
+}
+
+int lb_synchronize(lb_handle* h) {
+    if (!h) return LB_ERR_ARG;
+    if (h->device < 0) return LB_OK;
+    cudaSetDevice(h->device);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "synchronize");
+    return LB_OK;
+}
+
+}  // extern "C"

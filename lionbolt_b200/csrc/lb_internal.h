@@ -1,0 +1,167 @@
+// Internal state and kernel launchers of the B200 transport-solve library.
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+#include "../../include/lionbolt_b200.h"
+
+namespace lb {
+
+// Packed schedule item (one per element-direction, in sweep order):
+//   bits 0-23 element id, bits 24-27 upstream-face mask, bits 28-31 outflow-face mask.
+constexpr int kElemBits = 24;
+constexpr int kMaxElems = 1 << kElemBits;
+// Packed neighbour word (one per element face):
+//   bits 0-23 neighbour element (0xFFFFFF on the boundary), bits 24-29 three 2-bit local node
+//   indices in the neighbour of this face's nodes (gmsh face order), bits 30-31 two bits of the
+//   element's material id (face f holds bits 2f, 2f+1).
+constexpr uint32_t kNoNeighbour = 0xFFFFFFu;
+
+// Sweep chunk: up to 32 consecutive items of one (direction, level).
+//   x = direction | (count-1) << 24, y = first sweep position, z = global level id,
+//   w = size of the previous level of the same direction (0 for the first level).
+struct SweepStatus {
+    int work;        // next chunk to claim
+    int abort;       // set on any timeout; every warp stops
+    int err;         // LB_ERR_TIMEOUT when set
+    int err_chunk;   // chunk whose wait gave up
+};
+
+struct Timer {
+    cudaEvent_t a, b;
+    int kind;
+};
+
+struct DeviceBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+struct Handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int sm_count = 0;
+
+    // ---- mesh (host) ----
+    int NE = 0, NN = 0, Nm = 0;
+    long long NENK = 0;
+    std::vector<double> rg;        // [NN][3]
+    std::vector<int> node, nbr;    // [NE][4]
+    std::vector<int> mat;          // [NE]
+    std::vector<double> nrm;       // [NE][4][3] FP64 outward unit normals
+    std::vector<double> svec;      // [NE][4][3] area*n/volume (FP64)
+    std::vector<uint32_t> nbrpack; // [NE][4]
+    bool mesh_ready = false;
+
+    // ---- angular ----
+    int NI = 0, NIpad = 0;         // directions, and rounded up to a multiple of 16
+    std::vector<double> k, w;      // [NI][3], [NI]
+    std::vector<int> items;        // [NI][NE] packed sweep items
+    std::vector<int> lvl_start;    // concatenated level starts per direction
+    std::vector<int> lvl_base;     // [NI+1] offset of each direction's levels in lvl_start
+    std::vector<int> nlev;         // [NI]
+    long long nz_upstream = 0;
+    int nchunks = 0;
+    int total_levels = 0;
+    bool angle_ready = false;
+
+    // ---- physics ----
+    int Ls = -1, nm = 0, nmpad = 0, ybuilt_NI = -1;
+    std::vector<double> sigt, sigs;  // within group: [Nm], [Nm][Ls+1]
+    bool phys_ready = false;
+
+    // ---- device buffers ----
+    float4* d_geom = nullptr;      // [NE][4] (snx, sny, snz, nbrpack)
+    int* d_mat = nullptr;          // [NE]
+    int* d_items = nullptr;        // [NI][NE]
+    int4* d_chunks = nullptr;      // [nchunks]
+    int* d_done = nullptr;         // [total_levels]
+    SweepStatus* d_status = nullptr;
+    float4* d_dirs = nullptr;      // [NI] (kx, ky, kz, w)
+    float* d_sigt = nullptr;       // [Nm]
+    float* d_psi = nullptr;        // [NI][NENK] FP32 angular work vector
+    float* d_qext = nullptr;       // [NI][NENK] FP32 angular external source (angular API)
+    // moment-space operators (split BF16 hi/mid/lo planes)
+    __nv_bfloat16* d_Ym2d = nullptr;  // [3][NIpad][nmpad] Y_j(k_i)
+    __nv_bfloat16* d_Yd2m = nullptr;  // [3][nmpad][NIpad] w_i Y_j(k_i)
+    float* d_sigl = nullptr;          // [Nm][nmpad]  sigma_l(j) per material (within group)
+    int* d_lofj = nullptr;
+    size_t psi_elems = 0;
+
+    // ---- Krylov workspace (FP64, moment space) ----
+    int kry_m = 0;
+    double* d_V = nullptr;         // [(m+1)][N] basis
+    double* d_Z = nullptr;         // [m][N] flexible basis (FGMRES)
+    double* d_x = nullptr;         // solution
+    double* d_b = nullptr;         // rhs
+    double* d_t = nullptr;         // scratch
+    double* d_red = nullptr;       // reduction partials
+    double* h_red = nullptr;       // pinned host copy of reductions
+    size_t kry_n = 0;
+
+    // ---- multigroup ----
+    int G = 0;
+    std::vector<double> mg_sigt, mg_sigs, mg_dd;  // [G][Nm], [G][G][Nm][Ls+1], [G][Nm]
+    std::vector<double> beam_dir;
+    double* d_unc = nullptr;        // [NENK]
+    double* d_phi_all = nullptr;    // [G][nm][NENK] collided flux moments
+    double* d_src = nullptr;        // [nm][NENK] group source moments
+    double* d_dose = nullptr;       // [NENK]
+    double* d_flux = nullptr;       // [G][NENK]
+    float* d_sigl_mg = nullptr;     // [Nm][nmpad] scratch for transfer scaling
+
+    // ---- timers ----
+    std::vector<Timer> timers;
+    std::vector<Timer> free_timers;
+    double acc_ms[LB_NTIMERS] = {0};
+    long long launches[LB_NTIMERS] = {0};
+
+    // learned preconditioner state (mlp.cu)
+    void* mlp = nullptr;
+};
+
+// ---- host helpers (host.cpp) ----
+int fail(Handle* h, int code, const std::string& msg);
+int cuda_fail(Handle* h, cudaError_t e, const char* what);
+void real_sh(int Ls, const double* dir, double* Y);
+
+// ---- learned preconditioner (mlp.cu) ----
+void mlp_destroy(Handle* h);
+bool mlp_ready(Handle* h);
+int mlp_apply_precond(Handle* h, const double* v, double* z);
+
+// ---- timers ----
+void timer_begin(Handle* h, int kind, Timer& t);
+void timer_end(Handle* h, Timer& t);
+void timers_flush(Handle* h);
+
+// ---- kernels (sweep.cu / moments.cu / krylov.cu) ----
+// Full transport sweep psi <- T^{-1} psi (FP32, in place, natural layout [NI][NENK]).
+int launch_sweep(Handle* h, float* psi);
+// q[i][n] = sum_j Y_j(k_i) * (sigl[mat(n)][j] * x[j][n] + a[j][n]) (+ qadd[i][n] if given).
+// x and a are FP64 moment vectors [nm][NENK]; either may be null.
+int launch_m2d(Handle* h, const double* x, const float* sigl, const double* a, const float* qadd, float* q);
+// z[j][n] = sum_i w_i Y_j(k_i) psi[i][n]; out[j][n] = alpha * xin[j][n] + beta * z[j][n]
+// (xin may be null: out = beta * z).
+int launch_d2m(Handle* h, const float* psi, const double* xin, double alpha, double beta, double* out);
+
+// FP64 BLAS-1 on device vectors of length n
+int k_dots(Handle* h, const double* V, size_t ldv, int nv, const double* w, size_t n, double* out_host);
+int k_multi_axpy(Handle* h, double* w, const double* V, size_t ldv, int nv, const double* coef_host, size_t n);
+int k_axpby(Handle* h, double* y, const double* x, double a, double b, size_t n);   // y = a*x + b*y
+int k_scale(Handle* h, double* y, double a, size_t n);
+int k_copy(Handle* h, double* y, const double* x, size_t n);
+int k_fill(Handle* h, double* y, double v, size_t n);
+int k_f64_to_f32(Handle* h, float* y, const double* x, size_t n);
+int k_f32_to_f64(Handle* h, double* y, const float* x, size_t n);
+int k_dose_tally(Handle* h, const double* phi00, const double* unc, double unc_scale, const double* dd_mat,
+                 const int* mat, double* flux, double* dose, long long NENK);
+int k_moment_source(Handle* h, double* src, const double* phi, const float* sigl, const int* mat, long long NENK,
+                    int nm, int nmpad, int accumulate);
+int k_unc_source(Handle* h, double* src, const double* unc, const double* ybeam, const float* sigl, const int* mat,
+                 long long NENK, int nm, int nmpad);
+
+}  // namespace lb

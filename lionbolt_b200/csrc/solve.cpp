@@ -1,0 +1,469 @@
+// Operator applications and Krylov drivers in flux-moment space.
+//
+// Reference algorithm: BoltzmannOp%MatInv (BoltzmannOperator.f90:106-151) solves
+// (I - T^{-1}K) psi = T^{-1} q with SPARSKIT GMRES(m) on the full angular flux
+// (n = NENK*NI, iters.f:1901-2206) or with source iteration (SourceIteration.f90).
+// Here K = M Sigma D (exact, see moments.cu), so with phi = D psi the same fixed point solves
+//   A phi = (I - D T^{-1} M Sigma) phi = b,   b = D T^{-1} q,
+// and psi = T^{-1}(M Sigma phi + q).  The Krylov vectors shrink from NI*NENK to nm*NENK
+// (288 -> 36 per node at P5) and stay FP64; the sweep and the moment GEMMs run in FP32.
+// The Arnoldi/Givens/restart logic and the stopping test ||b - A phi|| <= rtol||b|| + atol follow
+// the reference's SPARSKIT gmres/fgmres; orthogonalisation is classical Gram-Schmidt with
+// selective re-orthogonalisation (one fused multi-dot and one fused multi-axpy per pass).
+#include "lb_internal.h"
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <omp.h>
+
+namespace lb {
+
+int k_multi_axpy_norm(Handle* h, double* w, const double* V, size_t ldv, int nv, const double* coef, size_t n, double* nrm2);
+
+static int need_ready(Handle* h, bool phys = true) {
+    if (h->device < 0) return fail(h, LB_ERR_STATE, "host-only handle: no device attached");
+    if (!h->mesh_ready || !h->angle_ready || (phys && !h->phys_ready))
+        return fail(h, LB_ERR_STATE, "operator was called, but the operator was not ready");
+    return LB_OK;
+}
+
+static int ensure_krylov(Handle* h, int m, bool flexible) {
+    size_t n = (size_t)h->nm * (size_t)h->NENK;
+    bool realloc_v = (h->kry_n != n) || (h->kry_m < m) || !h->d_V;
+    if (realloc_v) {
+        if (h->d_V) cudaFree(h->d_V);
+        if (h->d_x) cudaFree(h->d_x);
+        if (h->d_b) cudaFree(h->d_b);
+        if (h->d_t) cudaFree(h->d_t);
+        if (h->d_Z) { cudaFree(h->d_Z); h->d_Z = nullptr; }
+        h->d_V = h->d_x = h->d_b = h->d_t = nullptr;
+        cudaError_t e = cudaMalloc(&h->d_V, sizeof(double) * n * (size_t)(m + 1));
+        if (e == cudaSuccess) e = cudaMalloc(&h->d_x, sizeof(double) * n);
+        if (e == cudaSuccess) e = cudaMalloc(&h->d_b, sizeof(double) * n);
+        if (e == cudaSuccess) e = cudaMalloc(&h->d_t, sizeof(double) * n);
+        if (e != cudaSuccess) return cuda_fail(h, e, "Krylov workspace");
+        h->kry_n = n;
+        h->kry_m = m;
+    }
+    if (!h->d_red) {
+        cudaError_t e = cudaMalloc(&h->d_red, sizeof(double) * 65536);
+        if (e != cudaSuccess) return cuda_fail(h, e, "reduction buffer");
+    }
+    if (flexible && !h->d_Z) {
+        cudaError_t e = cudaMalloc(&h->d_Z, sizeof(double) * n * (size_t)h->kry_m);
+        if (e != cudaSuccess) return cuda_fail(h, e, "FGMRES workspace");
+    }
+    return LB_OK;
+}
+
+// y = A x = x - D T^{-1} M Sigma x   (sigl: per-material sigma_l table, within group)
+static int apply_A(Handle* h, const double* x, double* y, const float* sigl) {
+    int rc = launch_m2d(h, x, sigl, nullptr, nullptr, h->d_psi);
+    if (!rc) rc = launch_sweep(h, h->d_psi);
+    if (!rc) rc = launch_d2m(h, h->d_psi, x, 1.0, -1.0, y);
+    return rc;
+}
+
+// y = D T^{-1} (M (Sigma x + a) + qext)   (any of x, a, qext may be null)
+static int apply_transport_moments(Handle* h, const double* x, const float* sigl, const double* a, const float* qext,
+                                   double* y) {
+    int rc;
+    if (!x && !a) {
+        if (!qext) return fail(h, LB_ERR_ARG, "empty source");
+        cudaError_t e = cudaMemcpyAsync(h->d_psi, qext, sizeof(float) * h->psi_elems, cudaMemcpyDeviceToDevice, h->stream);
+        if (e != cudaSuccess) return cuda_fail(h, e, "copy source");
+        rc = LB_OK;
+    } else {
+        rc = launch_m2d(h, x, sigl, a, qext, h->d_psi);
+    }
+    if (!rc) rc = launch_sweep(h, h->d_psi);
+    if (!rc) rc = launch_d2m(h, h->d_psi, nullptr, 0.0, 1.0, y);
+    return rc;
+}
+
+static double vnorm(Handle* h, const double* v, size_t n, int* rc) {
+    double s = 0.0;
+    *rc = k_dots(h, v, n, 1, v, n, &s);
+    return std::sqrt(s);
+}
+
+struct KrylovResult {
+    int status = LB_OK;
+    int nmv = 0;
+    double resid = 0.0;
+};
+
+using DevOp = std::function<int(const double* in, double* out)>;
+
+// Restarted GMRES(m) / FGMRES(m) (right preconditioner `prec`), SPARSKIT semantics.
+static KrylovResult gmres_device(Handle* h, size_t n, const double* rhs, double* sol, int m, double rtol, double atol,
+                                 int maxit, const DevOp& matvec, const DevOp* prec) {
+    KrylovResult res;
+    int rc = 0;
+    double* V = h->d_V;
+    double* Z = h->d_Z;
+    std::vector<std::vector<double>> H(m + 2, std::vector<double>(m + 2, 0.0));   // H[col][row]
+    std::vector<double> c(m + 2), s(m + 2), rs(m + 2), hh(m + 2), h2(m + 2);
+    double rn = vnorm(h, rhs, n, &rc);
+    if (rc) { res.status = rc; return res; }
+    const double fpar4 = rtol * rn + atol;
+    double fpar5 = 0.0;
+    int nmv = 0;
+    while (true) {
+        // r = rhs - A sol
+        if ((rc = matvec(sol, V))) { res.status = rc; return res; }
+        ++nmv;
+        k_axpby(h, V, rhs, 1.0, -1.0, n);     // V0 = rhs - V0
+        double alpha = vnorm(h, V, n, &rc);
+        if (rc) { res.status = rc; return res; }
+        if (std::isnan(alpha)) { res.status = fail(h, LB_ERR_NAN, "RESIDUAL NORM is NaN."); return res; }
+        fpar5 = alpha;
+        rs[1] = alpha;
+        if (alpha <= fpar4) { res.status = LB_OK; res.nmv = nmv; res.resid = alpha; return res; }
+        k_scale(h, V, 1.0 / alpha, n);
+        int k = 0;
+        bool breakdown = false;
+        while (true) {
+            ++k;
+            const double* vin = V + (size_t)(k - 1) * n;
+            if (prec) {
+                if ((rc = (*prec)(vin, Z + (size_t)(k - 1) * n))) { res.status = rc; return res; }
+                vin = Z + (size_t)(k - 1) * n;
+            }
+            double* vk = V + (size_t)k * n;
+            if ((rc = matvec(vin, vk))) { res.status = rc; return res; }
+            ++nmv;
+            // orthogonalise vk against V[0..k-1]
+            if ((rc = k_dots(h, V, n, k + 1, vk, n, hh.data()))) { res.status = rc; return res; }
+            double nrm0 = hh[k];
+            double nrm1 = 0.0;
+            if ((rc = k_multi_axpy_norm(h, vk, V, n, k, hh.data(), n, &nrm1))) { res.status = rc; return res; }
+            if (nrm1 < 0.5 * nrm0) {
+                // significant cancellation: orthogonalise once more
+                if ((rc = k_dots(h, V, n, k, vk, n, h2.data()))) { res.status = rc; return res; }
+                if ((rc = k_multi_axpy_norm(h, vk, V, n, k, h2.data(), n, &nrm1))) { res.status = rc; return res; }
+                for (int i = 0; i < k; ++i) hh[i] += h2[i];
+            }
+            double hk = std::sqrt(std::max(0.0, nrm1));
+            if (std::isnan(hk)) { res.status = fail(h, LB_ERR_NAN, "RESIDUAL NORM is NaN."); return res; }
+            for (int i = 0; i < k; ++i) H[k][i + 1] = hh[i];
+            H[k][k + 1] = hk;
+            if (!(hk > 0.0)) { breakdown = true; --k; break; }
+            k_scale(h, vk, 1.0 / hk, n);
+            for (int i = 1; i <= k - 1; ++i) {
+                double a = H[k][i];
+                H[k][i] = c[i] * a + s[i] * H[k][i + 1];
+                H[k][i + 1] = c[i] * H[k][i + 1] - s[i] * a;
+            }
+            // SPARSKIT givens (iters.f:3225-3262)
+            double x = H[k][k], y = H[k][k + 1], cc, ss;
+            if (x == 0.0 && y == 0.0) { cc = 1.0; ss = 0.0; }
+            else if (std::fabs(y) > std::fabs(x)) { double t = x / y; x = std::sqrt(1.0 + t * t); ss = std::copysign(1.0 / x, y); cc = t * ss; }
+            else { double t = y / x; y = std::sqrt(1.0 + t * t); cc = std::copysign(1.0 / y, x); ss = t * cc; }
+            H[k][k] = std::fabs(x * y);
+            H[k][k + 1] = 0.0;
+            c[k] = cc; s[k] = ss;
+            double a = -ss * rs[k];
+            rs[k] = cc * rs[k];
+            rs[k + 1] = a;
+            alpha = std::fabs(a);
+            fpar5 = alpha;
+            if (k < m && !(alpha <= fpar4) && (maxit <= 0 || nmv < maxit)) continue;
+            break;
+        }
+        while (k > 0 && H[k][k] == 0.0) --k;
+        if (k == 0) {
+            if (breakdown) continue;   // nothing new in the basis: recompute the true residual
+            res.status = fail(h, LB_ERR_BREAKDOWN, "GMRES : Anticipated breakdown / division by zero.");
+            return res;
+        }
+        rs[k] = rs[k] / H[k][k];
+        for (int i = k - 1; i >= 1; --i) {
+            for (int ii = 1; ii <= i; ++ii) rs[ii] = rs[ii] - rs[i + 1] * H[i + 1][ii];
+            rs[i] = rs[i] / H[i][i];
+        }
+        // sol += sum_i y_i V_i (or Z_i): multi-axpy with negated coefficients
+        std::vector<double> coef(k);
+        for (int i = 0; i < k; ++i) coef[i] = -rs[i + 1];
+        if ((rc = k_multi_axpy(h, sol, prec ? Z : V, n, k, coef.data(), n))) { res.status = rc; return res; }
+        if (breakdown) continue;
+        if ((nmv < maxit || maxit <= 0) && fpar5 > fpar4) continue;
+        res.nmv = nmv;
+        res.resid = fpar5;
+        if (fpar5 <= fpar4) {
+            res.status = LB_OK;
+        } else {
+            res.status = fail(h, LB_ERR_NOCONV, "GMRES : Iteration did not converge in specified iteration limits.");
+        }
+        return res;
+    }
+}
+
+// Source iteration (SourceIteration.f90:33-80) in moment space: phi = b; w = b;
+// repeat w <- D T^{-1} M Sigma w; phi += w until ||w|| <= atol + rtol ||b||.
+static KrylovResult si_device(Handle* h, size_t n, const double* b, double* phi, double rtol, double atol, int maxit,
+                              const float* sigl) {
+    KrylovResult res;
+    int rc = 0;
+    double* w = h->d_t;
+    k_copy(h, phi, b, n);
+    k_copy(h, w, b, n);
+    double norms = vnorm(h, b, n, &rc);
+    int it = 1;
+    if ((rc = apply_transport_moments(h, w, sigl, nullptr, nullptr, w))) { res.status = rc; return res; }
+    k_axpby(h, phi, w, 1.0, 1.0, n);
+    while (true) {
+        ++it;
+        double rn = vnorm(h, w, n, &rc);
+        if (rc) { res.status = rc; return res; }
+        res.resid = rn;
+        res.nmv = it;
+        if (std::isnan(rn)) { res.status = fail(h, LB_ERR_NAN, "RESIDUAL NORM is NaN."); return res; }
+        if (rn <= atol + norms * rtol) return res;
+        if (maxit > 0 && it > maxit) { res.status = fail(h, LB_ERR_NOCONV, "SI did not converge in the iteration limit"); return res; }
+        if ((rc = apply_transport_moments(h, w, sigl, nullptr, nullptr, w))) { res.status = rc; return res; }
+        k_axpby(h, phi, w, 1.0, 1.0, n);
+    }
+}
+
+// Solve A phi = b in moment space with the selected solver; phi holds the initial guess.
+static KrylovResult moment_solve(Handle* h, const double* b, double* phi, int solver, int m, double rtol, double atol,
+                                 int maxit, const float* sigl) {
+    const size_t n = (size_t)h->nm * (size_t)h->NENK;
+    if (solver == LB_SOLVER_SI) return si_device(h, n, b, phi, rtol, atol, maxit, sigl);
+    DevOp mv = [h, sigl](const double* in, double* out) { return apply_A(h, in, out, sigl); };
+    if (solver == LB_SOLVER_FGMRES_ML) {
+        if (!mlp_ready(h)) {
+            // plain GMRES is the fallback when no trained network is loaded
+            return gmres_device(h, n, b, phi, m, rtol, atol, maxit, mv, nullptr);
+        }
+        DevOp pc = [h](const double* in, double* out) { return mlp_apply_precond(h, in, out); };
+        return gmres_device(h, n, b, phi, m, rtol, atol, maxit, mv, &pc);
+    }
+    return gmres_device(h, n, b, phi, m, rtol, atol, maxit, mv, nullptr);
+}
+
+// ---------------------------------------------------------------------------------------------
+//  angular <-> device transfers (FP64 host, FP32 device), chunked through a pinned staging area
+// ---------------------------------------------------------------------------------------------
+static int upload_angular(Handle* h, const double* hs, float* d) {
+    const size_t total = h->psi_elems;
+    const size_t chunk = (size_t)1 << 24;
+    double* stage = nullptr;
+    cudaError_t e = cudaMalloc(&stage, sizeof(double) * std::min(total, chunk));
+    if (e != cudaSuccess) return cuda_fail(h, e, "staging buffer");
+    for (size_t o = 0; o < total; o += chunk) {
+        size_t c = std::min(chunk, total - o);
+        e = cudaMemcpyAsync(stage, hs + o, sizeof(double) * c, cudaMemcpyHostToDevice, h->stream);
+        if (e != cudaSuccess) break;
+        k_f64_to_f32(h, d + o, stage, c);
+        e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) break;
+    }
+    cudaFree(stage);
+    return e == cudaSuccess ? LB_OK : cuda_fail(h, e, "upload angular vector");
+}
+
+static int download_angular(Handle* h, const float* d, double* hs) {
+    const size_t total = h->psi_elems;
+    const size_t chunk = (size_t)1 << 24;
+    double* stage = nullptr;
+    cudaError_t e = cudaMalloc(&stage, sizeof(double) * std::min(total, chunk));
+    if (e != cudaSuccess) return cuda_fail(h, e, "staging buffer");
+    for (size_t o = 0; o < total; o += chunk) {
+        size_t c = std::min(chunk, total - o);
+        k_f32_to_f64(h, stage, d + o, c);
+        e = cudaMemcpyAsync(hs + o, stage, sizeof(double) * c, cudaMemcpyDeviceToHost, h->stream);
+        if (e != cudaSuccess) break;
+        e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) break;
+    }
+    cudaFree(stage);
+    return e == cudaSuccess ? LB_OK : cuda_fail(h, e, "download angular vector");
+}
+
+}  // namespace lb
+
+using namespace lb;
+struct lb_handle : public lb::Handle {};
+
+extern "C" {
+
+int lb_transport_inv(lb_handle* h, double* s) {
+    if (!h || !s) return LB_ERR_ARG;
+    int rc = need_ready(h, false);
+    if (rc) return rc;
+    if (h->sigt.empty()) return fail(h, LB_ERR_STATE, "lb_transport_inv: cross sections not set");
+    cudaSetDevice(h->device);
+    if ((rc = upload_angular(h, s, h->d_psi))) return rc;
+    if ((rc = launch_sweep(h, h->d_psi))) return rc;
+    return download_angular(h, h->d_psi, s);
+}
+
+int lb_scatter_apply(lb_handle* h, double* x) {
+    if (!h || !x) return LB_ERR_ARG;
+    int rc = need_ready(h);
+    if (rc) return rc;
+    cudaSetDevice(h->device);
+    if ((rc = ensure_krylov(h, std::max(h->kry_m, 1), false))) return rc;
+    if ((rc = upload_angular(h, x, h->d_psi))) return rc;
+    if ((rc = launch_d2m(h, h->d_psi, nullptr, 0.0, 1.0, h->d_t))) return rc;
+    if ((rc = launch_m2d(h, h->d_t, h->d_sigl, nullptr, nullptr, h->d_psi))) return rc;
+    return download_angular(h, h->d_psi, x);
+}
+
+int lb_boltzmann_matvec(lb_handle* h, double* x) {
+    if (!h || !x) return LB_ERR_ARG;
+    int rc = need_ready(h);
+    if (rc) return rc;
+    cudaSetDevice(h->device);
+    if ((rc = ensure_krylov(h, std::max(h->kry_m, 1), false))) return rc;
+    if ((rc = upload_angular(h, x, h->d_psi))) return rc;
+    if ((rc = launch_d2m(h, h->d_psi, nullptr, 0.0, 1.0, h->d_t))) return rc;
+    if ((rc = launch_m2d(h, h->d_t, h->d_sigl, nullptr, nullptr, h->d_psi))) return rc;
+    if ((rc = launch_sweep(h, h->d_psi))) return rc;
+    std::vector<double> y(h->psi_elems);
+    if ((rc = download_angular(h, h->d_psi, y.data()))) return rc;
+#pragma omp parallel for schedule(static)
+    for (size_t q = 0; q < y.size(); ++q) x[q] = x[q] - y[q];
+    return LB_OK;
+}
+
+int lb_boltzmann_solve(lb_handle* h, double* s, int solver, int m, double rtol, double atol, int maxit, int* iters,
+                       double* resid) {
+    if (!h || !s) return LB_ERR_ARG;
+    int rc = need_ready(h);
+    if (rc) return rc;
+    if (solver < 0 || solver > 2) return fail(h, LB_ERR_ARG, "unknown solver");
+    if (m < 1) m = 10;
+    if (m > 30) return fail(h, LB_ERR_ARG, "restart length must be <= 30");
+    cudaSetDevice(h->device);
+    if ((rc = ensure_krylov(h, m, solver == LB_SOLVER_FGMRES_ML))) return rc;
+    if (!h->d_qext) {
+        cudaError_t e = cudaMalloc(&h->d_qext, sizeof(float) * h->psi_elems);
+        if (e != cudaSuccess) return cuda_fail(h, e, "angular source buffer");
+    }
+    if ((rc = upload_angular(h, s, h->d_qext))) return rc;
+    const size_t n = h->kry_n;
+    // b = D T^{-1} q
+    if ((rc = apply_transport_moments(h, nullptr, nullptr, nullptr, h->d_qext, h->d_b))) return rc;
+    k_copy(h, h->d_x, h->d_b, n);   // initial guess: the first-flight moments
+    KrylovResult kr = moment_solve(h, h->d_b, h->d_x, solver, m, rtol, atol, maxit, h->d_sigl);
+    if (iters) *iters = kr.nmv;
+    if (resid) *resid = kr.resid;
+    if (kr.status) return kr.status;
+    // psi = T^{-1} (M Sigma phi + q)
+    if ((rc = launch_m2d(h, h->d_x, h->d_sigl, nullptr, h->d_qext, h->d_psi))) return rc;
+    if ((rc = launch_sweep(h, h->d_psi))) return rc;
+    return download_angular(h, h->d_psi, s);
+}
+
+int lb_mg_set_problem(lb_handle* h, int G, int Ls, const double* sigt, const double* sigs, const double* dd,
+                      const double* unc, const double* beam_dir) {
+    if (!h || G < 1 || !sigt || !sigs || !dd) return LB_ERR_ARG;
+    if (h->device < 0) return fail(h, LB_ERR_STATE, "host-only handle: no device attached");
+    if (!h->mesh_ready || !h->angle_ready) return fail(h, LB_ERR_STATE, "lb_mg_set_problem: mesh/quadrature not set");
+    cudaSetDevice(h->device);
+    const int Nm = h->Nm;
+    h->G = G;
+    h->mg_sigt.assign(sigt, sigt + (size_t)G * Nm);
+    h->mg_sigs.assign(sigs, sigs + (size_t)G * G * Nm * (Ls + 1));
+    h->mg_dd.assign(dd, dd + (size_t)G * Nm);
+    h->beam_dir.assign(3, 0.0);
+    if (beam_dir) h->beam_dir.assign(beam_dir, beam_dir + 3);
+    // within-group XS of group 0 sets nm / the Y planes
+    int rc = lb_set_xs(h, Ls, sigt, sigs);
+    if (rc) return rc;
+    const int nm = h->nm, nmpad = h->nmpad;
+    // transfer tables sigma_l(j) for every (g', g) pair: [G][G][Nm][nmpad]
+    std::vector<float> tab((size_t)G * G * Nm * nmpad, 0.f);
+    for (int gp = 0; gp < G; ++gp)
+        for (int g = 0; g < G; ++g)
+            for (int m = 0; m < Nm; ++m)
+                for (int l = 0; l <= Ls; ++l)
+                    for (int j = l * l; j < (l + 1) * (l + 1); ++j)
+                        tab[(((size_t)gp * G + g) * Nm + m) * nmpad + j] =
+                            (float)sigs[(((size_t)gp * G + g) * Nm + m) * (Ls + 1) + l];
+    if (h->d_sigl_mg) cudaFree(h->d_sigl_mg);
+    cudaError_t e = cudaMalloc(&h->d_sigl_mg, sizeof(float) * tab.size());
+    if (e != cudaSuccess) return cuda_fail(h, e, "transfer tables");
+    cudaMemcpy(h->d_sigl_mg, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice);
+    const size_t NENK = (size_t)h->NENK;
+    auto realloc = [&](double** p, size_t cnt, const char* what) -> int {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+        cudaError_t ee = cudaMalloc(p, sizeof(double) * cnt);
+        return ee == cudaSuccess ? LB_OK : cuda_fail(h, ee, what);
+    };
+    if ((rc = realloc(&h->d_unc, NENK, "uncollided flux"))) return rc;
+    if ((rc = realloc(&h->d_phi_all, (size_t)G * nm * NENK, "group flux moments"))) return rc;
+    if ((rc = realloc(&h->d_src, (size_t)nm * NENK, "group source"))) return rc;
+    if ((rc = realloc(&h->d_dose, NENK, "dose"))) return rc;
+    if ((rc = realloc(&h->d_flux, (size_t)G * NENK, "group fluence"))) return rc;
+    if (unc) cudaMemcpy(h->d_unc, unc, sizeof(double) * NENK, cudaMemcpyHostToDevice);
+    else cudaMemset(h->d_unc, 0, sizeof(double) * NENK);
+    return LB_OK;
+}
+
+int lb_mg_solve(lb_handle* h, int solver, int m, double rtol, double atol, int maxit, int* iters) {
+    if (!h || h->device < 0 || h->G < 1 || !h->d_phi_all) return h ? fail(h, LB_ERR_STATE, "lb_mg_solve: problem not set") : LB_ERR_ARG;
+    if (solver < 0 || solver > 2) return fail(h, LB_ERR_ARG, "unknown solver");
+    if (m < 1) m = 10;
+    if (m > 30) return fail(h, LB_ERR_ARG, "restart length must be <= 30");
+    cudaSetDevice(h->device);
+    const int G = h->G, Nm = h->Nm, Ls = h->Ls;
+    int rc = ensure_krylov(h, m, solver == LB_SOLVER_FGMRES_ML);
+    if (rc) return rc;
+    const int nm = h->nm, nmpad = h->nmpad;
+    const size_t NENK = (size_t)h->NENK, n = h->kry_n;
+    // beam direction harmonics Y_j(Omega_b)
+    std::vector<double> yb(nm);
+    real_sh(Ls, h->beam_dir.data(), yb.data());
+    double* d_yb = nullptr;
+    double* d_dd = nullptr;
+    cudaMalloc(&d_yb, sizeof(double) * nm);
+    cudaMalloc(&d_dd, sizeof(double) * Nm);
+    cudaMemcpyAsync(d_yb, yb.data(), sizeof(double) * nm, cudaMemcpyHostToDevice, h->stream);
+    cudaMemsetAsync(h->d_dose, 0, sizeof(double) * NENK, h->stream);
+    auto table = [&](int gp, int g) { return h->d_sigl_mg + (((size_t)gp * G + g) * Nm) * nmpad; };
+    for (int g = 0; g < G; ++g) {
+        // group source: downscatter of every solved group + first collision of the beam
+        cudaMemsetAsync(h->d_src, 0, sizeof(double) * n, h->stream);
+        for (int gp = 0; gp < g; ++gp)
+            k_moment_source(h, h->d_src, h->d_phi_all + (size_t)gp * n, table(gp, g), h->d_mat, (long long)NENK, nm, nmpad, 1);
+        k_unc_source(h, h->d_src, h->d_unc, d_yb, table(0, g), h->d_mat, (long long)NENK, nm, nmpad);
+        // within-group operator of group g
+        std::vector<double> st(h->mg_sigt.begin() + (size_t)g * Nm, h->mg_sigt.begin() + (size_t)(g + 1) * Nm);
+        std::vector<double> ss((size_t)Nm * (Ls + 1));
+        for (int mm = 0; mm < Nm; ++mm)
+            for (int l = 0; l <= Ls; ++l)
+                ss[(size_t)mm * (Ls + 1) + l] = h->mg_sigs[(((size_t)g * G + g) * Nm + mm) * (Ls + 1) + l];
+        if ((rc = lb_set_xs(h, Ls, st.data(), ss.data()))) break;
+        // b = D T^{-1} M src
+        if ((rc = apply_transport_moments(h, nullptr, nullptr, h->d_src, nullptr, h->d_b))) break;
+        double* phi = h->d_phi_all + (size_t)g * n;
+        k_copy(h, phi, h->d_b, n);
+        KrylovResult kr = moment_solve(h, h->d_b, phi, solver, m, rtol, atol, maxit, table(g, g));
+        if (iters) iters[g] = kr.nmv;
+        if ((rc = kr.status)) break;
+        cudaMemcpyAsync(d_dd, h->mg_dd.data() + (size_t)g * Nm, sizeof(double) * Nm, cudaMemcpyHostToDevice, h->stream);
+        k_dose_tally(h, phi, h->d_unc, g == 0 ? 1.0 : 0.0, d_dd, h->d_mat, h->d_flux + (size_t)g * NENK, h->d_dose,
+                     (long long)NENK);
+        cudaStreamSynchronize(h->stream);
+    }
+    cudaStreamSynchronize(h->stream);
+    cudaFree(d_yb);
+    cudaFree(d_dd);
+    return rc;
+}
+
+int lb_mg_get_results(lb_handle* h, double* flux, double* dose) {
+    if (!h || h->device < 0 || !h->d_dose) return LB_ERR_STATE;
+    cudaSetDevice(h->device);
+    cudaError_t e = cudaSuccess;
+    if (flux) e = cudaMemcpy(flux, h->d_flux, sizeof(double) * (size_t)h->G * h->NENK, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && dose) e = cudaMemcpy(dose, h->d_dose, sizeof(double) * (size_t)h->NENK, cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? LB_OK : cuda_fail(h, e, "read results");
+}
+
+}  // extern "C"

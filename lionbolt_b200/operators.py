@@ -1,0 +1,191 @@
+"""Python mirror of the reference's operator API (src/LionboltAPI.f90 re-exports).
+
+    TransportOp   T   Build(mesh, angular, XS) / MatInv(s)            TransportOperator.f90
+    ScatteringOp  K   Build(mesh, angular, XS) / MatVec(x)            ScatteringOperator.f90
+    BoltzmannOp   L   Build(mesh, angular, XS) / MatVec(x) / MatInv(s) BoltzmannOperator.f90
+    SpaceAngleVector(mesh, angular) with .v and .Fluence(w)            LinearOperatorClass.f90
+
+Vectors are FP64 numpy arrays in the reference layout v[i*NENK + 4e + k]; operations are in
+place ("enters as source, leaves as solution", TransportAlgebra.f90:44).  Every call goes through
+the C ABI to the CUDA library; errors raise LionboltError (the reference calls stophere).
+"""
+import numpy as np
+
+from . import _lib
+from ._lib import as_f64, as_i32, dptr, iptr
+
+
+class AngularClass:
+    """SN quadrature, SNPrep.f90:39-86: AngularClass(L) gives Ng = L+1, Nc = 2 Ng; (Ng, Nc) may be
+    given explicitly for direction counts the reference's tied construction cannot make."""
+
+    def __init__(self, L=None, solver="GMRES", Ng=None, Nc=None, k=None, w=None):
+        if k is not None:
+            self.k, self.w = as_f64(k), as_f64(w)
+            self.L = L if L is not None else -1
+        else:
+            if Ng is None:
+                Ng = L + 1
+            if Nc is None:
+                Nc = 2 * Ng
+            self.k, self.w = _lib.sn_quadrature(Ng, Nc)
+            self.L = Ng - 1 if L is None else L
+        self.solver = solver
+
+    @property
+    def NI(self):
+        return int(self.k.shape[0])
+
+
+class XSType:
+    """Within-group cross sections: t[Nm] (XS%t) and s[Nm, L+1] (XS%s(0:L, m))."""
+
+    def __init__(self, t, s):
+        self.t = as_f64(np.atleast_1d(t))
+        self.s = as_f64(np.atleast_2d(s))
+
+    @property
+    def L(self):
+        return self.s.shape[1] - 1
+
+
+class SpaceAngleVector:
+    def __init__(self, mesh, angular, v=None):
+        self.NENK = mesh.NENK
+        self.NI = angular.NI
+        self.v = np.zeros(self.NENK * self.NI) if v is None else as_f64(v).copy()
+
+    def Fluence(self, w):
+        """fl = sum_i w_i v_i (LinearOperatorClass.f90:154-174)."""
+        return (np.asarray(w)[:, None] * self.v.reshape(self.NI, self.NENK)).sum(axis=0)
+
+
+class _Op:
+    name = "Operator"
+
+    def __init__(self, device=0):
+        self._h = _lib.Handle(device)
+        self.mesh = None
+        self.angular = None
+        self.XS = None
+
+    def Build(self, mesh, angular=None, XS=None):
+        """Generic Build => Space / SpaceAngle / Physics, as the reference's generic interface."""
+        h = self._h
+        if mesh is not None and mesh is not self.mesh:
+            h.call("lb_set_mesh", mesh.NE, mesh.NN, dptr(as_f64(mesh.rg)), iptr(as_i32(mesh.node)),
+                   iptr(as_i32(mesh.neighbors)), iptr(as_i32(mesh.mat)), int(mesh.Nm))
+            self.mesh = mesh
+            self.angular = None
+        if angular is not None and angular is not self.angular:
+            h.call("lb_set_quadrature", angular.NI, dptr(angular.k), dptr(angular.w))
+            self.angular = angular
+        if XS is not None:
+            self.set_xs(XS)
+        return self
+
+    def set_xs(self, XS):
+        t = as_f64(XS.t)
+        s = as_f64(XS.s)
+        self._h.call("lb_set_xs", int(s.shape[1] - 1), dptr(t), dptr(s))
+        self.XS = XS
+
+    def _vec(self, s):
+        v = s.v if isinstance(s, SpaceAngleVector) else s
+        if not (isinstance(v, np.ndarray) and v.dtype == np.float64 and v.flags.c_contiguous):
+            raise TypeError("vectors must be contiguous float64 numpy arrays")
+        if v.size != self.mesh.NENK * self.angular.NI:
+            raise ValueError("vector size does not match NENK*NI")
+        return v
+
+    def schedule(self):
+        """(sl [NI, NE], upmask [NI, NE], nlevels [NI], level_start [NI, NE+1])"""
+        NE, NI = self.mesh.NE, self.angular.NI
+        sl = np.zeros((NI, NE), dtype=np.int32)
+        up = np.zeros((NI, NE), dtype=np.uint8)
+        nl = np.zeros(NI, dtype=np.int32)
+        ls = np.zeros((NI, NE + 1), dtype=np.int32)
+        self._h.call("lb_get_schedule", iptr(sl), up.ctypes.data_as(_lib._c_ubyte_p), iptr(nl), iptr(ls))
+        return sl, up, nl, ls
+
+    def timers(self):
+        return self._h.timers()
+
+    def Destroy(self):
+        self._h.close()
+
+
+class TransportOp(_Op):
+    name = "Transport Operator"
+
+    def MatInv(self, s):
+        """s <- T^{-1} s (TransportOperator.f90:72-151)."""
+        self._h.call("lb_transport_inv", dptr(self._vec(s)))
+        return s
+
+    def MatVec(self, x):
+        raise _lib.LionboltError(_lib.LB_ERR_STATE,
+                                 "TransportOp%MatVec was called, but the operator has yet to be implemented.")
+
+
+class ScatteringOp(_Op):
+    name = "Scattering Operator"
+
+    def MatVec(self, x):
+        """x <- K x (ScatteringOperator.f90:39-70)."""
+        self._h.call("lb_scatter_apply", dptr(self._vec(x)))
+        return x
+
+    def MatInv(self, s):
+        raise _lib.LionboltError(_lib.LB_ERR_STATE, "ScatteringOp%MatInv was called, but this operation is undefined.")
+
+
+class BoltzmannOp(_Op):
+    name = "Boltzmann Operator"
+    _SOLVERS = {"SI": _lib.SOLVER_SI, "GMRES": _lib.SOLVER_GMRES, "FGMRES_ML": _lib.SOLVER_FGMRES_ML}
+
+    def __init__(self, device=0, m=10, rtol=1e-8, atol=1e-12, maxit=0):
+        super().__init__(device)
+        self.m, self.rtol, self.atol, self.maxit = m, rtol, atol, maxit
+        self.iters = 0
+        self.resid = 0.0
+
+    def MatVec(self, x):
+        """x <- x - T^{-1} K x (BoltzmannOperator.f90:59-104)."""
+        self._h.call("lb_boltzmann_matvec", dptr(self._vec(x)))
+        return x
+
+    def MatInv(self, s, solver=None):
+        """s <- L^{-1} s (BoltzmannOperator.f90:106-151).  Default solver: angular%solver."""
+        solver = solver or (self.angular.solver if self.angular is not None else "GMRES")
+        it = np.zeros(1, dtype=np.int32)
+        rs = np.zeros(1)
+        self._h.call("lb_boltzmann_solve", dptr(self._vec(s)), self._SOLVERS[solver], int(self.m), float(self.rtol),
+                     float(self.atol), int(self.maxit), iptr(it), dptr(rs))
+        self.iters, self.resid = int(it[0]), float(rs[0])
+        return s
+
+
+class MultigroupSolver(_Op):
+    """Group loop of Main.f90:326-476 with the dose tally (CalculateDeposition, Main.f90:750-824)."""
+
+    name = "Multigroup solve"
+
+    def set_problem(self, prob):
+        self.Build(prob.mesh, AngularClass(k=prob.k, w=prob.w))
+        self.prob = prob
+        self._h.call("lb_mg_set_problem", int(prob.G), int(prob.Ls), dptr(as_f64(prob.sigt)), dptr(as_f64(prob.sigs)),
+                     dptr(as_f64(prob.dd)), dptr(as_f64(prob.unc)), dptr(as_f64(prob.beam_dir)))
+        return self
+
+    def solve(self, solver="GMRES", m=20, rtol=1e-6, atol=0.0, maxit=0):
+        it = np.zeros(self.prob.G, dtype=np.int32)
+        self._h.call("lb_mg_solve", BoltzmannOp._SOLVERS[solver], int(m), float(rtol), float(atol), int(maxit), iptr(it))
+        return it
+
+    def results(self):
+        G, NENK = self.prob.G, self.mesh.NENK
+        flux = np.zeros((G, NENK))
+        dose = np.zeros(NENK)
+        self._h.call("lb_mg_get_results", dptr(flux), dptr(dose))
+        return flux, dose

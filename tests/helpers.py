@@ -1,0 +1,71 @@
+"""Shared helpers for the parity tests (the oracle is the checker, never the product)."""
+import decimal
+import fractions
+import os
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64).ravel()
+    b = np.asarray(b, dtype=np.float64).ravel()
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def golden(name):
+    return np.loadtxt(os.path.join(GOLDEN, name))
+
+
+def scatter_moment(n):
+    """XS%s(n) of the reference's ScatterMMS driver (validation/operators/ScatterMMS.f90:91-128):
+    2 pi (S1 e - S2 (-1)^n / e), zero for n >= 14, evaluated in extended precision."""
+    if n >= 14:
+        return 0.0
+    S1 = fractions.Fraction(0)
+    S2 = fractions.Fraction(0)
+    tmp = fractions.Fraction(1)
+    for m in range(n + 1):
+        S1 += tmp * (-1) ** m
+        S2 += tmp
+        if m == n:
+            break
+        tmp = tmp * (n + m + 1) * (n - m) / (2 * (m + 1))
+    with decimal.localcontext() as ctx:
+        ctx.prec = 50
+        e = decimal.Decimal(1).exp()
+        d1 = decimal.Decimal(S1.numerator) / decimal.Decimal(S1.denominator)
+        d2 = decimal.Decimal(S2.numerator) / decimal.Decimal(S2.denominator)
+        f = d1 * e - d2 * (-1) ** n / e
+    return 2.0 * np.pi * float(f)
+
+
+def scatter_mms(mesh, k):
+    """Input psi = exp(r.k) and exact K psi = 2 pi (e^t - e^-t)/t, t = |r + k| (ScatterMMS.f90:51-70)."""
+    r = mesh.node_coords()                      # [NENK, 3]
+    psi = np.exp(k @ r.T)                       # [NI, NENK]
+    t = np.linalg.norm(r[None, :, :] + k[:, None, :], axis=2)
+    exact = np.where(t == 0, 4 * np.pi, 2 * np.pi * (np.exp(t) - np.exp(-t)) / np.where(t == 0, 1, t))
+    return psi.ravel(), exact.ravel()
+
+
+def transport_mms(mesh, k, sigma=1e-10, A=10.0):
+    """Source (-2A k.r + sigma) exp(-A r^2) and exact exp(-A r^2) (TransportMMS.f90:62-77)."""
+    r = mesh.node_coords()
+    g = np.exp(-A * (r * r).sum(axis=1))
+    src = (-2 * A * (k @ r.T) + sigma) * g[None, :]
+    exact = np.broadcast_to(g[None, :], src.shape)
+    return src.ravel(), np.ascontiguousarray(exact).ravel()
+
+
+def jittered(mesh, amount, seed=1):
+    """Copy of a box mesh with interior nodes moved randomly (general face normals)."""
+    rg = mesh.rg.copy()
+    lo, hi = rg.min(axis=0), rg.max(axis=0)
+    interior = np.all((rg > lo + 1e-12) & (rg < hi - 1e-12), axis=1)
+    rng = np.random.default_rng(seed)
+    rg[interior] += amount * rng.uniform(-1, 1, size=(interior.sum(), 3))
+    from lionbolt_b200.mesh import Mesh
+    return Mesh(rg=rg, node=mesh.node.copy(), neighbors=mesh.neighbors.copy(), mat=mesh.mat.copy(), Nm=mesh.Nm,
+                shape=mesh.shape)

@@ -1,0 +1,172 @@
+"""GPU parity: the CUDA path through the C ABI against the FP64 oracle on the same seeded inputs.
+
+Tolerances: the sweep and the moment contractions run in FP32 (split-BF16 tensor-core products
+reproduce FP32), the Krylov iteration in FP64.  Results must agree with the FP64 oracle to
+1e-5 relative L2 (the target stated for scalar flux and dose)."""
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import jittered, rel_l2, scatter_mms, scatter_moment, transport_mms
+from lionbolt_b200 import AngularClass, BoltzmannOp, MultigroupSolver, ScatteringOp, TransportOp, XSType
+from lionbolt_b200 import _lib
+from lionbolt_b200 import mesh as M
+from lionbolt_b200 import problems as P
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def _pair(m, k, w, sigt, sigs, L=None):
+    """(oracle, product TransportOp/ScatteringOp/BoltzmannOp builder) on the same inputs."""
+    L = sigs.shape[1] - 1 if L is None else L
+    o = O.Oracle(m)
+    assert o.set_angular(k, w, L) == 0
+    o.set_xs(sigt, sigs)
+    ang = AngularClass(k=k, w=w)
+    xs = XSType(sigt, sigs)
+    return o, ang, xs
+
+
+SWEEP_CASES = {
+    "one_hex": lambda: (M.box_mesh(1, 1, 1), P.quadrature(2, 4), np.array([1.0]), np.zeros((1, 1))),
+    "cube_2x2x2": lambda: (M.box_mesh(2, 2, 2, (0, 0, 0), (1, 1, 1)), P.quadrature(4, 8), np.array([0.7]),
+                           np.zeros((1, 1))),
+    "config0": lambda: (P.config0().mesh, P.quadrature(8, 10), np.array([0.2]), np.zeros((1, 1))),
+    "two_material": lambda: (P.config1_small(n=(6, 6, 12)).mesh, P.quadrature(6, 12), np.array([0.05, 0.135]),
+                             np.zeros((2, 1))),
+    "jittered": lambda: (jittered(M.box_mesh(6, 5, 4, (0, 0, 0), (3.0, 2.5, 2.0)), 0.07), P.quadrature(4, 8),
+                         np.array([1.3]), np.zeros((1, 1))),
+    "thin_air": lambda: (M.box_mesh(4, 4, 4, (0, 0, 0), (2, 2, 2)), P.quadrature(4, 8), np.array([1e-6]),
+                         np.zeros((1, 1))),
+}
+
+
+@pytest.mark.parametrize("case", sorted(SWEEP_CASES))
+def test_transport_inverse_matches_oracle(case):
+    m, (k, w), sigt, sigs = SWEEP_CASES[case]()
+    o, ang, xs = _pair(m, k, w, sigt, sigs)
+    T = TransportOp().Build(m, ang, xs)
+    rng = np.random.default_rng(7)
+    q = rng.uniform(0.0, 1.0, size=m.NENK * k.shape[0])
+    ref = o.transport_inv(q)
+    out = q.copy()
+    T.MatInv(out)
+    assert rel_l2(out, ref) < TOL
+    # the GPU path is the one that ran
+    assert T.timers()["sweep"][1] >= 1
+
+
+def test_transport_mms_matches_oracle():
+    m = M.box_mesh(6, 6, 6, (-1, -1, -1), (1, 1, 1))
+    k, w = P.quadrature(4, 8)
+    o, ang, xs = _pair(m, k, w, np.array([1e-10]), np.zeros((1, 1)))
+    src, exact = transport_mms(m, k)
+    ref = o.transport_inv(src)
+    out = src.copy()
+    TransportOp().Build(m, ang, xs).MatInv(out)
+    assert rel_l2(out, ref) < TOL
+    assert abs(rel_l2(out, exact) - rel_l2(ref, exact)) < 1e-4
+
+
+def test_transport_is_linear_and_zero_preserving():
+    m = M.box_mesh(5, 5, 5, (0, 0, 0), (2, 2, 2))
+    k, w = P.quadrature(4, 8)
+    T = TransportOp().Build(m, AngularClass(k=k, w=w), XSType([0.4], np.zeros((1, 1))))
+    z = np.zeros(m.NENK * k.shape[0])
+    T.MatInv(z)
+    assert not np.any(z)
+    rng = np.random.default_rng(11)
+    a, b = rng.uniform(size=z.size), rng.uniform(size=z.size)
+    ta, tb, tab = a.copy(), b.copy(), (2 * a - 3 * b)
+    T.MatInv(ta)
+    T.MatInv(tb)
+    T.MatInv(tab)
+    assert rel_l2(tab, 2 * ta - 3 * tb) < 1e-5
+
+
+@pytest.mark.parametrize("nmat", [1, 2])
+def test_scattering_matches_oracle(nmat):
+    """Nm = 1 follows the reference's dgemm path, Nm > 1 its per-node dgemv loop."""
+    if nmat == 1:
+        m = M.box_mesh(3, 3, 3, (0, 0, 0), (1, 1, 1))
+        sigt, sigs = np.array([0.5]), np.array([[0.45 * 0.8 ** l for l in range(6)]])
+    else:
+        m = P.config1_small(n=(3, 3, 6)).mesh
+        sigt = np.array([0.3, 0.81])
+        sigs = np.array([[0.27 * 0.7 ** l for l in range(6)], [0.6 * 0.9 ** l for l in range(6)]])
+    k, w = P.quadrature(6, 12)
+    o, ang, xs = _pair(m, k, w, sigt, sigs, L=5)
+    rng = np.random.default_rng(5)
+    x = rng.normal(size=m.NENK * k.shape[0])
+    ref = o.scatter_apply(x)
+    out = x.copy()
+    ScatteringOp().Build(m, ang, xs).MatVec(out)
+    assert rel_l2(out, ref) < TOL
+
+
+def test_scatter_mms_known_answer_on_gpu():
+    m = M.box_mesh(2, 2, 2, (-1, -1, -1), (1, 1, 1))
+    L = 15
+    k, w = P.quadrature(L + 1, 2 * (L + 1))
+    s = np.array([[scatter_moment(l) for l in range(L + 1)]])
+    K = ScatteringOp().Build(m, AngularClass(k=k, w=w), XSType([1.0], s))
+    psi, exact = scatter_mms(m, k)
+    out = psi.copy()
+    K.MatVec(out)
+    assert rel_l2(out, exact) < 2e-5
+
+
+@pytest.mark.parametrize("solver", ["GMRES", "SI"])
+def test_boltzmann_solve_matches_oracle(solver):
+    prob = P.config0()
+    m = prob.mesh
+    o, ang, xs = _pair(m, prob.k, prob.w, prob.sigt[0], prob.sigs[0, 0])
+    rng = np.random.default_rng(2)
+    q = rng.uniform(0, 1, size=m.NENK * prob.NI)
+    ref, info = o.boltzmann_solve(q, "GMRES", m=20, rtol=1e-11)
+    assert info["status"] == 0
+    L = BoltzmannOp(m=20, rtol=1e-8, atol=0.0).Build(m, ang, xs)
+    out = q.copy()
+    L.MatInv(out, solver=solver)
+    assert L.iters > 1
+    assert rel_l2(out, ref) < TOL
+    fl, flr = o.fluence(out), o.fluence(ref)
+    assert rel_l2(fl, flr) < TOL
+
+
+def test_boltzmann_matvec_matches_oracle():
+    m = M.box_mesh(3, 3, 3, (0, 0, 0), (3, 3, 3))
+    k, w = P.quadrature(4, 8)
+    sigt, sigs = np.array([0.6]), np.array([[0.5, 0.3, 0.1, 0.02]])
+    o, ang, xs = _pair(m, k, w, sigt, sigs)
+    x = np.random.default_rng(9).normal(size=m.NENK * k.shape[0])
+    ref = o.boltzmann_matvec(x)
+    out = x.copy()
+    BoltzmannOp().Build(m, ang, xs).MatVec(out)
+    assert rel_l2(out, ref) < TOL
+
+
+def test_multigroup_flux_and_dose_match_oracle():
+    prob = P.config1_small(n=(6, 6, 12), G=4, Ng=6, Nc=12)
+    o = O.Oracle(prob.mesh)
+    assert o.set_angular(prob.k, prob.w, prob.Ls) == 0
+    flux_ref, dose_ref, it_ref = o.multigroup(prob, "GMRES", m=20, rtol=1e-11)
+    mg = MultigroupSolver().set_problem(prob)
+    it = mg.solve("GMRES", m=20, rtol=1e-8)
+    flux, dose = mg.results()
+    assert np.all(it > 0)
+    assert rel_l2(dose, dose_ref) < TOL
+    for g in range(prob.G):
+        assert rel_l2(flux[g], flux_ref[g]) < TOL, g
+
+
+def test_gmres_iteration_limit_reports_noconv():
+    prob = P.config0()
+    L = BoltzmannOp(m=5, rtol=1e-14, atol=0.0, maxit=3).Build(prob.mesh, AngularClass(k=prob.k, w=prob.w),
+                                                              XSType(prob.sigt[0], prob.sigs[0, 0]))
+    q = np.ones(prob.mesh.NENK * prob.NI)
+    with pytest.raises(_lib.LionboltError) as ei:
+        L.MatInv(q)
+    assert ei.value.status == _lib.LB_ERR_NOCONV

@@ -1,0 +1,189 @@
+"""Host logic of the product library on CPU: exported C ABI, quadrature, and the sweep schedule
+(bit-exact against the oracle's literal restatement of SweepOrder.f90 / SweepArrays.f90).
+These tests use host-only handles (lb_create(-1)): no GPU, no kernel launches."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import golden, jittered
+from lionbolt_b200 import _lib
+from lionbolt_b200 import mesh as M
+from lionbolt_b200 import problems as P
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "lionbolt_b200.h")
+
+
+def header_symbols():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(lb_\w+)\s*\(", txt, flags=re.M)))
+
+
+def test_library_exports_every_header_symbol():
+    lib = _lib.load()
+    syms = header_symbols()
+    assert len(syms) >= 20
+    for s in syms:
+        assert hasattr(lib, s), s
+        assert s in _lib.SIGNATURES, f"{s} missing from the ctypes signature table"
+
+
+def test_status_strings():
+    lib = _lib.load()
+    assert lib.lb_status_string(0) == b"ok"
+    assert b"stagnant" in lib.lb_status_string(_lib.LB_ERR_CYCLE)
+
+
+@pytest.mark.parametrize("L,fname", [(11, "ordinates_L11.txt"), (7, "ordinates_L7.txt")])
+def test_product_quadrature_matches_reference_log(L, fname):
+    k, w = _lib.sn_quadrature(L + 1, 2 * (L + 1))
+    assert np.abs(k - golden(fname)).max() < 2.5e-16
+    assert abs(w.sum() - 4 * np.pi) < 1e-13
+
+
+class HostHandle:
+    def __init__(self):
+        self.lib = _lib.load()
+        self.h = ctypes.c_void_p()
+        assert self.lib.lb_create(-1, ctypes.byref(self.h)) == 0
+
+    def mesh(self, m):
+        return self.lib.lb_set_mesh(self.h, m.NE, m.NN, _lib.dptr(_lib.as_f64(m.rg)), _lib.iptr(_lib.as_i32(m.node)),
+                                    _lib.iptr(_lib.as_i32(m.neighbors)), _lib.iptr(_lib.as_i32(m.mat)), int(m.Nm))
+
+    def quad(self, k, w):
+        return self.lib.lb_set_quadrature(self.h, k.shape[0], _lib.dptr(_lib.as_f64(k)), _lib.dptr(_lib.as_f64(w)))
+
+    def schedule(self, NE, NI):
+        sl = np.zeros((NI, NE), np.int32)
+        up = np.zeros((NI, NE), np.uint8)
+        nl = np.zeros(NI, np.int32)
+        ls = np.zeros((NI, NE + 1), np.int32)
+        assert self.lib.lb_get_schedule(self.h, _lib.iptr(sl), up.ctypes.data_as(_lib._c_ubyte_p), _lib.iptr(nl),
+                                        _lib.iptr(ls)) == 0
+        return sl, up, nl, ls
+
+    def error(self):
+        buf = ctypes.create_string_buffer(256)
+        self.lib.lb_last_error(self.h, buf, 256)
+        return buf.value.decode()
+
+    def __del__(self):
+        self.lib.lb_destroy(self.h)
+
+
+def reference_arrays_from_product(sl, up, m):
+    """Derive SweepArrays.f90 arrays (UFoffset, upfaces, ipsf) from the product's schedule."""
+    NI, NE = sl.shape
+    isl = np.empty_like(sl)
+    for i in range(NI):
+        isl[i, sl[i]] = np.arange(NE)
+    upf, ipsf, UF = [], [], np.zeros((NI, NE + 1), np.int64)
+    j = 0
+    for i in range(NI):
+        for es in range(NE):
+            e = sl[i, es]
+            UF[i, es] = j
+            for f in range(4):
+                if (up[i, es] >> f) & 1:
+                    upf.append(f)
+                    ep = m.neighbors[e, f]
+                    ipsf.append(i * 4 * NE + 4 * isl[i, ep])
+                    j += 1
+        UF[i, NE] = j
+    return isl, np.array(upf, np.int32), np.array(ipsf, np.int64), UF
+
+
+CASES = {
+    "config0": lambda: (P.config0().mesh, P.quadrature(8, 10)),
+    "two_material": lambda: (P.config1_small(n=(4, 4, 8)).mesh, P.quadrature(6, 12)),
+    "jittered": lambda: (jittered(M.box_mesh(5, 4, 3, (0, 0, 0), (2.5, 2.0, 1.5)), 0.06), P.quadrature(4, 8)),
+    "L11_288": lambda: (M.box_mesh(3, 3, 6, (0, 0, 0), (1.5, 1.5, 3.0)), P.quadrature(12, 24)),
+}
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_schedule_bitexact_vs_literal_sweep_order(case):
+    m, (k, w) = CASES[case]()
+    o = O.Oracle(m)
+    assert o.set_angular(k, w, 0, literal=True) == 0
+    ref = o.schedule()
+    hh = HostHandle()
+    assert hh.mesh(m) == 0, hh.error()
+    assert hh.quad(k, w) == 0, hh.error()
+    sl, up, nl, ls = hh.schedule(m.NE, k.shape[0])
+    assert np.array_equal(sl, ref["sl"])
+    assert np.array_equal(nl, ref["nlevels"])
+    isl, upf, ipsf, UF = reference_arrays_from_product(sl, up, m)
+    assert np.array_equal(isl, ref["isl"])
+    assert np.array_equal(upf, ref["upfaces"])
+    assert np.array_equal(ipsf, ref["ipsf"])
+    assert np.array_equal(UF, ref["UFoffset"])
+    # level starts: contiguous, ascending element ids inside every level
+    for i in range(0, k.shape[0], max(1, k.shape[0] // 7)):
+        st = ls[i, :nl[i] + 1]
+        assert st[0] == 0 and st[-1] == m.NE
+        for a, b in zip(st[:-1], st[1:]):
+            assert np.all(np.diff(sl[i, a:b]) > 0)
+
+
+def test_empty_and_invalid_meshes_are_rejected():
+    hh = HostHandle()
+    lib = hh.lib
+    z = np.zeros(12)
+    zi = np.zeros(4, np.int32)
+    assert lib.lb_set_mesh(hh.h, 0, 4, _lib.dptr(z), _lib.iptr(zi), _lib.iptr(zi), _lib.iptr(zi), 1) == _lib.LB_ERR_ARG
+    m = M.box_mesh(1, 1, 1)
+    bad = m.node.copy()
+    bad[0, 0] = m.NN + 5
+    assert lib.lb_set_mesh(hh.h, m.NE, m.NN, _lib.dptr(_lib.as_f64(m.rg)), _lib.iptr(_lib.as_i32(bad)),
+                           _lib.iptr(_lib.as_i32(m.neighbors)), _lib.iptr(_lib.as_i32(m.mat)), 1) == _lib.LB_ERR_ARG
+    # quadrature before a mesh: operator not ready
+    hh2 = HostHandle()
+    k, w = P.quadrature(2, 4)
+    assert hh2.quad(k, w) == _lib.LB_ERR_STATE
+    # non-conforming neighbour table
+    nb = m.neighbors.copy()
+    nb[0, :] = -1
+    m2 = M.Mesh(rg=m.rg, node=m.node, neighbors=nb, mat=m.mat, Nm=1)
+    assert hh.mesh(m2) == _lib.LB_ERR_ARG
+
+
+def test_folded_mesh_cycle_is_reported():
+    """Two tets on the same side of their shared face both see it as an inflow face for some
+    direction: the level loop stagnates, which the reference reports as 'Sweep is stagnant'."""
+    rg = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0.2, 0.2, 1.0], [0.3, 0.25, 0.5]], dtype=np.float64)
+    node = np.array([[0, 1, 2, 3], [0, 2, 1, 4]], dtype=np.int32)   # both apexes above the z=0 face
+    nb = np.array([[1, -1, -1, -1], [1 * 0, -1, -1, -1]], dtype=np.int32)
+    nb[1, 0] = 0
+    m = M.Mesh(rg=rg, node=node, neighbors=nb, mat=np.zeros(2, np.int32), Nm=1)
+    hh = HostHandle()
+    assert hh.mesh(m) == 0, hh.error()
+    k = np.array([[0.0, 0.0, 1.0]])
+    w = np.array([4 * np.pi])
+    assert hh.quad(k, w) == _lib.LB_ERR_CYCLE
+    assert "stagnant" in hh.error()
+
+
+def test_host_only_handle_refuses_compute():
+    m = M.box_mesh(1, 1, 1)
+    hh = HostHandle()
+    assert hh.mesh(m) == 0
+    k, w = P.quadrature(2, 4)
+    assert hh.quad(k, w) == 0
+    s = np.zeros(m.NENK * k.shape[0])
+    assert hh.lib.lb_transport_inv(hh.h, _lib.dptr(s)) == _lib.LB_ERR_STATE
+
+
+def test_nan_cross_section_rejected():
+    m = M.box_mesh(1, 1, 1)
+    hh = HostHandle()
+    hh.mesh(m)
+    k, w = P.quadrature(2, 4)
+    hh.quad(k, w)
+    st = np.array([np.nan])
+    ss = np.zeros((1, 2))
+    assert hh.lib.lb_set_xs(hh.h, 1, _lib.dptr(st), _lib.dptr(ss)) == _lib.LB_ERR_NAN
