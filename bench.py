@@ -1,0 +1,348 @@
+#!/usr/bin/env python
+"""Benchmark: time-to-dose of the multigroup transport solve on B200, and the CPU baseline.
+
+Workload (one step): the full multigroup dose solve of the 768,000-tet box (40 x 40 x 80 hexes,
+20 x 20 x 40 cm, 288 directions, 20 groups, P5 scattering, 2 materials, beam 15 degrees off axis),
+every group solved to a 1e-6 relative moment residual.  Synthetic, seeded inputs (no dataset).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--solver GMRES|FGMRES_ML]
+
+value = dose solves per second over all ranks (replicas: every rank solves its own copy, so the
+per-rank work is fixed and scaling is weak); ms_per_step = time-to-dose.  Device time is measured
+with CUDA events on the library's stream, max over ranks.  `e2e` repeats the solve through the
+public C ABI with the per-step inputs copied from pinned host memory and the dose read back.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "B200 time-to-dose @1e-6 resid: learned-precond FGMRES vs plain GMRES; sweep GB/s"
+UNIT = "dose solves/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--solver", default="GMRES", choices=["GMRES", "FGMRES_ML", "SI"])
+    p.add_argument("--m", type=int, default=20)
+    p.add_argument("--rtol", type=float, default=1e-6)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=20.0)
+    return p.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            parts = [p.strip() for p in l.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------------
+#  CPU baseline: the FP64 oracle (a restatement of the reference's OpenMP CPU path) on a bounded
+#  sample of the same workload.
+# ---------------------------------------------------------------------------------------------
+_CPU_CACHE = {}
+
+
+def cpu_setup(prob, threads):
+    """Oracle on the full mesh (sweep sample) and on a sub-box (scattering sample)."""
+    if "o_full" in _CPU_CACHE:
+        return _CPU_CACHE
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from lionbolt_b200 import problems as P
+    O.set_threads(threads)
+    o_full = O.Oracle(prob.mesh)
+    sel = np.linspace(0, prob.NI - 1, threads).astype(int)         # one direction per thread
+    o_full.set_angular(prob.k[sel], prob.w[sel], prob.Ls, literal=False)
+    sigt, sigs = prob.within_group(0)
+    o_full.set_xs(sigt, sigs)
+    sub = P.multigroup_box(n=(6, 6, 12), size=(3.0, 3.0, 6.0), G=1, Ng=prob.Ng, Nc=prob.Nc, slab=(1.0, 2.0))
+    o_sub = O.Oracle(sub.mesh)
+    o_sub.set_angular(sub.k, sub.w, prob.Ng - 1, literal=False)
+    s = np.zeros((2, prob.Ng))
+    s[:, :sigs.shape[1]] = sigs
+    o_sub.set_xs(sigt, s)
+    # matvec count of the FP64 reference method (angular GMRES(m)) per group, from the same physics
+    # on a coarsened mesh (iteration counts of the within-group solve depend on the scattering
+    # ratios and the optical size, not on the mesh resolution to first order)
+    coarse = P.multigroup_box(n=(4, 4, 8), G=prob.G, Ng=prob.Ng, Nc=prob.Nc)
+    o_c = O.Oracle(coarse.mesh)
+    o_c.set_angular(coarse.k, coarse.w, prob.Ls, literal=False)
+    t0 = time.perf_counter()
+    _, _, iters = o_c.multigroup(coarse, "GMRES", m=20, rtol=1e-6)
+    _CPU_CACHE.update(o_full=o_full, sel=sel, o_sub=o_sub, sub=sub, iters=iters,
+                      iter_seconds=time.perf_counter() - t0)
+    return _CPU_CACHE
+
+
+def cpu_sample(prob, threads, budget_s):
+    """One bounded sample -> (estimated seconds per dose, details)."""
+    c = cpu_setup(prob, threads)
+    o_full, sel, o_sub, sub = c["o_full"], c["sel"], c["o_sub"], c["sub"]
+    rng = np.random.default_rng(0)
+    q = rng.uniform(size=o_full.NENK * len(sel))
+    t_sw, n_sw = 0.0, 0
+    x = rng.normal(size=o_sub.NENK * sub.NI)
+    t_k, n_k = 0.0, 0
+    t_end = time.perf_counter() + budget_s
+    while True:
+        t0 = time.perf_counter()
+        o_full.transport_inv(q)
+        t_sw += time.perf_counter() - t0
+        n_sw += 1
+        t0 = time.perf_counter()
+        o_sub.scatter_apply(x)
+        t_k += time.perf_counter() - t0
+        n_k += 1
+        if time.perf_counter() > t_end:
+            break
+    NI = prob.NI
+    sweep_full = (t_sw / n_sw) * NI / len(sel)                    # all 288 directions
+    k_full = (t_k / n_k) * prob.mesh.NENK / o_sub.NENK              # all 3,072,000 nodes
+    matvec = sweep_full + k_full
+    nmv = int(np.sum(c["iters"])) + 2 * prob.G                     # + RHS sweep and final sweep per group
+    sec_per_dose = nmv * matvec
+    return sec_per_dose, dict(sweep_s=sweep_full, scatter_s=k_full, matvecs=nmv, iters=c["iters"].tolist(),
+                              sweep_dirs=len(sel), scatter_nodes=o_sub.NENK)
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from lionbolt_b200 import problems as P
+    prob = P.config1()
+    threads = os.cpu_count() or 1
+    per_step = max(3.0, min(args.cpu_seconds, 12.0))
+    for _ in range(args.warmup):
+        cpu_sample(prob, threads, 1.0)
+    times, det = [], None
+    for _ in range(args.steps):
+        s, det = cpu_sample(prob, threads, per_step)
+        times.append(s)
+    sec = float(np.mean(times))
+    value = 1.0 / sec
+    sample = (f"FP64 oracle (CPU restatement of the reference OpenMP path; the Fortran reference has no compiler "
+              f"here): T^-1 over {det['sweep_dirs']} of 288 directions on the full 768k-tet mesh + K (per-node "
+              f"dgemv path, 2 materials) on {det['scatter_nodes']} nodes, scaled to the full sizes; "
+              f"x {det['matvecs']} operator applications (angular GMRES(20) counts of the same physics on a "
+              f"coarsened mesh)")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "config1 multigroup dose solve: 768000 tets x 288 dirs x 20 groups, P5, GMRES to 1e-6",
+                       "timing": "CPU wall clock of a bounded sample, extrapolated"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "details": det}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    rank, world, local = dist_env()
+    import torch
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from lionbolt_b200 import MultigroupSolver
+    from lionbolt_b200 import _lib
+    from lionbolt_b200 import problems as P
+
+    prob = P.config1()
+    mg = MultigroupSolver(device=local).set_problem(prob)
+    h = mg._h
+
+    def step():
+        return mg.solve(args.solver, m=args.m, rtol=args.rtol, atol=0.0)
+
+    for _ in range(args.warmup):
+        step()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        h.call("lb_synchronize")
+
+    # ---- device-timed region ----
+    barrier()
+    h.reset_timers()
+    iters = None
+    with ClockSampler(local) as clocks:
+        h.mark(0)
+        for _ in range(args.steps):
+            iters = step()
+        h.mark(1)
+        dev_ms = h.elapsed_ms(0, 1)
+    barrier()
+    tm = h.timers()
+    launches = int(sum(v[1] for v in tm.values()))
+    t_max = dev_ms
+    if world > 1:
+        t = torch.tensor([dev_ms], device=f"cuda:{local}", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        t_max = float(t.item())
+    ms_per_step = t_max / args.steps
+    value = world * args.steps / (t_max / 1e3)
+
+    # sweep roofline
+    by, up, nz = np.zeros(1), np.zeros(1), np.zeros(1, dtype=np.int64)
+    h.call("lb_sweep_stats", _lib.dptr(by), _lib.dptr(up), nz.ctypes.data_as(_lib._c_ll_p))
+    sw_ms, sw_n = tm["sweep"]
+    per_sweep_ms = sw_ms / max(sw_n, 1)
+    achieved = by[0] / (per_sweep_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "sweep_dram_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            d = json.load(f)
+        # dram bytes of one captured sweep, scaled by the update count of this workload
+        traffic = d["dram_bytes"] * (up[0] / d["updates"])
+
+    # ---- end-to-end through the C ABI with pinned host buffers ----
+    NENK, G = prob.mesh.NENK, prob.G
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).pin_memory()
+    h_sigt, h_sigs, h_dd, h_unc, h_dir = (pin(prob.sigt), pin(prob.sigs), pin(prob.dd), pin(prob.unc),
+                                          pin(prob.beam_dir))
+    h_dose = torch.empty(NENK, dtype=torch.float64).pin_memory()
+    dp = lambda t: _lib.ctypes.cast(t.data_ptr(), _lib._c_double_p)
+    h2d = sum(int(t.numel()) * 8 for t in (h_sigt, h_sigs, h_dd, h_unc, h_dir))
+    d2h = NENK * 8
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        h.call("lb_mg_update_inputs", dp(h_sigt), dp(h_sigs), dp(h_dd), dp(h_unc), dp(h_dir))
+        step()
+        h.call("lb_mg_get_results", None, dp(h_dose))
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * args.steps / e2e_s
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        sec, det = cpu_sample(prob, threads, args.cpu_seconds)
+        cpu = {"value": 1.0 / sec, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": (f"FP64 oracle, T^-1 over {det['sweep_dirs']} directions of the full mesh + K on "
+                          f"{det['scatter_nodes']} nodes scaled to full size, x {det['matvecs']} operator "
+                          f"applications; {args.cpu_seconds:.0f} s budget")}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32 sweep / split-bf16 tensor-core moments / f64 Krylov",
+                "data": "synthetic",
+                "config": {"workload": "config1 multigroup dose solve: 768000 tets x 288 dirs x 20 groups, P5, "
+                                       f"{args.solver}({args.m}) to {args.rtol:g}",
+                           "parallelism": f"replicas x{world}", "l2": "inputs > L2 (3.5 GB angular vector)"},
+                "time_to_dose_s": ms_per_step / 1e3,
+                "iterations_per_group": [int(x) for x in iters],
+                "updates_per_s": float(up[0]) * (sum(int(x) for x in iters) + 2 * G) / (ms_per_step / 1e3),
+                "phase_ms_per_step": {k: v[0] / args.steps for k, v in tm.items()},
+                "sweep": {"ms": per_sweep_ms, "gbs": achieved, "updates_per_s": up[0] / (per_sweep_ms / 1e3),
+                          "launch": h.sweep_config()},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": traffic, "kernel": "sweep_levels_kernel",
+                             "peak_source": peak_kind},
+                "gpu_launches": launches,
+                "clocks": clocks.summary(),
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    mg.Destroy()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

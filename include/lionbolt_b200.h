@@ -49,7 +49,8 @@ enum lb_solver {
 };
 
 /* phase timers reported by lb_get_timers (milliseconds of device time, CUDA events) */
-enum lb_timer { LB_T_SWEEP = 0, LB_T_M2D = 1, LB_T_D2M = 2, LB_T_KRYLOV = 3, LB_T_COPY = 4, LB_T_PRECOND = 5, LB_NTIMERS = 6 };
+enum lb_timer { LB_T_SWEEP = 0, LB_T_M2D = 1, LB_T_D2M = 2, LB_T_KRYLOV = 3, LB_T_COPY = 4, LB_T_PRECOND = 5,
+                LB_T_TALLY = 6, LB_NTIMERS = 7 };
 
 int lb_version(void);
 const char* lb_status_string(int status);
@@ -124,10 +125,19 @@ int lb_boltzmann_solve(lb_handle* h, double* s, int solver, int m, double rtol, 
  *   at every DG node; beam_dir[3] its direction (monodirectional first-collision source). */
 int lb_mg_set_problem(lb_handle* h, int G, int Ls, const double* sigt, const double* sigs, const double* dd,
                       const double* unc, const double* beam_dir);
+/* Replaces the per-solve inputs of a problem already set with the same sizes (no allocation):
+ * cross sections, dose cross sections, uncollided flux and beam direction. */
+int lb_mg_update_inputs(lb_handle* h, const double* sigt, const double* sigs, const double* dd, const double* unc,
+                        const double* beam_dir);
 /* Runs every group to the stopping test; iters[G] receives operator applications per group. */
 int lb_mg_solve(lb_handle* h, int solver, int m, double rtol, double atol, int maxit, int* iters);
 /* flux[G][NENK] scalar fluence (collided + uncollided), dose[NENK]; either may be NULL. */
 int lb_mg_get_results(lb_handle* h, double* flux, double* dose);
+
+/* Records CUDA event `slot` (0..15) on the handle's stream; lb_elapsed_ms returns the device time
+ * between two recorded slots (synchronising on the later one). */
+int lb_mark(lb_handle* h, int slot);
+int lb_elapsed_ms(lb_handle* h, int slot_a, int slot_b, double* ms);
 
 /* Device-time phase timers (ms) accumulated since the last reset, and kernel launch counts. */
 int lb_get_timers(lb_handle* h, double* ms, long long* launches);
@@ -135,6 +145,10 @@ int lb_reset_timers(lb_handle* h);
 /* Algorithmic traffic of one full sweep (bytes) and its update count (NE*NI). */
 int lb_sweep_stats(lb_handle* h, double* bytes_per_sweep, double* updates_per_sweep, long long* upstream_faces);
 int lb_synchronize(lb_handle* h);
+/* Sweep launch shape picked by the autotuner: cfg[0] schedule (0 levels, 1 dataflow), cfg[1]
+ * threads per CTA, cfg[2] directions per CTA, cfg[3] updates in flight per thread.  Returns
+ * LB_ERR_STATE while candidates are still being timed (the first sweeps of a handle). */
+int lb_get_sweep_config(lb_handle* h, int* cfg);
 
 #ifdef __cplusplus
 }

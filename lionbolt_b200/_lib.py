@@ -26,7 +26,7 @@ SOLVER_SI = 0
 SOLVER_GMRES = 1
 SOLVER_FGMRES_ML = 2
 
-TIMER_NAMES = ("sweep", "m2d", "d2m", "krylov", "copy", "precond")
+TIMER_NAMES = ("sweep", "m2d", "d2m", "krylov", "copy", "precond", "tally")
 
 _c_double_p = ctypes.POINTER(ctypes.c_double)
 _c_int_p = ctypes.POINTER(ctypes.c_int)
@@ -61,6 +61,10 @@ SIGNATURES = {
     "lb_reset_timers": (ctypes.c_int, [_vp]),
     "lb_sweep_stats": (ctypes.c_int, [_vp, _c_double_p, _c_double_p, _c_ll_p]),
     "lb_synchronize": (ctypes.c_int, [_vp]),
+    "lb_get_sweep_config": (ctypes.c_int, [_vp, _c_int_p]),
+    "lb_mg_update_inputs": (ctypes.c_int, [_vp, _c_double_p, _c_double_p, _c_double_p, _c_double_p, _c_double_p]),
+    "lb_mark": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "lb_elapsed_ms": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _c_double_p]),
 }
 
 _lib = None
@@ -141,10 +145,26 @@ class Handle:
         return check(self.h, getattr(self.lib, name)(self.h, *args))
 
     def timers(self):
-        ms = np.zeros(6)
-        n = np.zeros(6, dtype=np.int64)
+        ms = np.zeros(len(TIMER_NAMES))
+        n = np.zeros(len(TIMER_NAMES), dtype=np.int64)
         self.call("lb_get_timers", dptr(ms), n.ctypes.data_as(_c_ll_p))
         return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(TIMER_NAMES)}
+
+    def sweep_config(self):
+        cfg = np.zeros(4, dtype=np.int32)
+        st = self.lib.lb_get_sweep_config(self.h, iptr(cfg))
+        if st != LB_OK:
+            return None
+        return dict(schedule=("levels", "dataflow")[int(cfg[0])], threads=int(cfg[1]), dirs_per_cta=int(cfg[2]),
+                    ilp=int(cfg[3]))
+
+    def mark(self, slot):
+        self.call("lb_mark", int(slot))
+
+    def elapsed_ms(self, a, b):
+        ms = np.zeros(1)
+        self.call("lb_elapsed_ms", int(a), int(b), dptr(ms))
+        return float(ms[0])
 
     def reset_timers(self):
         self.call("lb_reset_timers")

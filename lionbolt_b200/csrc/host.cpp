@@ -119,14 +119,15 @@ static int dev_upload(Handle* h, T** p, const T* src, size_t count, const char* 
 }
 
 static void free_all(Handle* h) {
-    void* ptrs[] = {h->d_geom, h->d_mat, h->d_items, h->d_chunks, h->d_done, h->d_status, h->d_dirs, h->d_sigt,
+    void* ptrs[] = {h->d_geom, h->d_mat, h->d_items, h->d_chunks, h->d_lvl_start, h->d_lvl_base, h->d_nlev, h->d_done, h->d_status, h->d_dirs, h->d_sigt,
                     h->d_psi, h->d_qext, h->d_Ym2d, h->d_Yd2m, h->d_sigl, h->d_lofj, h->d_V, h->d_Z, h->d_x,
                     h->d_b, h->d_t, h->d_red, h->d_unc, h->d_phi_all, h->d_src, h->d_dose, h->d_flux,
-                    h->d_sigl_mg};
+                    h->d_sigl_mg, h->d_yb, h->d_dd};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (h->h_red) cudaFreeHost(h->h_red);
     for (auto& t : h->timers) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
     for (auto& t : h->free_timers) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
+    for (auto& m : h->marks) if (m) cudaEventDestroy(m);
 }
 
 // ----------------------------------------------------------------------------------------------
@@ -456,6 +457,15 @@ int lb_set_quadrature(lb_handle* h, int NI, const double* k, const double* w) {
     if (rc) return rc;
     rc = dev_alloc(h, &h->d_done, (size_t)h->total_levels, "level counters");
     if (rc) return rc;
+    rc = dev_upload(h, &h->d_lvl_start, h->lvl_start.data(), h->lvl_start.size(), "upload level starts");
+    if (rc) return rc;
+    rc = dev_upload(h, &h->d_lvl_base, h->lvl_base.data(), h->lvl_base.size(), "upload level offsets");
+    if (rc) return rc;
+    rc = dev_upload(h, &h->d_nlev, h->nlev.data(), h->nlev.size(), "upload level counts");
+    if (rc) return rc;
+    h->sweep_cfg = -1;
+    h->sweep_trial = 0;
+    h->sweep_trial_ms.clear();
     std::vector<float4> dirs(NI);
     for (int i = 0; i < NI; ++i)
         dirs[i] = make_float4((float)k[i * 3], (float)k[i * 3 + 1], (float)k[i * 3 + 2], (float)w[i]);
@@ -579,6 +589,32 @@ int lb_sweep_stats(lb_handle* h, double* bytes, double* updates, long long* upfa
     if (bytes) *bytes = b;
     if (updates) *updates = upd;
     if (upfaces) *upfaces = h->nz_upstream;
+    return LB_OK;
+}
+
+int lb_mark(lb_handle* h, int slot) {
+    if (!h || slot < 0 || slot >= 16) return LB_ERR_ARG;
+    if (h->device < 0) return fail(h, LB_ERR_STATE, "host-only handle");
+    cudaSetDevice(h->device);
+    if (!h->marks[slot] && cudaEventCreate(&h->marks[slot]) != cudaSuccess) return fail(h, LB_ERR_CUDA, "event create");
+    cudaError_t e = cudaEventRecord(h->marks[slot], h->stream);
+    return e == cudaSuccess ? LB_OK : cuda_fail(h, e, "event record");
+}
+
+int lb_elapsed_ms(lb_handle* h, int a, int b, double* ms) {
+    if (!h || !ms || a < 0 || b < 0 || a >= 16 || b >= 16 || !h->marks[a] || !h->marks[b]) return LB_ERR_ARG;
+    cudaSetDevice(h->device);
+    cudaError_t e = cudaEventSynchronize(h->marks[b]);
+    float f = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&f, h->marks[a], h->marks[b]);
+    if (e != cudaSuccess) return cuda_fail(h, e, "event elapsed");
+    *ms = f;
+    return LB_OK;
+}
+
+int lb_get_sweep_config(lb_handle* h, int* cfg) {
+    if (!h || !cfg) return LB_ERR_ARG;
+    if (sweep_config(h, &cfg[0], &cfg[1], &cfg[2], &cfg[3]) < 0) return LB_ERR_STATE;
     return LB_OK;
 }
 

@@ -203,7 +203,10 @@ int k_copy(Handle* h, double* y, const double* x, size_t n) {
 }
 
 int k_fill(Handle* h, double* y, double v, size_t n) {
+    Timer t;
+    timer_begin(h, LB_T_KRYLOV, t);
     fill_kernel<<<grid_for(h, n), 256, 0, h->stream>>>(y, v, n);
+    timer_end(h, t);
     return LB_OK;
 }
 
@@ -225,19 +228,28 @@ int k_f32_to_f64(Handle* h, double* y, const float* x, size_t n) {
 
 int k_moment_source(Handle* h, double* src, const double* phi, const float* sigl, const int* mat, long long NENK, int nm,
                     int nmpad, int accumulate) {
+    Timer t;
+    timer_begin(h, LB_T_TALLY, t);
     moment_source_kernel<<<grid_for(h, (size_t)nm * NENK), 256, 0, h->stream>>>(src, phi, sigl, mat, NENK, nm, nmpad, accumulate);
+    timer_end(h, t);
     return LB_OK;
 }
 
 int k_unc_source(Handle* h, double* src, const double* unc, const double* ybeam, const float* sigl, const int* mat,
                  long long NENK, int nm, int nmpad) {
+    Timer t;
+    timer_begin(h, LB_T_TALLY, t);
     unc_source_kernel<<<grid_for(h, (size_t)nm * NENK), 256, 0, h->stream>>>(src, unc, ybeam, sigl, mat, NENK, nm, nmpad);
+    timer_end(h, t);
     return LB_OK;
 }
 
 int k_dose_tally(Handle* h, const double* phi00, const double* unc, double unc_scale, const double* dd_mat, const int* mat,
                  double* flux, double* dose, long long NENK) {
+    Timer t;
+    timer_begin(h, LB_T_TALLY, t);
     dose_kernel<<<grid_for(h, (size_t)NENK), 256, 0, h->stream>>>(phi00, unc, unc_scale, dd_mat, mat, flux, dose, NENK);
+    timer_end(h, t);
     return LB_OK;
 }
 

@@ -78,6 +78,9 @@ struct Handle {
     int* d_mat = nullptr;          // [NE]
     int* d_items = nullptr;        // [NI][NE]
     int4* d_chunks = nullptr;      // [nchunks]
+    int* d_lvl_start = nullptr;    // concatenated level starts (copy of lvl_start)
+    int* d_lvl_base = nullptr;     // [NI+1]
+    int* d_nlev = nullptr;         // [NI]
     int* d_done = nullptr;         // [total_levels]
     SweepStatus* d_status = nullptr;
     float4* d_dirs = nullptr;      // [NI] (kx, ky, kz, w)
@@ -111,13 +114,26 @@ struct Handle {
     double* d_src = nullptr;        // [nm][NENK] group source moments
     double* d_dose = nullptr;       // [NENK]
     double* d_flux = nullptr;       // [G][NENK]
-    float* d_sigl_mg = nullptr;     // [Nm][nmpad] scratch for transfer scaling
+    float* d_sigl_mg = nullptr;     // [G][G][Nm][nmpad] transfer tables sigma_l(j)
+    double* d_yb = nullptr;         // [nm] beam-direction harmonics
+    double* d_dd = nullptr;         // [G][Nm] dose cross sections
+    int mg_alloc_G = 0, mg_alloc_nm = 0;
+    long long mg_alloc_NENK = 0;
+    size_t mg_alloc_tab = 0;
 
     // ---- timers ----
     std::vector<Timer> timers;
     std::vector<Timer> free_timers;
     double acc_ms[LB_NTIMERS] = {0};
     long long launches[LB_NTIMERS] = {0};
+
+    // sweep launch configuration chosen by the online autotuner (sweep.cu)
+    int sweep_cfg = -1;            // index into the candidate table, -1 = still tuning
+    int sweep_trial = 0;
+    std::vector<float> sweep_trial_ms;
+    int sweep_cfg_forced = -1;     // set through LB_SWEEP_CONFIG for experiments
+
+    cudaEvent_t marks[16] = {};
 
     // learned preconditioner state (mlp.cu)
     void* mlp = nullptr;
@@ -141,6 +157,8 @@ void timers_flush(Handle* h);
 // ---- kernels (sweep.cu / moments.cu / krylov.cu) ----
 // Full transport sweep psi <- T^{-1} psi (FP32, in place, natural layout [NI][NENK]).
 int launch_sweep(Handle* h, float* psi);
+// Chosen sweep launch shape (-1 while the autotuner is still timing candidates).
+int sweep_config(Handle* h, int* kind, int* threads, int* dpc, int* ilp);
 // q[i][n] = sum_j Y_j(k_i) * (sigl[mat(n)][j] * x[j][n] + a[j][n]) (+ qadd[i][n] if given).
 // x and a are FP64 moment vectors [nm][NENK]; either may be null.
 int launch_m2d(Handle* h, const double* x, const float* sigl, const double* a, const float* qadd, float* q);

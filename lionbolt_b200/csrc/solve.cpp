@@ -384,25 +384,41 @@ int lb_mg_set_problem(lb_handle* h, int G, int Ls, const double* sigt, const dou
                     for (int j = l * l; j < (l + 1) * (l + 1); ++j)
                         tab[(((size_t)gp * G + g) * Nm + m) * nmpad + j] =
                             (float)sigs[(((size_t)gp * G + g) * Nm + m) * (Ls + 1) + l];
-    if (h->d_sigl_mg) cudaFree(h->d_sigl_mg);
-    cudaError_t e = cudaMalloc(&h->d_sigl_mg, sizeof(float) * tab.size());
-    if (e != cudaSuccess) return cuda_fail(h, e, "transfer tables");
-    cudaMemcpy(h->d_sigl_mg, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice);
     const size_t NENK = (size_t)h->NENK;
-    auto realloc = [&](double** p, size_t cnt, const char* what) -> int {
-        if (*p) cudaFree(*p);
-        *p = nullptr;
-        cudaError_t ee = cudaMalloc(p, sizeof(double) * cnt);
-        return ee == cudaSuccess ? LB_OK : cuda_fail(h, ee, what);
-    };
-    if ((rc = realloc(&h->d_unc, NENK, "uncollided flux"))) return rc;
-    if ((rc = realloc(&h->d_phi_all, (size_t)G * nm * NENK, "group flux moments"))) return rc;
-    if ((rc = realloc(&h->d_src, (size_t)nm * NENK, "group source"))) return rc;
-    if ((rc = realloc(&h->d_dose, NENK, "dose"))) return rc;
-    if ((rc = realloc(&h->d_flux, (size_t)G * NENK, "group fluence"))) return rc;
-    if (unc) cudaMemcpy(h->d_unc, unc, sizeof(double) * NENK, cudaMemcpyHostToDevice);
-    else cudaMemset(h->d_unc, 0, sizeof(double) * NENK);
+    const bool same = h->mg_alloc_G == G && h->mg_alloc_nm == nm && h->mg_alloc_NENK == (long long)NENK &&
+                      h->mg_alloc_tab == tab.size();
+    if (!same) {
+        auto realloc = [&](auto** p, size_t cnt, const char* what) -> int {
+            if (*p) cudaFree(*p);
+            *p = nullptr;
+            cudaError_t ee = cudaMalloc((void**)p, sizeof(**p) * cnt);
+            return ee == cudaSuccess ? LB_OK : cuda_fail(h, ee, what);
+        };
+        if ((rc = realloc(&h->d_sigl_mg, tab.size(), "transfer tables"))) return rc;
+        if ((rc = realloc(&h->d_unc, NENK, "uncollided flux"))) return rc;
+        if ((rc = realloc(&h->d_phi_all, (size_t)G * nm * NENK, "group flux moments"))) return rc;
+        if ((rc = realloc(&h->d_src, (size_t)nm * NENK, "group source"))) return rc;
+        if ((rc = realloc(&h->d_dose, NENK, "dose"))) return rc;
+        if ((rc = realloc(&h->d_flux, (size_t)G * NENK, "group fluence"))) return rc;
+        if ((rc = realloc(&h->d_yb, 256, "beam harmonics"))) return rc;
+        if ((rc = realloc(&h->d_dd, (size_t)G * Nm, "dose cross sections"))) return rc;
+        h->mg_alloc_G = G; h->mg_alloc_nm = nm; h->mg_alloc_NENK = (long long)NENK; h->mg_alloc_tab = tab.size();
+    }
+    cudaError_t e = cudaMemcpyAsync(h->d_sigl_mg, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_dd, dd, sizeof(double) * (size_t)G * Nm, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) {
+        if (unc) e = cudaMemcpyAsync(h->d_unc, unc, sizeof(double) * NENK, cudaMemcpyHostToDevice, h->stream);
+        else e = cudaMemsetAsync(h->d_unc, 0, sizeof(double) * NENK, h->stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "upload problem");
     return LB_OK;
+}
+
+int lb_mg_update_inputs(lb_handle* h, const double* sigt, const double* sigs, const double* dd, const double* unc,
+                        const double* beam_dir) {
+    if (!h || h->device < 0 || h->G < 1 || !h->d_phi_all) return h ? fail(h, LB_ERR_STATE, "lb_mg_update_inputs: problem not set") : LB_ERR_ARG;
+    return lb_mg_set_problem(h, h->G, h->Ls, sigt, sigs, dd, unc, beam_dir);
 }
 
 int lb_mg_solve(lb_handle* h, int solver, int m, double rtol, double atol, int maxit, int* iters) {
@@ -419,10 +435,7 @@ int lb_mg_solve(lb_handle* h, int solver, int m, double rtol, double atol, int m
     // beam direction harmonics Y_j(Omega_b)
     std::vector<double> yb(nm);
     real_sh(Ls, h->beam_dir.data(), yb.data());
-    double* d_yb = nullptr;
-    double* d_dd = nullptr;
-    cudaMalloc(&d_yb, sizeof(double) * nm);
-    cudaMalloc(&d_dd, sizeof(double) * Nm);
+    double* d_yb = h->d_yb;
     cudaMemcpyAsync(d_yb, yb.data(), sizeof(double) * nm, cudaMemcpyHostToDevice, h->stream);
     cudaMemsetAsync(h->d_dose, 0, sizeof(double) * NENK, h->stream);
     auto table = [&](int gp, int g) { return h->d_sigl_mg + (((size_t)gp * G + g) * Nm) * nmpad; };
@@ -446,14 +459,11 @@ int lb_mg_solve(lb_handle* h, int solver, int m, double rtol, double atol, int m
         KrylovResult kr = moment_solve(h, h->d_b, phi, solver, m, rtol, atol, maxit, table(g, g));
         if (iters) iters[g] = kr.nmv;
         if ((rc = kr.status)) break;
-        cudaMemcpyAsync(d_dd, h->mg_dd.data() + (size_t)g * Nm, sizeof(double) * Nm, cudaMemcpyHostToDevice, h->stream);
-        k_dose_tally(h, phi, h->d_unc, g == 0 ? 1.0 : 0.0, d_dd, h->d_mat, h->d_flux + (size_t)g * NENK, h->d_dose,
-                     (long long)NENK);
-        cudaStreamSynchronize(h->stream);
+        k_dose_tally(h, phi, h->d_unc, g == 0 ? 1.0 : 0.0, h->d_dd + (size_t)g * Nm, h->d_mat,
+                     h->d_flux + (size_t)g * NENK, h->d_dose, (long long)NENK);
     }
-    cudaStreamSynchronize(h->stream);
-    cudaFree(d_yb);
-    cudaFree(d_dd);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (!rc && e != cudaSuccess) rc = cuda_fail(h, e, "multigroup solve");
     return rc;
 }
 
@@ -461,8 +471,10 @@ int lb_mg_get_results(lb_handle* h, double* flux, double* dose) {
     if (!h || h->device < 0 || !h->d_dose) return LB_ERR_STATE;
     cudaSetDevice(h->device);
     cudaError_t e = cudaSuccess;
-    if (flux) e = cudaMemcpy(flux, h->d_flux, sizeof(double) * (size_t)h->G * h->NENK, cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess && dose) e = cudaMemcpy(dose, h->d_dose, sizeof(double) * (size_t)h->NENK, cudaMemcpyDeviceToHost);
+    if (flux) e = cudaMemcpyAsync(flux, h->d_flux, sizeof(double) * (size_t)h->G * h->NENK, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess && dose)
+        e = cudaMemcpyAsync(dose, h->d_dose, sizeof(double) * (size_t)h->NENK, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     return e == cudaSuccess ? LB_OK : cuda_fail(h, e, "read results");
 }
 
