@@ -19,18 +19,24 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-// partial[b][j] = sum over this block's share of q of V[j][q] * w[q], j < nv
+// partial[b][j] = sum over this block's share of q of V[j][q] * w[q], j < nv.
+// Vectors are read as double2 (n is even: n = nm * NENK with NENK a multiple of 4).
 __global__ void __launch_bounds__(kRedThreads) dots_kernel(const double* __restrict__ V, size_t ldv, int nv,
                                                           const double* __restrict__ w, size_t n, double* partial) {
     __shared__ double s[kRedThreads / 32][kMaxDots];
     double acc[kMaxDots];
 #pragma unroll
     for (int j = 0; j < kMaxDots; ++j) acc[j] = 0.0;
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
-        const double wq = __ldcs(&w[q]);
+    const size_t n2 = n / 2;
+    const double2* w2 = reinterpret_cast<const double2*>(w);
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n2; q += (size_t)gridDim.x * blockDim.x) {
+        const double2 wq = __ldcs(&w2[q]);
 #pragma unroll
         for (int j = 0; j < kMaxDots; ++j)
-            if (j < nv) acc[j] = fma(__ldcs(&V[(size_t)j * ldv + q]), wq, acc[j]);
+            if (j < nv) {
+                const double2 v = __ldcs(reinterpret_cast<const double2*>(V + (size_t)j * ldv) + q);
+                acc[j] = fma(v.x, wq.x, fma(v.y, wq.y, acc[j]));
+            }
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
@@ -53,13 +59,19 @@ __global__ void __launch_bounds__(kRedThreads) axpy_norm_kernel(double* w, const
                                                                Coefs cf, size_t n, double* partial) {
     __shared__ double s[kRedThreads / 32];
     double acc = 0.0;
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
-        double v = w[q];
+    const size_t n2 = n / 2;
+    double2* w2 = reinterpret_cast<double2*>(w);
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n2; q += (size_t)gridDim.x * blockDim.x) {
+        double2 v = w2[q];
 #pragma unroll
         for (int j = 0; j < kMaxDots; ++j)
-            if (j < nv) v = fma(-cf.c[j], __ldcs(&V[(size_t)j * ldv + q]), v);
-        w[q] = v;
-        acc = fma(v, v, acc);
+            if (j < nv) {
+                const double2 u = __ldcs(reinterpret_cast<const double2*>(V + (size_t)j * ldv) + q);
+                v.x = fma(-cf.c[j], u.x, v.x);
+                v.y = fma(-cf.c[j], u.y, v.y);
+            }
+        w2[q] = v;
+        acc = fma(v.x, v.x, fma(v.y, v.y, acc));
     }
     acc = warp_sum(acc);
     if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = acc;
@@ -141,7 +153,8 @@ inline int grid_for(Handle* h, size_t n) {
 
 int k_dots(Handle* h, const double* V, size_t ldv, int nv, const double* w, size_t n, double* out) {
     if (nv > kMaxDots) return fail(h, LB_ERR_ARG, "dots: too many vectors");
-    const int grid = h->sm_count * 2;
+    if (n % 2) return fail(h, LB_ERR_ARG, "dots: odd vector length");
+    const int grid = h->sm_count * 4;
     Timer t;
     timer_begin(h, LB_T_KRYLOV, t);
     dots_kernel<<<grid, kRedThreads, 0, h->stream>>>(V, ldv, nv, w, n, h->d_red);
@@ -160,9 +173,10 @@ int k_dots(Handle* h, const double* V, size_t ldv, int nv, const double* w, size
 // w -= sum_j coef[j] V[j]; returns ||w||^2 through *nrm2 (may be null)
 int k_multi_axpy_norm(Handle* h, double* w, const double* V, size_t ldv, int nv, const double* coef, size_t n, double* nrm2) {
     if (nv > kMaxDots) return fail(h, LB_ERR_ARG, "axpy: too many vectors");
+    if (n % 2) return fail(h, LB_ERR_ARG, "axpy: odd vector length");
     Coefs cf;
     for (int j = 0; j < kMaxDots; ++j) cf.c[j] = (j < nv) ? coef[j] : 0.0;
-    const int grid = h->sm_count * 2;
+    const int grid = h->sm_count * 4;
     Timer t;
     timer_begin(h, LB_T_KRYLOV, t);
     axpy_norm_kernel<<<grid, kRedThreads, 0, h->stream>>>(w, V, ldv, nv, cf, n, h->d_red);

@@ -216,6 +216,175 @@ __global__ void __launch_bounds__(kThreads) d2m_kernel(const float* __restrict__
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Streaming versions.  The constant operand (Y or w*Y planes) is copied once per persistent CTA into
+// shared memory with rows padded to an odd multiple of 16 bytes and fed to the tensor cores with
+// ldmatrix; the data operand streams from HBM straight into mma fragments (each warp load instruction
+// touches 4 rows x 32 contiguous bytes) and is split into BF16 planes in registers.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ void ldsm_x4(uint32_t* r, const void* smem_row) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(smem_row);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(a));
+}
+
+// (v0, v1) -> packed hi / mid / lo BF16 pairs (low half = v0)
+__device__ __forceinline__ void split_pair(float v0, float v1, uint32_t& hi, uint32_t& mid, uint32_t& lo) {
+    __nv_bfloat162 h = __floats2bfloat162_rn(v0, v1);
+    float2 fh = __bfloat1622float2(h);
+    const float r0 = v0 - fh.x, r1 = v1 - fh.y;
+    __nv_bfloat162 m = __floats2bfloat162_rn(r0, r1);
+    float2 fm = __bfloat1622float2(m);
+    __nv_bfloat162 l = __floats2bfloat162_rn(r0 - fm.x, r1 - fm.y);
+    hi = *reinterpret_cast<uint32_t*>(&h);
+    mid = *reinterpret_cast<uint32_t*>(&m);
+    lo = *reinterpret_cast<uint32_t*>(&l);
+}
+
+// Copy the [3][rows][cols] BF16 planes into shared memory with row stride cols + 8.
+__device__ __forceinline__ void stage_planes(const __nv_bfloat16* __restrict__ g, __nv_bfloat16* s, int rows, int cols) {
+    const int cw = cols / 8, rs = cols + 8;      // 16-byte chunks per row, padded row stride (halves)
+    const int total = 3 * rows * cw;
+    for (int c = threadIdx.x; c < total; c += blockDim.x) {
+        const int pr = c / cw, q = c % cw;       // pr = plane*rows + row
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(g + (size_t)pr * cols) + q);
+        *reinterpret_cast<uint4*>(s + (size_t)pr * rs + q * 8) = v;
+    }
+    __syncthreads();
+}
+
+// M2D: q[i][n] = sum_j Y[i][j] xt[j][n] (+ qadd),  xt = sigl[mat(n)][j] x[j][n] + a[j][n].
+// Warp w owns nodes n0 + 8w .. +7 of the 64-node tile; its B fragments for all K stay in registers.
+template <int KT>
+__global__ void __launch_bounds__(kThreads) m2d_stream_kernel(const double* __restrict__ x, const float* __restrict__ sigl,
+                                                             const double* __restrict__ add, const float* __restrict__ qadd,
+                                                             const int* __restrict__ mat, const __nv_bfloat16* __restrict__ Y,
+                                                             float* __restrict__ q, long long NENK, int NI, int NIpad,
+                                                             int nm, int nmpad, long long ntiles) {
+    extern __shared__ __align__(16) __nv_bfloat16 ys[];     // [3][NIpad][nmpad + 8]
+    stage_planes(Y, ys, NIpad, nmpad);
+    const int rs = nmpad + 8;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int mi = lane >> 3, rr = lane & 7;                // ldmatrix: matrix index, row in matrix
+    const int arow = rr + 8 * (mi & 1), acol = 8 * (mi >> 1);
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long long n = tile * kTileN + warp * 8 + g;   // node of this thread's B column
+        const bool nok = n < NENK;
+        const int m = nok ? __ldg(&mat[n >> 2]) : 0;
+        uint32_t bf[KT][3][2];
+#pragma unroll
+        for (int kt = 0; kt < KT; ++kt) {
+            float v[4];
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                const int j = kt * 16 + 2 * t + (h & 1) + 8 * (h >> 1);
+                double s = 0.0;
+                if (nok && j < nm) {
+                    if (x) s = (double)__ldg(&sigl[(size_t)m * nmpad + j]) * __ldcs(&x[(size_t)j * NENK + n]);
+                    if (add) s += __ldcs(&add[(size_t)j * NENK + n]);
+                }
+                v[h] = (float)s;
+            }
+            split_pair(v[0], v[1], bf[kt][0][0], bf[kt][1][0], bf[kt][2][0]);
+            split_pair(v[2], v[3], bf[kt][0][1], bf[kt][1][1], bf[kt][2][1]);
+        }
+        const long long nc = tile * kTileN + warp * 8 + 2 * t;   // output column pair of this thread
+        for (int m0 = 0; m0 < NIpad; m0 += 16) {
+            float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int kt = 0; kt < KT; ++kt) {
+                uint32_t af[3][4];
+#pragma unroll
+                for (int p = 0; p < 3; ++p)
+                    ldsm_x4(af[p], ys + ((size_t)p * NIpad + m0 + arow) * rs + kt * 16 + acol);
+                mma_split6(acc, af, bf[kt]);
+            }
+            if (nc < NENK) {
+                const int r0 = m0 + g, r1 = m0 + g + 8;
+                if (r0 < NI) {
+                    float2 v = make_float2(acc[0], acc[1]);
+                    if (qadd) { float2 u = *reinterpret_cast<const float2*>(&qadd[(size_t)r0 * NENK + nc]); v.x += u.x; v.y += u.y; }
+                    __stcs(reinterpret_cast<float2*>(&q[(size_t)r0 * NENK + nc]), v);
+                }
+                if (r1 < NI) {
+                    float2 v = make_float2(acc[2], acc[3]);
+                    if (qadd) { float2 u = *reinterpret_cast<const float2*>(&qadd[(size_t)r1 * NENK + nc]); v.x += u.x; v.y += u.y; }
+                    __stcs(reinterpret_cast<float2*>(&q[(size_t)r1 * NENK + nc]), v);
+                }
+            }
+        }
+    }
+}
+
+// D2M: z[j][n] = sum_i Dw[j][i] psi[i][n];  out = alpha * xin + beta * z.
+// Warp w owns nodes n0 + 8w .. +7; psi fragments stream from HBM one k-step ahead of the MMAs.
+template <int MT>
+__global__ void __launch_bounds__(kThreads) d2m_stream_kernel(const float* __restrict__ psi, const __nv_bfloat16* __restrict__ Dw,
+                                                             const double* xin, double alpha, double beta, double* out,
+                                                             long long NENK, int NI, int NIpad, int nm, int nmpad,
+                                                             long long ntiles) {
+    extern __shared__ __align__(16) __nv_bfloat16 ds[];     // [3][nmpad][NIpad + 8]
+    stage_planes(Dw, ds, nmpad, NIpad);
+    const int rs = NIpad + 8;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int mi = lane >> 3, rr = lane & 7;
+    const int arow = rr + 8 * (mi & 1), acol = 8 * (mi >> 1);
+    const int mtiles = nmpad / 16;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long long n = tile * kTileN + warp * 8 + g;
+        const bool nok = n < NENK;
+        float acc[MT][4];
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) acc[mt][0] = acc[mt][1] = acc[mt][2] = acc[mt][3] = 0.f;
+        auto load = [&](int k0, float* v) {
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                const int i = k0 + 2 * t + (h & 1) + 8 * (h >> 1);
+                v[h] = (nok && i < NI) ? __ldcs(&psi[(size_t)i * NENK + n]) : 0.f;
+            }
+        };
+        float cur[4], nxt[4];
+        load(0, cur);
+        for (int k0 = 0; k0 < NIpad; k0 += 16) {
+            if (k0 + 16 < NIpad) load(k0 + 16, nxt);
+            uint32_t bf[3][2];
+            split_pair(cur[0], cur[1], bf[0][0], bf[1][0], bf[2][0]);
+            split_pair(cur[2], cur[3], bf[0][1], bf[1][1], bf[2][1]);
+#pragma unroll
+            for (int mt = 0; mt < MT; ++mt) {
+                if (mt >= mtiles) break;
+                uint32_t af[3][4];
+#pragma unroll
+                for (int p = 0; p < 3; ++p)
+                    ldsm_x4(af[p], ds + ((size_t)p * nmpad + mt * 16 + arow) * rs + k0 + acol);
+                mma_split6(acc[mt], af, bf);
+            }
+#pragma unroll
+            for (int h = 0; h < 4; ++h) cur[h] = nxt[h];
+        }
+        const long long nc = tile * kTileN + warp * 8 + 2 * t;
+        if (nc < NENK) {
+#pragma unroll
+            for (int mt = 0; mt < MT; ++mt) {
+                if (mt >= mtiles) break;
+                const int r0 = mt * 16 + g, r1 = r0 + 8;
+                if (r0 < nm) {
+                    double2 v = make_double2(beta * (double)acc[mt][0], beta * (double)acc[mt][1]);
+                    if (xin) { double2 u = *reinterpret_cast<const double2*>(&xin[(size_t)r0 * NENK + nc]); v.x += alpha * u.x; v.y += alpha * u.y; }
+                    *reinterpret_cast<double2*>(&out[(size_t)r0 * NENK + nc]) = v;
+                }
+                if (r1 < nm) {
+                    double2 v = make_double2(beta * (double)acc[mt][2], beta * (double)acc[mt][3]);
+                    if (xin) { double2 u = *reinterpret_cast<const double2*>(&xin[(size_t)r1 * NENK + nc]); v.x += alpha * u.x; v.y += alpha * u.y; }
+                    *reinterpret_cast<double2*>(&out[(size_t)r1 * NENK + nc]) = v;
+                }
+            }
+        }
+    }
+}
+
 template <int MT>
 int run_d2m(Handle* h, const float* psi, const double* xin, double alpha, double beta, double* out, long long ntiles,
             int grid, size_t smem) {
@@ -229,49 +398,107 @@ int run_d2m(Handle* h, const float* psi, const double* xin, double alpha, double
     return LB_OK;
 }
 
+
+template <int KT>
+cudaError_t run_m2d_stream(Handle* h, const double* x, const float* sigl, const double* a, const float* qadd, float* q,
+                           long long ntiles, size_t smem) {
+    static int per_sm = -1;
+    if (per_sm < 0) {
+        cudaFuncSetAttribute(m2d_stream_kernel<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, m2d_stream_kernel<KT>, kThreads, smem);
+        if (per_sm < 1) per_sm = 1;
+    }
+    long long grid = std::min<long long>(ntiles, (long long)h->sm_count * per_sm);
+    m2d_stream_kernel<KT><<<(int)grid, kThreads, smem, h->stream>>>(x, sigl, a, qadd, h->d_mat, h->d_Ym2d, q, h->NENK,
+                                                                    h->NI, h->NIpad, h->nm, h->nmpad, ntiles);
+    return cudaGetLastError();
+}
+
+template <int MT>
+cudaError_t run_d2m_stream(Handle* h, const float* psi, const double* xin, double alpha, double beta, double* out,
+                           long long ntiles, size_t smem) {
+    static int per_sm = -1;
+    if (per_sm < 0) {
+        cudaFuncSetAttribute(d2m_stream_kernel<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, d2m_stream_kernel<MT>, kThreads, smem);
+        if (per_sm < 1) per_sm = 1;
+    }
+    long long grid = std::min<long long>(ntiles, (long long)h->sm_count * per_sm);
+    d2m_stream_kernel<MT><<<(int)grid, kThreads, smem, h->stream>>>(psi, h->d_Yd2m, xin, alpha, beta, out, h->NENK,
+                                                                    h->NI, h->NIpad, h->nm, h->nmpad, ntiles);
+    return cudaGetLastError();
+}
+
+constexpr size_t kStreamSmemLimit = 200 * 1024;
+
 }  // namespace
 
 int launch_m2d(Handle* h, const double* x, const float* sigl, const double* a, const float* qadd, float* q) {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(m2d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        attr = true;
-    }
+    if (!sigl) sigl = h->d_sigl;
     const long long ntiles = (h->NENK + kTileN - 1) / kTileN;
-    const size_t smem = (size_t)3 * kTileN * smem_stride_words(h->nmpad) * 4;
-    if (smem > 227 * 1024) return fail(h, LB_ERR_ARG, "m2d: too many moments for the shared-memory tile");
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, m2d_kernel, kThreads, smem);
-    if (per_sm < 1) per_sm = 1;
-    long long grid = std::min<long long>(ntiles, (long long)h->sm_count * per_sm);
+    const int KT = h->nmpad / 16;
+    const size_t smem_stream = (size_t)3 * h->NIpad * (h->nmpad + 8) * 2;
     Timer t;
     timer_begin(h, LB_T_M2D, t);
-    m2d_kernel<<<(int)grid, kThreads, smem, h->stream>>>(x, sigl ? sigl : h->d_sigl, a, qadd, h->d_mat, h->d_Ym2d, q,
-                                                         h->NENK, h->NI, h->NIpad, h->nm, h->nmpad, ntiles);
+    cudaError_t e = cudaSuccess;
+    if (KT <= 8 && smem_stream <= kStreamSmemLimit) {
+        switch (KT) {
+            case 1: e = run_m2d_stream<1>(h, x, sigl, a, qadd, q, ntiles, smem_stream); break;
+            case 2: e = run_m2d_stream<2>(h, x, sigl, a, qadd, q, ntiles, smem_stream); break;
+            case 3: e = run_m2d_stream<3>(h, x, sigl, a, qadd, q, ntiles, smem_stream); break;
+            case 4: e = run_m2d_stream<4>(h, x, sigl, a, qadd, q, ntiles, smem_stream); break;
+            case 5: e = run_m2d_stream<5>(h, x, sigl, a, qadd, q, ntiles, smem_stream); break;
+            case 6: e = run_m2d_stream<6>(h, x, sigl, a, qadd, q, ntiles, smem_stream); break;
+            case 7: e = run_m2d_stream<7>(h, x, sigl, a, qadd, q, ntiles, smem_stream); break;
+            default: e = run_m2d_stream<8>(h, x, sigl, a, qadd, q, ntiles, smem_stream); break;
+        }
+    } else {
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(m2d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+            attr = true;
+        }
+        const size_t smem = (size_t)3 * kTileN * smem_stride_words(h->nmpad) * 4;
+        if (smem > 227 * 1024) { timer_end(h, t); return fail(h, LB_ERR_ARG, "m2d: too many moments for the shared-memory tile"); }
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, m2d_kernel, kThreads, smem);
+        if (per_sm < 1) per_sm = 1;
+        long long grid = std::min<long long>(ntiles, (long long)h->sm_count * per_sm);
+        m2d_kernel<<<(int)grid, kThreads, smem, h->stream>>>(x, sigl, a, qadd, h->d_mat, h->d_Ym2d, q, h->NENK, h->NI,
+                                                             h->NIpad, h->nm, h->nmpad, ntiles);
+        e = cudaGetLastError();
+    }
     timer_end(h, t);
-    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(h, e, "m2d kernel launch");
     return LB_OK;
 }
 
 int launch_d2m(Handle* h, const float* psi, const double* xin, double alpha, double beta, double* out) {
     const long long ntiles = (h->NENK + kTileN - 1) / kTileN;
-    const size_t smem = (size_t)3 * kTileN * smem_stride_words(h->NIpad) * 4;
-    if (smem > 227 * 1024) return fail(h, LB_ERR_ARG, "d2m: too many directions for the shared-memory tile");
     const int mtiles = h->nmpad / 16;
-    int per_sm = 2;
-    if (smem > 110 * 1024) per_sm = 1;
-    long long grid = std::min<long long>(ntiles, (long long)h->sm_count * per_sm);
+    const size_t smem_stream = (size_t)3 * h->nmpad * (h->NIpad + 8) * 2;
     Timer t;
     timer_begin(h, LB_T_D2M, t);
-    int rc;
-    if (mtiles <= 1) rc = run_d2m<1>(h, psi, xin, alpha, beta, out, ntiles, (int)grid, smem);
-    else if (mtiles <= 3) rc = run_d2m<3>(h, psi, xin, alpha, beta, out, ntiles, (int)grid, smem);
-    else if (mtiles <= 7) rc = run_d2m<7>(h, psi, xin, alpha, beta, out, ntiles, (int)grid, smem);
-    else rc = run_d2m<16>(h, psi, xin, alpha, beta, out, ntiles, (int)grid, smem);
+    cudaError_t e = cudaSuccess;
+    int rc = LB_OK;
+    if (smem_stream <= kStreamSmemLimit) {
+        if (mtiles <= 1) e = run_d2m_stream<1>(h, psi, xin, alpha, beta, out, ntiles, smem_stream);
+        else if (mtiles <= 3) e = run_d2m_stream<3>(h, psi, xin, alpha, beta, out, ntiles, smem_stream);
+        else if (mtiles <= 7) e = run_d2m_stream<7>(h, psi, xin, alpha, beta, out, ntiles, smem_stream);
+        else e = run_d2m_stream<16>(h, psi, xin, alpha, beta, out, ntiles, smem_stream);
+    } else {
+        const size_t smem = (size_t)3 * kTileN * smem_stride_words(h->NIpad) * 4;
+        if (smem > 227 * 1024) { timer_end(h, t); return fail(h, LB_ERR_ARG, "d2m: too many directions for the shared-memory tile"); }
+        int per_sm = smem > 110 * 1024 ? 1 : 2;
+        long long grid = std::min<long long>(ntiles, (long long)h->sm_count * per_sm);
+        if (mtiles <= 1) rc = run_d2m<1>(h, psi, xin, alpha, beta, out, ntiles, (int)grid, smem);
+        else if (mtiles <= 3) rc = run_d2m<3>(h, psi, xin, alpha, beta, out, ntiles, (int)grid, smem);
+        else if (mtiles <= 7) rc = run_d2m<7>(h, psi, xin, alpha, beta, out, ntiles, (int)grid, smem);
+        else rc = run_d2m<16>(h, psi, xin, alpha, beta, out, ntiles, (int)grid, smem);
+        e = cudaGetLastError();
+    }
     timer_end(h, t);
     if (rc) return rc;
-    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(h, e, "d2m kernel launch");
     return LB_OK;
 }
