@@ -103,6 +103,17 @@ int lb_get_schedule(lb_handle* h, int* sl, unsigned char* upmask, int* nlevels, 
  * leaves as solution (FP64 host buffer; the sweep runs in FP32 on the device). */
 int lb_transport_inv(lb_handle* h, double* s);
 
+/* T^{-1} in place on a caller-owned device vector, without allocating: psi is the FP32 angular
+ * vector [NI][NENK] in device memory of the handle's GPU (same layout as lb_transport_inv).  No
+ * counterpart in the reference: it exists for callers that cannot allocate device memory at solve
+ * time (a host framework that owns the allocator, a Fortran runtime that only passes pre-allocated
+ * device arrays, a loop that must not hit cudaMalloc's implicit synchronisation).  Its dependency
+ * counters live in a fixed 1 MiB file-scope device array (at most 262,144 direction-level pairs;
+ * larger schedules return LB_ERR_ARG) that every GPU loading the library keeps until exit.  The
+ * first call on a device looks up the array's device address; make that first call before any
+ * stream capture.  All calls on a device share the array: calls that overlap on the GPU race. */
+int lb_transport_inv_noalloc(lb_handle* h, float* psi);
+
 /* K x in place: replaces ScatteringOp%MatVec (ScatteringOperator.f90:39-70 ->
  * ScatteringAlgebra.f90:13-55).  Evaluated as moment-to-discrete (discrete-to-moment (x)). */
 int lb_scatter_apply(lb_handle* h, double* x);

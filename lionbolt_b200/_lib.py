@@ -64,6 +64,7 @@ SIGNATURES = {
     "lb_get_sweep_config": (ctypes.c_int, [_vp, _c_int_p]),
     "lb_mg_update_inputs": (ctypes.c_int, [_vp, _c_double_p, _c_double_p, _c_double_p, _c_double_p, _c_double_p]),
     "lb_mark": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "lb_transport_inv_noalloc": (ctypes.c_int, [_vp, ctypes.c_void_p]),
     "lb_elapsed_ms": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _c_double_p]),
 }
 

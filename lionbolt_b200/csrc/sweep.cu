@@ -398,3 +398,98 @@ int sweep_config(Handle* h, int* kind, int* threads, int* dpc, int* ilp) {
 }
 
 }  // namespace lb
+
+// =============================================================================================
+//  Allocation-free sweep.
+//
+//  For callers that cannot allocate device memory at solve time: code running inside a host
+//  framework that owns the device allocator (a memory pool, a Fortran runtime that only hands out
+//  pre-allocated device arrays), or a real-time loop where cudaMalloc's implicit device
+//  synchronisation is not acceptable.  The caller passes its own FP32 angular vector; the
+//  dataflow schedule's per-level completion counters and status word live in the file-scope array
+//  below instead of handle memory, so a call makes no cudaMalloc / cudaFree.
+//
+//  Limits and sharing: the array holds kNoAllocMaxLevels (direction, level) counters (1 MiB); a
+//  problem with more levels is rejected.  Every GPU that loads this library keeps the array until
+//  the process exits.  All calls on a device share it and it keeps the last call's contents: the
+//  counters are cleared at the start of every call, and calls that overlap on the GPU (two streams,
+//  two handles on one device) race on it and must be serialised by the caller.
+// =============================================================================================
+namespace lb {
+namespace {
+
+constexpr int kNoAllocMaxLevels = 1 << 18;
+constexpr int kNoAllocStatusInts = 8;   // SweepStatus, padded
+static __device__ __align__(256) int g_noalloc_scratch[kNoAllocStatusInts + kNoAllocMaxLevels];
+
+constexpr int kMaxDevices = 64;
+void* g_noalloc_ptr[kMaxDevices] = {};
+
+}  // namespace
+}  // namespace lb
+
+extern "C" int lb_transport_inv_noalloc(lb_handle* hh, float* psi) {
+    using namespace lb;
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || !psi) return LB_ERR_ARG;
+    if (h->device < 0) return fail(h, LB_ERR_STATE, "host-only handle: no device attached");
+    if (!h->mesh_ready || !h->angle_ready || h->sigt.empty())
+        return fail(h, LB_ERR_STATE, "TransportOp%MatInv was called, but the operator was not ready.");
+    if (h->total_levels > kNoAllocMaxLevels) {
+        char buf[200];
+        std::snprintf(buf, sizeof buf,
+                      "lb_transport_inv_noalloc: the schedule has %d (direction, level) pairs; the allocation-free "
+                      "entry point holds at most %d",
+                      h->total_levels, kNoAllocMaxLevels);
+        return fail(h, LB_ERR_ARG, buf);
+    }
+    if (h->device >= kMaxDevices) return fail(h, LB_ERR_ARG, "lb_transport_inv_noalloc: device index too large");
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) return cuda_fail(h, e, "lb_transport_inv_noalloc: set device");
+    // once per device, with that device current: the device address of the scratch array
+    if (!g_noalloc_ptr[h->device]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) return cuda_fail(h, e, "lb_transport_inv_noalloc: scratch address");
+        g_noalloc_ptr[h->device] = p;
+    }
+    int* base = static_cast<int*>(g_noalloc_ptr[h->device]);
+    SweepArgs a;
+    a.items = h->d_items;
+    a.chunks = h->d_chunks;
+    a.lvl_start = h->d_lvl_start;
+    a.lvl_base = h->d_lvl_base;
+    a.nlev = h->d_nlev;
+    a.done = base + kNoAllocStatusInts;
+    a.geom = h->d_geom;
+    a.dirs = h->d_dirs;
+    a.sigt = h->d_sigt;
+    a.psi = psi;
+    a.NENK = h->NENK;
+    a.NE = h->NE;
+    a.NI = h->NI;
+    a.nchunks = h->nchunks;
+    a.Nm = h->Nm;
+    a.status = reinterpret_cast<SweepStatus*>(base);
+    a.spin_limit = 1LL << 24;
+    e = cudaMemsetAsync(base, 0, sizeof(int) * ((size_t)kNoAllocStatusInts + h->total_levels), h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "lb_transport_inv_noalloc: clear scratch");
+    static int per_sm = -1;
+    if (per_sm < 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_dataflow_kernel, 256, 0);
+        if (per_sm < 1) per_sm = 1;
+    }
+    sweep_dataflow_kernel<<<h->sm_count * per_sm, 256, 0, h->stream>>>(a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(h, e, "lb_transport_inv_noalloc: launch");
+    SweepStatus st;
+    e = cudaMemcpyAsync(&st, base, sizeof(st), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "lb_transport_inv_noalloc: sweep");
+    if (st.err) {
+        char buf[160];
+        std::snprintf(buf, sizeof buf, "sweep: dependency wait timed out at chunk %d", st.err_chunk);
+        return fail(h, LB_ERR_TIMEOUT, buf);
+    }
+    return LB_OK;
+}
