@@ -119,7 +119,7 @@ static int dev_upload(Handle* h, T** p, const T* src, size_t count, const char* 
 }
 
 static void free_all(Handle* h) {
-    void* ptrs[] = {h->d_geom, h->d_mat, h->d_items, h->d_chunks, h->d_lvl_start, h->d_lvl_base, h->d_nlev, h->d_done, h->d_status, h->d_dirs, h->d_sigt,
+    void* ptrs[] = {h->d_geom, h->d_mat, h->d_items, h->d_groups, h->d_pitems, h->d_pbase, h->d_chunks, h->d_lvl_start, h->d_lvl_base, h->d_nlev, h->d_done, h->d_status, h->d_dirs, h->d_sigt,
                     h->d_psi, h->d_qext, h->d_Ym2d, h->d_Yd2m, h->d_sigl, h->d_lofj, h->d_V, h->d_Z, h->d_x,
                     h->d_b, h->d_t, h->d_red, h->d_unc, h->d_phi_all, h->d_src, h->d_dose, h->d_flux,
                     h->d_sigl_mg, h->d_yb, h->d_dd};
@@ -457,12 +457,71 @@ int lb_set_quadrature(lb_handle* h, int NI, const double* k, const double* w) {
     if (rc) return rc;
     rc = dev_alloc(h, &h->d_done, (size_t)h->total_levels, "level counters");
     if (rc) return rc;
+    {
+        // items with every level padded to a multiple of 32 (padding = -1): a 32-element chunk of the
+        // padded order never spans two levels, so its elements never depend on each other
+        std::vector<long long> pbase(NI + 1, 0);
+        for (int i = 0; i < NI; ++i) {
+            long long len = 0;
+            const int* st = &h->lvl_start[h->lvl_base[i]];
+            for (int L = 0; L < h->nlev[i]; ++L) len += ((st[L + 1] - st[L]) + 31) / 32 * 32;
+            pbase[i + 1] = pbase[i] + len;
+        }
+        std::vector<int> pitems((size_t)pbase[NI], -1);
+#pragma omp parallel for schedule(dynamic, 4)
+        for (int i = 0; i < NI; ++i) {
+            const int* st = &h->lvl_start[h->lvl_base[i]];
+            long long o = pbase[i];
+            for (int L = 0; L < h->nlev[i]; ++L) {
+                for (int es = st[L]; es < st[L + 1]; ++es) pitems[(size_t)o++] = h->items[(size_t)i * NE + es];
+                o = pbase[i] + (o - pbase[i] + 31) / 32 * 32;
+            }
+        }
+        h->npitems = pbase[NI];
+        rc = dev_upload(h, &h->d_pitems, pitems.data(), pitems.size(), "upload padded items");
+        if (rc) return rc;
+        rc = dev_upload(h, &h->d_pbase, pbase.data(), pbase.size(), "upload padded offsets");
+        if (rc) return rc;
+    }
     rc = dev_upload(h, &h->d_lvl_start, h->lvl_start.data(), h->lvl_start.size(), "upload level starts");
     if (rc) return rc;
     rc = dev_upload(h, &h->d_lvl_base, h->lvl_base.data(), h->lvl_base.size(), "upload level offsets");
     if (rc) return rc;
     rc = dev_upload(h, &h->d_nlev, h->nlev.data(), h->nlev.size(), "upload level counts");
     if (rc) return rc;
+    {
+        // classes of directions with identical schedules (exact comparison after a hash)
+        std::vector<unsigned long long> hsh(NI);
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < NI; ++i) {
+            unsigned long long x = 1469598103934665603ULL ^ (unsigned long long)h->nlev[i];
+            const int* it = &h->items[(size_t)i * NE];
+            for (int es = 0; es < NE; ++es) { x ^= (unsigned)it[es]; x *= 1099511628211ULL; }
+            hsh[i] = x;
+        }
+        h->dir_class.assign(NI, -1);
+        for (int i = 0; i < NI; ++i) {
+            if (h->dir_class[i] >= 0) continue;
+            h->dir_class[i] = i;
+            for (int j = i + 1; j < NI; ++j) {
+                if (h->dir_class[j] >= 0 || hsh[j] != hsh[i] || h->nlev[j] != h->nlev[i]) continue;
+                if (std::memcmp(&h->items[(size_t)i * NE], &h->items[(size_t)j * NE], sizeof(int) * (size_t)NE) == 0 &&
+                    std::equal(&h->lvl_start[h->lvl_base[i]], &h->lvl_start[h->lvl_base[i]] + h->nlev[i] + 1,
+                               &h->lvl_start[h->lvl_base[j]]))
+                    h->dir_class[j] = i;
+            }
+        }
+        h->class_members.clear();
+        h->class_start.assign(1, 0);
+        for (int i = 0; i < NI; ++i) {
+            if (h->dir_class[i] != i) continue;
+            for (int j = i; j < NI; ++j)
+                if (h->dir_class[j] == i) h->class_members.push_back(j);
+            h->class_start.push_back((int)h->class_members.size());
+        }
+        h->groups_gmax = 0;
+        h->ngroups = 0;
+    }
     h->sweep_cfg = -1;
     h->sweep_trial = 0;
     h->sweep_trial_ms.clear();

@@ -26,7 +26,15 @@ struct SweepStatus {
     int work;        // next chunk to claim
     int abort;       // set on any timeout; every warp stops
     int err;         // LB_ERR_TIMEOUT when set
-    int err_chunk;   // chunk whose wait gave up
+    int err_chunk;   // chunk (dataflow) or direction (element flags) whose wait gave up
+    int err_elem;    // element that waited (element flags)
+    int err_dep;     // upstream element it waited for
+    int err_pos;     // chunk start in the padded order
+    int err_bit;     // the awaited done bit as last read
+    int dbg_next;    // chunks claimed so far in that direction (x32)
+    int dbg_done;    // elements completed in that direction
+    int dbg_exited;  // warps that left the claim loop
+    int dbg_len;     // padded length of the direction
 };
 
 struct Timer {
@@ -78,6 +86,15 @@ struct Handle {
     int* d_mat = nullptr;          // [NE]
     int* d_items = nullptr;        // [NI][NE]
     int4* d_chunks = nullptr;      // [nchunks]
+    int* d_pitems = nullptr;       // padded items: every level of every direction padded to 32 with -1
+    long long* d_pbase = nullptr;  // [NI+1] start of each direction in d_pitems
+    long long npitems = 0;
+    // directions whose schedules are bit-identical (same order, same face masks) share a walk
+    std::vector<int> dir_class;    // [NI] class representative (smallest direction id of the class)
+    std::vector<int> class_members;  // directions sorted by class
+    std::vector<int> class_start;    // [nclass+1]
+    int* d_groups = nullptr;       // per-CTA groups for the grouped sweep, built per group size
+    int groups_gmax = 0, ngroups = 0;
     int* d_lvl_start = nullptr;    // concatenated level starts (copy of lvl_start)
     int* d_lvl_base = nullptr;     // [NI+1]
     int* d_nlev = nullptr;         // [NI]
@@ -148,6 +165,20 @@ void real_sh(int Ls, const double* dir, double* Y);
 void mlp_destroy(Handle* h);
 bool mlp_ready(Handle* h);
 int mlp_apply_precond(Handle* h, const double* v, double* z);
+
+// Allow a kernel the largest dynamic shared memory the device permits next to its static
+// shared memory (227 KB per CTA on sm_100 in total).  Clears the error state it may leave.
+template <class K>
+inline void allow_max_dynamic_smem(K kernel) {
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess) { cudaGetLastError(); return; }
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    int dyn = optin - (int)fa.sharedSizeBytes;
+    if (dyn > 0) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    cudaGetLastError();
+}
 
 // ---- timers ----
 void timer_begin(Handle* h, int kind, Timer& t);

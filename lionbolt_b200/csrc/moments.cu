@@ -390,7 +390,7 @@ int run_d2m(Handle* h, const float* psi, const double* xin, double alpha, double
             int grid, size_t smem) {
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(d2m_kernel<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        allow_max_dynamic_smem(d2m_kernel<MT>);
         attr = true;
     }
     d2m_kernel<MT><<<grid, kThreads, smem, h->stream>>>(psi, h->d_Yd2m, xin, alpha, beta, out, h->NENK, h->NI,
@@ -404,7 +404,7 @@ cudaError_t run_m2d_stream(Handle* h, const double* x, const float* sigl, const 
                            long long ntiles, size_t smem) {
     static int per_sm = -1;
     if (per_sm < 0) {
-        cudaFuncSetAttribute(m2d_stream_kernel<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        allow_max_dynamic_smem(m2d_stream_kernel<KT>);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, m2d_stream_kernel<KT>, kThreads, smem);
         if (per_sm < 1) per_sm = 1;
     }
@@ -419,7 +419,7 @@ cudaError_t run_d2m_stream(Handle* h, const float* psi, const double* xin, doubl
                            long long ntiles, size_t smem) {
     static int per_sm = -1;
     if (per_sm < 0) {
-        cudaFuncSetAttribute(d2m_stream_kernel<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        allow_max_dynamic_smem(d2m_stream_kernel<MT>);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, d2m_stream_kernel<MT>, kThreads, smem);
         if (per_sm < 1) per_sm = 1;
     }
@@ -455,7 +455,7 @@ int launch_m2d(Handle* h, const double* x, const float* sigl, const double* a, c
     } else {
         static bool attr = false;
         if (!attr) {
-            cudaFuncSetAttribute(m2d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+            allow_max_dynamic_smem(m2d_kernel);
             attr = true;
         }
         const size_t smem = (size_t)3 * kTileN * smem_stride_words(h->nmpad) * 4;

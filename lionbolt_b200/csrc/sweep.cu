@@ -34,9 +34,15 @@ namespace {
 constexpr float kThird = 1.0f / 3.0f;
 constexpr float kFiveThirds = 5.0f / 3.0f;
 constexpr float kFourThirds = 4.0f / 3.0f;
+// Padding entry of the padded sweep order.  Real items can be negative (bit 31 carries the outflow
+// flag of face 3), so padding is recognised by equality; no real item is all ones because element
+// ids stay below 0xFFFFFF.
+constexpr int kPad = -1;
 
 struct SweepArgs {
     const int* __restrict__ items;
+    const int* __restrict__ pitems;
+    const long long* __restrict__ pbase;
     const int4* __restrict__ chunks;
     const int* __restrict__ lvl_start;
     const int* __restrict__ lvl_base;
@@ -89,19 +95,42 @@ struct Update {
 //   T = d I + a 1^T + 1 b^T,  d = sigma + (5/3) Ct,  a_k = (5/3) ci_{3-k},  b_k = (Ct - co_{3-k}) / 3
 // (row k of the convection term is constant, column kp of the outflow term is constant off the
 // diagonal), so the 4x4 solve reduces to a 2x2 one (Sherman-Morrison-Woodbury).
-template <bool kCG>
+struct Geom {
+    float4 gx, gy, gz;
+    int4 gn;
+};
+
+__device__ __forceinline__ Geom load_geom(const float4* __restrict__ geom, int e) {
+    Geom g;
+    g.gx = __ldg(&geom[(size_t)e * 4 + 0]);
+    g.gy = __ldg(&geom[(size_t)e * 4 + 1]);
+    g.gz = __ldg(&geom[(size_t)e * 4 + 2]);
+    g.gn = __ldg(reinterpret_cast<const int4*>(&geom[(size_t)e * 4 + 3]));
+    return g;
+}
+
+template <bool kCG, bool kHaveQ = false>
+__device__ __forceinline__ void assemble_g(const float* base, float4 dir, int item, const Geom& G, const float* s_sigt,
+                                           Update& u, float4 qpre);
+
+template <bool kCG, bool kHaveQ = false>
 __device__ __forceinline__ void assemble(const SweepArgs& a, const float* base, float4 dir, int item,
-                                         const float* s_sigt, Update& u) {
+                                         const float* s_sigt, Update& u, float4 qpre = make_float4(0.f, 0.f, 0.f, 0.f)) {
+    const Geom G = load_geom(a.geom, item & 0xFFFFFF);
+    assemble_g<kCG, kHaveQ>(base, dir, item, G, s_sigt, u, qpre);
+}
+
+template <bool kCG, bool kHaveQ>
+__device__ __forceinline__ void assemble_g(const float* base, float4 dir, int item, const Geom& G, const float* s_sigt,
+                                           Update& u, float4 qpre) {
     // gmsh face -> local nodes; the vertex opposite face f is 3 - f
     constexpr int F[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
     const int e = item & 0xFFFFFF;
     const int upm = (item >> 24) & 0xF;
     const int outm = (item >> 28) & 0xF;
-    const float4 gx = __ldg(&a.geom[(size_t)e * 4 + 0]);
-    const float4 gy = __ldg(&a.geom[(size_t)e * 4 + 1]);
-    const float4 gz = __ldg(&a.geom[(size_t)e * 4 + 2]);
-    const int4 gn = __ldg(reinterpret_cast<const int4*>(&a.geom[(size_t)e * 4 + 3]));
-    const float4 q = ld4<kCG>(base + 4 * (size_t)e);
+    const float4 gx = G.gx, gy = G.gy, gz = G.gz;
+    const int4 gn = G.gn;
+    const float4 q = kHaveQ ? qpre : ld4<kCG>(base + 4 * (size_t)e);
     float c[4];
     c[0] = fmaf(dir.x, gx.x, fmaf(dir.y, gy.x, dir.z * gz.x));
     c[1] = fmaf(dir.x, gx.y, fmaf(dir.y, gy.y, dir.z * gz.y));
@@ -225,6 +254,256 @@ __global__ void __launch_bounds__(ILP == 1 ? 1024 : 512) sweep_levels_kernel(Swe
     }
 }
 
+// Level-synchronous schedule with the next level's first item and source prefetched before the CTA
+// barrier (they do not depend on the current level), so after the barrier only the geometry and
+// the upstream values are waited for.  MINB = 2 asks for two 1024-thread CTAs per SM (32 registers).
+template <int MINB>
+__global__ void __launch_bounds__(1024, MINB) sweep_levels_pf_kernel(SweepArgs a) {
+    __shared__ float s_sigt[256];
+    load_sigt(a, s_sigt);
+    const int nt = blockDim.x;
+    for (int i = blockIdx.x; i < a.NI; i += gridDim.x) {
+        const int nl = __ldg(&a.nlev[i]);
+        const int lb = __ldg(&a.lvl_base[i]);
+        const float4 dir = __ldg(&a.dirs[i]);
+        const int* it = a.items + (size_t)i * a.NE;
+        float* base = a.psi + (size_t)i * (size_t)a.NENK;
+        int s0 = __ldg(&a.lvl_start[lb]);
+        int s1 = __ldg(&a.lvl_start[lb + 1]);
+        // prefetched first update of this thread in the current level
+        int pitem = (s0 + (int)threadIdx.x < s1) ? __ldcs(&it[s0 + threadIdx.x]) : 0;
+        float4 pq = (s0 + (int)threadIdx.x < s1) ? *reinterpret_cast<const float4*>(base + 4 * (size_t)(pitem & 0xFFFFFF))
+                                                 : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int L = 0; L < nl; ++L) {
+            const int es0 = s0 + threadIdx.x;
+            const int cur_item = pitem;
+            const float4 cur_q = pq;
+            // next level bounds and prefetch (independent of this level's results)
+            const int n0 = s1;
+            const int n1 = (L + 1 < nl) ? __ldg(&a.lvl_start[lb + L + 2]) : s1;
+            if (n0 + (int)threadIdx.x < n1) {
+                pitem = __ldcs(&it[n0 + threadIdx.x]);
+                pq = *reinterpret_cast<const float4*>(base + 4 * (size_t)(pitem & 0xFFFFFF));
+            }
+            if (es0 < s1) {
+                Update up;
+                assemble<false, true>(a, base, dir, cur_item, s_sigt, up, cur_q);
+                finish<false>(base, cur_item, up);
+            }
+            for (int es = es0 + nt; es < s1; es += nt) {
+                const int item = __ldcs(&it[es]);
+                Update up;
+                assemble<false>(a, base, dir, item, s_sigt, up);
+                finish<false>(base, item, up);
+            }
+            s0 = n0;
+            s1 = n1;
+            __syncthreads();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Element-flag schedule: one CTA per direction, no barriers between levels.  Warps claim 32-element
+// chunks of the direction's padded sweep order (levels padded to multiples of 32, so a chunk's
+// elements are mutually independent) from a shared counter, prefetch the next chunk's items,
+// geometry and source, and wait -- bounded -- only for the done bits of their own upstream
+// neighbours (one bit per element in shared memory).  Claims are made in sweep order and every
+// dependency lies earlier in that order, so the earliest unfinished chunk can always proceed.
+// ---------------------------------------------------------------------------------------------
+template <int NT>
+__global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 2) sweep_flags_kernel(SweepArgs a) {
+    extern __shared__ uint32_t s_done[];                      // one bit per element of the mesh
+    __shared__ float s_sigt[256];
+    __shared__ int s_next;
+    __shared__ int s_abort;
+    __shared__ int s_ndone, s_nexit;
+    load_sigt(a, s_sigt);
+    const int lane = threadIdx.x & 31;
+    const int nwords = (a.NE + 31) >> 5;
+    volatile uint32_t* vdone = s_done;
+    for (int i = blockIdx.x; i < a.NI; i += gridDim.x) {
+        for (int w = threadIdx.x; w < nwords; w += NT) s_done[w] = 0u;
+        if (threadIdx.x == 0) { s_next = 0; s_abort = 0; s_ndone = 0; s_nexit = 0; }
+        __syncthreads();
+        const long long pb = __ldg(&a.pbase[i]);
+        const int len = (int)(__ldg(&a.pbase[i + 1]) - pb);
+        const int* pit = a.pitems + pb;
+        const float4 dir = __ldg(&a.dirs[i]);
+        float* base = a.psi + (size_t)i * (size_t)a.NENK;
+        int c = 0;
+        if (lane == 0) c = atomicAdd(&s_next, 32);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        int item = -1;
+        Geom G;
+        float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (c < len) {
+            item = __ldcs(&pit[c + lane]);
+            if (item != kPad) { G = load_geom(a.geom, item & 0xFFFFFF); q = *reinterpret_cast<const float4*>(base + 4 * (size_t)(item & 0xFFFFFF)); }
+        }
+        while (c < len) {
+            int cn = 0;
+            if (lane == 0) cn = atomicAdd(&s_next, 32);
+            cn = __shfl_sync(0xffffffffu, cn, 0);
+            int nitem = -1;
+            Geom NG;
+            float4 nq = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (cn < len) {
+                nitem = __ldcs(&pit[cn + lane]);
+                if (nitem != kPad) { NG = load_geom(a.geom, nitem & 0xFFFFFF); nq = *reinterpret_cast<const float4*>(base + 4 * (size_t)(nitem & 0xFFFFFF)); }
+            }
+            bool ok = true;
+            if (item != kPad) {
+                // wait for the upstream neighbours of this element
+                const int upm = (item >> 24) & 0xF;
+                const unsigned nw[4] = {(unsigned)G.gn.x, (unsigned)G.gn.y, (unsigned)G.gn.z, (unsigned)G.gn.w};
+                long long spins = 0;
+                int waited = -1;
+#pragma unroll
+                for (int f = 0; f < 4; ++f) {
+                    if (!((upm >> f) & 1)) continue;
+                    const int ep = (int)(nw[f] & 0xFFFFFFu);
+                    const uint32_t bit = 1u << (ep & 31);
+                    while (!(vdone[ep >> 5] & bit)) {
+                        if (++spins > a.spin_limit || *((volatile int*)&s_abort)) { ok = false; waited = ep; break; }
+                        __nanosleep(32);
+                    }
+                    if (!ok) break;
+                }
+                if (ok) {
+                    __threadfence_block();
+                    Update u;
+                    assemble_g<false, true>(base, dir, item, G, s_sigt, u, q);
+                    finish<false>(base, item, u);
+                    __threadfence_block();
+                    const int e = item & 0xFFFFFF;
+                    atomicOr(&s_done[e >> 5], 1u << (e & 31));
+                    atomicAdd(&s_ndone, 1);
+                } else if (atomicExch(&s_abort, 1) == 0) {
+                    if (atomicExch(&a.status->abort, 1) == 0) {
+                        a.status->err = LB_ERR_TIMEOUT;
+                        a.status->err_chunk = i;
+                        a.status->err_elem = item & 0xFFFFFF;
+                        a.status->err_dep = waited;
+                        a.status->err_pos = c;
+                        a.status->err_bit = waited >= 0 ? (int)((vdone[waited >> 5] >> (waited & 31)) & 1u) : -1;
+                        a.status->dbg_next = *((volatile int*)&s_next);
+                        a.status->dbg_done = *((volatile int*)&s_ndone);
+                        a.status->dbg_exited = *((volatile int*)&s_nexit);
+                        a.status->dbg_len = len;
+                    }
+                }
+            }
+            if (__any_sync(0xffffffffu, !ok) || *((volatile int*)&s_abort)) break;
+            c = cn;
+            item = nitem;
+            G = NG;
+            q = nq;
+        }
+        if (lane == 0) atomicAdd(&s_nexit, 1);
+        __syncthreads();
+        if (*((volatile int*)&s_abort)) return;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Grouped level schedule: directions whose schedules are bit-identical (same order and same face
+// masks for every element) are walked together.  Each element's item and geometry are loaded once
+// for the group, the group's source and upstream values are all requested before any of its
+// updates is computed, so the memory latency of one element is paid once for G directions.
+// groups: per CTA work item {representative direction, count, d0 .. d5}.
+// ---------------------------------------------------------------------------------------------
+template <int G>
+__device__ __forceinline__ void group_update(const SweepArgs& a, float* const* base, const float4* dir, int n, int item,
+                                             const float* s_sigt) {
+    constexpr int F[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
+    const int e = item & 0xFFFFFF;
+    const int upm = (item >> 24) & 0xF;
+    const int outm = (item >> 28) & 0xF;
+    const Geom g = load_geom(a.geom, e);
+    const unsigned nw[4] = {(unsigned)g.gn.x, (unsigned)g.gn.y, (unsigned)g.gn.z, (unsigned)g.gn.w};
+    // request every direction's source and upstream values first
+    float4 q[G], up[G][4];
+#pragma unroll
+    for (int j = 0; j < G; ++j) {
+        if (j >= n) break;
+        q[j] = *reinterpret_cast<const float4*>(base[j] + 4 * (size_t)e);
+#pragma unroll
+        for (int f = 0; f < 4; ++f)
+            if ((upm >> f) & 1) up[j][f] = *reinterpret_cast<const float4*>(base[j] + 4 * (size_t)(nw[f] & 0xFFFFFFu));
+    }
+    const int matid = (int)((nw[0] >> 30) | ((nw[1] >> 30) << 2) | ((nw[2] >> 30) << 4) | ((nw[3] >> 30) << 6));
+    const float sig = s_sigt[matid];
+#pragma unroll
+    for (int j = 0; j < G; ++j) {
+        if (j >= n) break;
+        const float4 d = dir[j];
+        float c[4];
+        c[0] = fmaf(d.x, g.gx.x, fmaf(d.y, g.gy.x, d.z * g.gz.x));
+        c[1] = fmaf(d.x, g.gx.y, fmaf(d.y, g.gy.y, d.z * g.gz.y));
+        c[2] = fmaf(d.x, g.gx.z, fmaf(d.y, g.gy.z, d.z * g.gz.z));
+        c[3] = fmaf(d.x, g.gx.w, fmaf(d.y, g.gy.w, d.z * g.gz.w));
+        Update u;
+        u.r[0] = q[j].x; u.r[1] = q[j].y; u.r[2] = q[j].z; u.r[3] = q[j].w;
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+            if ((upm >> f) & 1) {
+                const unsigned wd = nw[f];
+                const float u0 = pick(up[j][f], (wd >> 24) & 3);
+                const float u1 = pick(up[j][f], (wd >> 26) & 3);
+                const float u2 = pick(up[j][f], (wd >> 28) & 3);
+                const float U = u0 + u1 + u2;
+                const float cf = c[f];
+                const float t3 = U * kThird;
+                u.r[F[f][0]] = fmaf(-cf, fmaf(kFiveThirds, u0, t3), u.r[F[f][0]]);
+                u.r[F[f][1]] = fmaf(-cf, fmaf(kFiveThirds, u1, t3), u.r[F[f][1]]);
+                u.r[F[f][2]] = fmaf(-cf, fmaf(kFiveThirds, u2, t3), u.r[F[f][2]]);
+                u.r[3 - f] = fmaf(cf * kFourThirds, U, u.r[3 - f]);
+            }
+        }
+        float co[4];
+#pragma unroll
+        for (int f = 0; f < 4; ++f) co[f] = ((outm >> f) & 1) ? c[f] : 0.0f;
+        const float Ct = (co[0] + co[1]) + (co[2] + co[3]);
+        u.d = fmaf(kFiveThirds, Ct, sig);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            u.a[k] = kFiveThirds * (c[3 - k] - co[3 - k]);
+            u.b[k] = (Ct - co[3 - k]) * kThird;
+        }
+        solve_rank2(u);
+        *reinterpret_cast<float4*>(base[j] + 4 * (size_t)e) = make_float4(u.r[0], u.r[1], u.r[2], u.r[3]);
+    }
+}
+
+template <int G, int NT>
+__global__ void __launch_bounds__(NT, 1) sweep_group_kernel(SweepArgs a, const int* __restrict__ groups, int ngroups) {
+    __shared__ float s_sigt[256];
+    load_sigt(a, s_sigt);
+    for (int gi = blockIdx.x; gi < ngroups; gi += gridDim.x) {
+        const int* gr = groups + (size_t)gi * 8;
+        const int rep = __ldg(&gr[0]);
+        const int n = __ldg(&gr[1]);
+        float* base[G];
+        float4 dir[G];
+#pragma unroll
+        for (int j = 0; j < G; ++j) {
+            const int i = (j < n) ? __ldg(&gr[2 + j]) : rep;
+            base[j] = a.psi + (size_t)i * (size_t)a.NENK;
+            dir[j] = __ldg(&a.dirs[i]);
+        }
+        const int nl = __ldg(&a.nlev[rep]);
+        const int lb = __ldg(&a.lvl_base[rep]);
+        const int* it = a.items + (size_t)rep * a.NE;
+        for (int L = 0; L < nl; ++L) {
+            const int s0 = __ldg(&a.lvl_start[lb + L]);
+            const int s1 = __ldg(&a.lvl_start[lb + L + 1]);
+            for (int es = s0 + threadIdx.x; es < s1; es += NT) group_update<G>(a, base, dir, n, __ldcs(&it[es]), s_sigt);
+            __syncthreads();
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------------------------
 // Dataflow schedule: global chunk queue with bounded waits on per-level completion counters.
 // ---------------------------------------------------------------------------------------------
@@ -277,15 +556,15 @@ __global__ void __launch_bounds__(256) sweep_dataflow_kernel(SweepArgs a) {
 }
 
 struct Config {
-    int kind;      // 0 levels, 1 dataflow
+    int kind;      // 0 levels, 1 dataflow, 2 levels with next-level prefetch, 3 element flags, 4 grouped levels
     int threads;
-    int dpc;
+    int dpc;       // directions per CTA (kind 0); minimum CTAs per SM (kind 2)
     int ilp;
 };
 
 const Config kConfigs[] = {
-    {0, 512, 1, 1}, {0, 512, 1, 2}, {0, 768, 1, 1}, {0, 640, 1, 1}, {0, 1024, 1, 1},
-    {0, 256, 1, 2}, {0, 512, 2, 1}, {0, 512, 2, 2}, {0, 1024, 2, 1}, {1, 256, 0, 0},
+    {4, 1024, 2, 1}, {4, 512, 2, 1}, {4, 512, 3, 1}, {4, 1024, 3, 1}, {4, 512, 6, 1},
+    {0, 1024, 1, 1}, {0, 512, 1, 1}, {2, 1024, 1, 1}, {3, 512, 0, 1}, {1, 256, 0, 0},
 };
 constexpr int kNumConfigs = sizeof(kConfigs) / sizeof(kConfigs[0]);
 
@@ -300,11 +579,80 @@ cudaError_t launch_levels(const SweepArgs& a, int threads, int sm_count, cudaStr
     return cudaGetLastError();
 }
 
+template <int G, int NT>
+cudaError_t launch_group(const SweepArgs& a, const int* groups, int ngroups, int sm_count, cudaStream_t s) {
+    static int per_sm = -1;
+    if (per_sm < 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_group_kernel<G, NT>, NT, 0);
+        if (per_sm < 1) per_sm = 1;
+    }
+    int grid = std::min(ngroups, sm_count * per_sm);
+    sweep_group_kernel<G, NT><<<grid, NT, 0, s>>>(a, groups, ngroups);
+    return cudaGetLastError();
+}
+
+// per-CTA groups of at most gmax directions with identical schedules
+int build_groups(Handle* h, int gmax) {
+    if (h->groups_gmax == gmax && h->d_groups) return LB_OK;
+    std::vector<int> gr;
+    int ng = 0;
+    for (size_t c = 0; c + 1 < h->class_start.size(); ++c) {
+        const int a0 = h->class_start[c], a1 = h->class_start[c + 1];
+        for (int s = a0; s < a1; s += gmax) {
+            const int n = std::min(gmax, a1 - s);
+            int rec[8] = {h->class_members[a0], n, 0, 0, 0, 0, 0, 0};
+            for (int j = 0; j < n; ++j) rec[2 + j] = h->class_members[s + j];
+            gr.insert(gr.end(), rec, rec + 8);
+            ++ng;
+        }
+    }
+    if (h->d_groups) { cudaFree(h->d_groups); h->d_groups = nullptr; }
+    cudaError_t e = cudaMalloc(&h->d_groups, sizeof(int) * gr.size());
+    if (e == cudaSuccess) e = cudaMemcpy(h->d_groups, gr.data(), sizeof(int) * gr.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(h, e, "sweep groups");
+    h->groups_gmax = gmax;
+    h->ngroups = ng;
+    const char* verbose = std::getenv("LB_SWEEP_VERBOSE");
+    if (verbose && *verbose == '1')
+        std::fprintf(stderr, "sweep: %d directions in %zu schedule classes -> %d groups of <= %d\n", h->NI,
+                     h->class_start.size() - 1, ng, gmax);
+    return LB_OK;
+}
+
+template <int NT>
+cudaError_t launch_flags(const SweepArgs& a, int sm_count, cudaStream_t s) {
+    const size_t smem = sizeof(uint32_t) * (size_t)((a.NE + 31) / 32);
+    if (smem > 200 * 1024) return cudaErrorInvalidConfiguration;
+    static int per_sm = -1;
+    static size_t last_smem = 0;
+    if (per_sm < 0 || last_smem != smem) {
+        allow_max_dynamic_smem(sweep_flags_kernel<NT>);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_flags_kernel<NT>, NT, smem);
+        if (per_sm < 1) per_sm = 1;
+        last_smem = smem;
+    }
+    int grid = std::min(a.NI, sm_count * per_sm);
+    sweep_flags_kernel<NT><<<grid, NT, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int MINB>
+cudaError_t launch_levels_pf(const SweepArgs& a, int threads, int sm_count, cudaStream_t s) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_levels_pf_kernel<MINB>, threads, 0);
+    if (per_sm < 1) per_sm = 1;
+    int grid = std::min(a.NI, sm_count * per_sm);
+    sweep_levels_pf_kernel<MINB><<<grid, threads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 int launch_sweep(Handle* h, float* psi) {
     SweepArgs a;
     a.items = h->d_items;
+    a.pitems = h->d_pitems;
+    a.pbase = h->d_pbase;
     a.chunks = h->d_chunks;
     a.lvl_start = h->d_lvl_start;
     a.lvl_base = h->d_lvl_base;
@@ -333,17 +681,58 @@ int launch_sweep(Handle* h, float* psi) {
     if (h->sweep_cfg_forced < kNumConfigs) cfg_idx = h->sweep_cfg_forced;
     else if (h->sweep_cfg >= 0) cfg_idx = h->sweep_cfg;
     else { cfg_idx = h->sweep_trial; tuning = true; }
-    const Config cfg = kConfigs[cfg_idx];
+    if (tuning && h->sweep_trial == 0) {
+        // load every candidate's module before timing, so the first trial does not pay for it
+        cudaFuncAttributes fa;
+        cudaFuncGetAttributes(&fa, sweep_group_kernel<2, 1024>);
+        cudaFuncGetAttributes(&fa, sweep_group_kernel<2, 512>);
+        cudaFuncGetAttributes(&fa, sweep_group_kernel<3, 1024>);
+        cudaFuncGetAttributes(&fa, sweep_group_kernel<3, 512>);
+        cudaFuncGetAttributes(&fa, sweep_group_kernel<6, 512>);
+        cudaFuncGetAttributes(&fa, sweep_flags_kernel<256>);
+        cudaFuncGetAttributes(&fa, sweep_flags_kernel<512>);
+        cudaFuncGetAttributes(&fa, sweep_flags_kernel<1024>);
+        cudaFuncGetAttributes(&fa, sweep_levels_pf_kernel<1>);
+        cudaFuncGetAttributes(&fa, sweep_levels_pf_kernel<2>);
+        cudaFuncGetAttributes(&fa, sweep_levels_kernel<1, 1>);
+        cudaFuncGetAttributes(&fa, sweep_levels_kernel<1, 2>);
+        cudaFuncGetAttributes(&fa, sweep_levels_kernel<2, 1>);
+        cudaFuncGetAttributes(&fa, sweep_levels_kernel<2, 2>);
+        cudaFuncGetAttributes(&fa, sweep_dataflow_kernel);
+    }
+    Config cfg = kConfigs[cfg_idx];
+    // the element-flag schedule keeps one bit per element in shared memory
+    if (cfg.kind == 3 && (size_t)((h->NE + 31) / 32) * 4 > 200 * 1024) cfg = Config{0, 1024, 1, 1};
 
     cudaError_t e = cudaSuccess;
     if (cfg.kind == 1) {
         e = cudaMemsetAsync(h->d_done, 0, sizeof(int) * (size_t)h->total_levels, h->stream);
-        if (e == cudaSuccess) e = cudaMemsetAsync(h->d_status, 0, sizeof(SweepStatus), h->stream);
         if (e != cudaSuccess) return cuda_fail(h, e, "sweep: reset counters");
+    }
+    if (cfg.kind == 1 || cfg.kind == 3) {
+        e = cudaMemsetAsync(h->d_status, 0, sizeof(SweepStatus), h->stream);
+        if (e != cudaSuccess) return cuda_fail(h, e, "sweep: reset status");
+    }
+    if (cfg.kind == 4) {
+        int rc = build_groups(h, cfg.dpc);
+        if (rc) return rc;
     }
     Timer t;
     timer_begin(h, LB_T_SWEEP, t);
-    if (cfg.kind == 1) {
+    if (cfg.kind == 4) {
+        if (cfg.dpc == 2) e = cfg.threads == 1024 ? launch_group<2, 1024>(a, h->d_groups, h->ngroups, h->sm_count, h->stream)
+                                                  : launch_group<2, 512>(a, h->d_groups, h->ngroups, h->sm_count, h->stream);
+        else if (cfg.dpc == 3) e = cfg.threads == 1024 ? launch_group<3, 1024>(a, h->d_groups, h->ngroups, h->sm_count, h->stream)
+                                                       : launch_group<3, 512>(a, h->d_groups, h->ngroups, h->sm_count, h->stream);
+        else e = launch_group<6, 512>(a, h->d_groups, h->ngroups, h->sm_count, h->stream);
+    } else if (cfg.kind == 3) {
+        e = (cfg.threads == 256) ? launch_flags<256>(a, h->sm_count, h->stream)
+          : (cfg.threads == 1024) ? launch_flags<1024>(a, h->sm_count, h->stream)
+                                  : launch_flags<512>(a, h->sm_count, h->stream);
+    } else if (cfg.kind == 2) {
+        e = (cfg.dpc == 2) ? launch_levels_pf<2>(a, cfg.threads, h->sm_count, h->stream)
+                           : launch_levels_pf<1>(a, cfg.threads, h->sm_count, h->stream);
+    } else if (cfg.kind == 1) {
         static int df_per_sm = -1;
         if (df_per_sm < 0) {
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&df_per_sm, sweep_dataflow_kernel, 256, 0);
@@ -357,14 +746,20 @@ int launch_sweep(Handle* h, float* psi) {
     else e = launch_levels<2, 2>(a, cfg.threads, h->sm_count, h->stream);
     timer_end(h, t);
     if (e != cudaSuccess) return cuda_fail(h, e, "sweep kernel launch");
-    if (cfg.kind == 1) {
+    if (cfg.kind == 1 || cfg.kind == 3) {
         SweepStatus st;
         e = cudaMemcpyAsync(&st, h->d_status, sizeof(st), cudaMemcpyDeviceToHost, h->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
         if (e != cudaSuccess) return cuda_fail(h, e, "sweep kernel");
         if (st.err) {
-            char buf[160];
-            std::snprintf(buf, sizeof buf, "sweep: dependency wait timed out at chunk %d", st.err_chunk);
+            char buf[256];
+            if (cfg.kind == 3)
+                std::snprintf(buf, sizeof buf, "sweep: dependency wait timed out in direction %d: element %d waited for "
+                              "element %d (bit %d), chunk at %d; claimed %d of %d, completed %d, warps exited %d",
+                              st.err_chunk, st.err_elem, st.err_dep, st.err_bit, st.err_pos, st.dbg_next, st.dbg_len,
+                              st.dbg_done, st.dbg_exited);
+            else
+                std::snprintf(buf, sizeof buf, "sweep: dependency wait timed out at chunk %d", st.err_chunk);
             return fail(h, LB_ERR_TIMEOUT, buf);
         }
     }
@@ -456,6 +851,8 @@ extern "C" int lb_transport_inv_noalloc(lb_handle* hh, float* psi) {
     int* base = static_cast<int*>(g_noalloc_ptr[h->device]);
     SweepArgs a;
     a.items = h->d_items;
+    a.pitems = h->d_pitems;
+    a.pbase = h->d_pbase;
     a.chunks = h->d_chunks;
     a.lvl_start = h->d_lvl_start;
     a.lvl_base = h->d_lvl_base;

@@ -58,6 +58,21 @@ def test_transport_inverse_matches_oracle(case):
     assert T.timers()["sweep"][1] >= 1
 
 
+@pytest.mark.parametrize("cfg", range(10))
+def test_every_sweep_schedule_matches_oracle(cfg, monkeypatch):
+    """Each launch candidate of the sweep autotuner (levels, prefetching levels, element flags,
+    dataflow) reproduces the oracle's T^{-1} on a two-material mesh."""
+    monkeypatch.setenv("LB_SWEEP_CONFIG", str(cfg))
+    m, (k, w), sigt, sigs = SWEEP_CASES["two_material"]()
+    o, ang, xs = _pair(m, k, w, sigt, sigs)
+    T = TransportOp().Build(m, ang, xs)
+    q = np.random.default_rng(cfg).uniform(0.0, 1.0, size=m.NENK * k.shape[0])
+    ref = o.transport_inv(q)
+    out = q.copy()
+    T.MatInv(out)
+    assert rel_l2(out, ref) < TOL
+
+
 def test_transport_mms_matches_oracle():
     m = M.box_mesh(6, 6, 6, (-1, -1, -1), (1, 1, 1))
     k, w = P.quadrature(4, 8)
