@@ -41,7 +41,29 @@ def parse():
     p.add_argument("--rtol", type=float, default=1e-6)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=20.0)
+    p.add_argument("--mesh", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
+                   help="hexes per axis of a reduced box with the same physics (profiling cases)")
+    p.add_argument("--groups", type=int, default=None, help="energy groups of the reduced box")
+    p.add_argument("--no-learned", action="store_true",
+                   help="skip the learned-preconditioner FGMRES comparison (training + timed solves)")
+    p.add_argument("--lp-problems", type=int, default=3, help="training problems (seeded cross sections / slab)")
+    p.add_argument("--lp-samples", type=int, default=2000, help="training samples per group and problem")
+    p.add_argument("--lp-steps", type=int, default=1500, help="Adam steps")
+    p.add_argument("--profile-range", action="store_true",
+                   help="bracket the device-timed steps with cudaProfilerStart/Stop (ncu --profile-from-start off)")
     return p.parse_args()
+
+
+def workload(args):
+    """The benchmarked problem: config1 (768,000 tets, 288 directions, 20 groups) unless reduced."""
+    from lionbolt_b200 import problems as P
+    if args.mesh is None and args.groups is None:
+        return P.config1(), "config1 multigroup dose solve: 768000 tets x 288 dirs x 20 groups, P5"
+    n = tuple(args.mesh) if args.mesh else (40, 40, 80)
+    G = args.groups or 20
+    prob = P.multigroup_box(n=n, size=(0.5 * n[0], 0.5 * n[1], 0.5 * n[2]), G=G,
+                            slab=(5.0 * n[2] / 80, 7.0 * n[2] / 80), name=f"box{n}")
+    return prob, (f"reduced config1 physics (profiling case): {prob.mesh.NE} tets x 288 dirs x {G} groups, P5")
 
 
 def dist_env():
@@ -181,6 +203,56 @@ def cpu_sample(prob, threads, budget_s):
                               sweep_dirs=len(sel), scatter_nodes=o_sub.NENK)
 
 
+def training_problem(args, k):
+    """Training problem k of the learned preconditioner: the benchmarked geometry with other seeded
+    cross sections and another slab position."""
+    from lionbolt_b200 import problems as P
+    n = tuple(args.mesh) if args.mesh else (40, 40, 80)
+    depth = 0.5 * n[2]
+    z0 = depth * (0.08 + 0.25 * k)
+    return P.multigroup_box(n=n, size=(0.5 * n[0], 0.5 * n[1], depth), G=args.groups or 20, seed=1000 + k,
+                            slab=(z0, z0 + 0.05 * depth), name=f"train{k}")
+
+
+def learned_comparison(args, mg, device, barrier, gmres_ms, gmres_dose):
+    """Train the per-cell network on plain-solver data (untimed), then time FGMRES with it on the
+    benchmarked problem; the plain-GMRES dose judges its answer."""
+    from lionbolt_b200 import MultigroupSolver
+    t0 = time.perf_counter()
+    tr = MultigroupSolver(device=device)
+    tr.lp_init(seed=7)
+    total = 0
+    for k in range(args.lp_problems):
+        tr.set_problem(training_problem(args, k))
+        total = tr.lp_generate(samples_per_group=args.lp_samples, iters=8, seed=total + 1)
+    t_gen = time.perf_counter() - t0
+    loss = tr.lp_train(steps=args.lp_steps, batch=2048, lr=3e-3, seed=11)
+    w = tr.lp_get_weights()
+    tr.Destroy()
+    t_train = time.perf_counter() - t0 - t_gen
+    mg.lp_set_weights(w)
+    h = mg._h
+    warm = min(args.warmup, 1)
+    for _ in range(warm):
+        mg.solve("FGMRES_ML", m=args.m, rtol=args.rtol, atol=0.0)
+    barrier()
+    h.mark(2)
+    it = None
+    for _ in range(args.steps):
+        it = mg.solve("FGMRES_ML", m=args.m, rtol=args.rtol, atol=0.0)
+    h.mark(3)
+    ml_ms = h.elapsed_ms(2, 3) / args.steps
+    _, dose = mg.results()
+    mg.lp_enable(False)
+    rel = float(np.linalg.norm(dose - gmres_dose) / max(np.linalg.norm(gmres_dose), 1e-300))
+    return {"solver": f"FGMRES({args.m}) + per-cell MLP right preconditioner", "time_to_dose_s": ml_ms / 1e3,
+            "speedup_vs_gmres": gmres_ms / ml_ms, "iterations_per_group": [int(x) for x in it],
+            "dose_rel_l2_vs_gmres": rel, "warmup": warm, "steps": args.steps,
+            "training": {"problems": args.lp_problems, "samples": int(total), "adam_steps": int(args.lp_steps),
+                         "loss_first20": float(np.mean(loss[:20])), "loss_last50": float(np.mean(loss[-50:])),
+                         "generate_s": t_gen, "train_s": t_train}}
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -226,7 +298,7 @@ def run_ours(args):
     from lionbolt_b200 import _lib
     from lionbolt_b200 import problems as P
 
-    prob = P.config1()
+    prob, wl = workload(args)
     mg = MultigroupSolver(device=local).set_problem(prob)
     h = mg._h
 
@@ -247,11 +319,15 @@ def run_ours(args):
     h.reset_timers()
     iters = None
     with ClockSampler(local) as clocks:
+        if args.profile_range:
+            torch.cuda.profiler.start()
         h.mark(0)
         for _ in range(args.steps):
             iters = step()
         h.mark(1)
         dev_ms = h.elapsed_ms(0, 1)
+        if args.profile_range:
+            torch.cuda.profiler.stop()
     barrier()
     tm = h.timers()
     launches = int(sum(v[1] for v in tm.values()))
@@ -299,6 +375,11 @@ def run_ours(args):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_s = float(t.item())
     e2e_value = world * args.steps / e2e_s
+    gmres_dose = h_dose.numpy().copy()
+
+    learned = None
+    if not args.no_learned and args.solver == "GMRES":
+        learned = learned_comparison(args, mg, local, barrier, ms_per_step, gmres_dose)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -314,8 +395,7 @@ def run_ours(args):
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32 sweep / split-bf16 tensor-core moments / f64 Krylov",
                 "data": "synthetic",
-                "config": {"workload": "config1 multigroup dose solve: 768000 tets x 288 dirs x 20 groups, P5, "
-                                       f"{args.solver}({args.m}) to {args.rtol:g}",
+                "config": {"workload": f"{wl}, {args.solver}({args.m}) to {args.rtol:g}",
                            "parallelism": f"replicas x{world}", "l2": "inputs > L2 (3.5 GB angular vector)"},
                 "time_to_dose_s": ms_per_step / 1e3,
                 "iterations_per_group": [int(x) for x in iters],
@@ -329,7 +409,8 @@ def run_ours(args):
                 "gpu_launches": launches,
                 "clocks": clocks.summary(),
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-                "cpu_baseline": cpu}
+                "cpu_baseline": cpu,
+                "learned_preconditioner": learned}
         print(json.dumps(line), flush=True)
     mg.Destroy()
     if world > 1:

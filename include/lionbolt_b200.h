@@ -161,6 +161,45 @@ int lb_synchronize(lb_handle* h);
  * LB_ERR_STATE while candidates are still being timed (the first sweeps of a handle). */
 int lb_get_sweep_config(lb_handle* h, int* cfg);
 
+
+/* ---- Learned right preconditioner (no counterpart in the reference) ------------------------------
+ * A per-cell MLP (19 -> 64 -> 64 -> 16, ReLU, 6,480 parameters, BF16 weights and activations with
+ * FP32 accumulation) used by LB_SOLVER_FGMRES_ML as the right preconditioner of FGMRES(m).  For a
+ * moment vector v it reads, per cell, the 16 cell-averaged moments j < 16 scaled by their RMS s,
+ * sigma_t*ell, sigma_s0*ell and sigma_s0/sigma_t (ell = 4V/S, the mean chord) and returns
+ * z = v + s * net(x) on the cell's nodes for j < 16 (z = v for j >= 16).  Parameter layout (FP32):
+ * W1[64][19], b1[64], W2[64][64], b2[64], W3[16][64], b3[16].  Without weights, or when disabled,
+ * LB_SOLVER_FGMRES_ML runs plain GMRES; with weights the learned iterate is judged by its true
+ * residual and finished with plain GMRES when it misses the tolerance. */
+int lb_lp_nparams(void);
+/* He-uniform initialisation from `seed` (output layer scaled by 0.1); enables the network. */
+int lb_lp_init(lb_handle* h, unsigned long long seed);
+int lb_lp_set_weights(lb_handle* h, const float* w);
+int lb_lp_get_weights(lb_handle* h, float* w);
+/* on = 0 makes LB_SOLVER_FGMRES_ML run plain GMRES while keeping the weights. */
+int lb_lp_enable(lb_handle* h, int on);
+/* y[n][16] = net(x[n][19]) on the device (tensor-core inference kernel). */
+int lb_lp_forward(lb_handle* h, int n, const float* x, float* y);
+/* z = preconditioner(v) for host moment vectors v, z [nm][NENK] with the current cross sections. */
+int lb_lp_apply(lb_handle* h, const double* v, double* z);
+/* Loss 1/(2n) sum_k w_k |net(x_k) - t_k|^2 over n samples (w = NULL: all weights 1) and its
+ * gradient (FP32, parameter layout above). */
+int lb_lp_loss_grad(lb_handle* h, int n, const float* x, const float* t, const float* w, double* loss, float* grad);
+/* Training data from plain-solver runs of the multigroup problem set on the handle: per group a
+ * GMRES reference solve (rtol 1e-10), then `iters` source iterations from the first-flight
+ * moments; samples_per_group cells drawn (seeded) from the (residual, error) pairs of those
+ * iterates are appended to the handle's device-resident training set. */
+int lb_lp_generate(lb_handle* h, int samples_per_group, int iters, unsigned long long seed, long long* total);
+int lb_lp_num_samples(lb_handle* h, long long* n);
+/* x[n][19], t[n][16] and loss weights w[n] of the stored samples (any may be NULL).  A sample's
+ * target is (ebar - rbar)/s for the cell-averaged residual rbar and error ebar, s the RMS of rbar
+ * over the 16 moments; its weight is s^2 over the mean square of the residual field's moments. */
+int lb_lp_get_samples(lb_handle* h, float* x, float* t, float* w);
+int lb_lp_clear_samples(lb_handle* h);
+/* `steps` Adam steps (cosine-decayed learning rate from lr to lr/20) on batches of `batch` samples
+ * drawn from the training set; loss_hist[steps] (optional) receives the batch losses. */
+int lb_lp_train(lb_handle* h, int steps, int batch, double lr, unsigned long long seed, double* loss_hist);
+
 #ifdef __cplusplus
 }
 #endif

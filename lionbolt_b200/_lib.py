@@ -29,6 +29,7 @@ SOLVER_FGMRES_ML = 2
 TIMER_NAMES = ("sweep", "m2d", "d2m", "krylov", "copy", "precond", "tally")
 
 _c_double_p = ctypes.POINTER(ctypes.c_double)
+_c_float_p = ctypes.POINTER(ctypes.c_float)
 _c_int_p = ctypes.POINTER(ctypes.c_int)
 _c_ubyte_p = ctypes.POINTER(ctypes.c_ubyte)
 _c_ll_p = ctypes.POINTER(ctypes.c_longlong)
@@ -66,6 +67,20 @@ SIGNATURES = {
     "lb_mark": (ctypes.c_int, [_vp, ctypes.c_int]),
     "lb_transport_inv_noalloc": (ctypes.c_int, [_vp, ctypes.c_void_p]),
     "lb_elapsed_ms": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _c_double_p]),
+    "lb_lp_nparams": (ctypes.c_int, []),
+    "lb_lp_init": (ctypes.c_int, [_vp, ctypes.c_ulonglong]),
+    "lb_lp_set_weights": (ctypes.c_int, [_vp, _c_float_p]),
+    "lb_lp_get_weights": (ctypes.c_int, [_vp, _c_float_p]),
+    "lb_lp_enable": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "lb_lp_forward": (ctypes.c_int, [_vp, ctypes.c_int, _c_float_p, _c_float_p]),
+    "lb_lp_apply": (ctypes.c_int, [_vp, _c_double_p, _c_double_p]),
+    "lb_lp_loss_grad": (ctypes.c_int, [_vp, ctypes.c_int, _c_float_p, _c_float_p, _c_float_p, _c_double_p,
+                                       _c_float_p]),
+    "lb_lp_generate": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong, _c_ll_p]),
+    "lb_lp_num_samples": (ctypes.c_int, [_vp, _c_ll_p]),
+    "lb_lp_get_samples": (ctypes.c_int, [_vp, _c_float_p, _c_float_p, _c_float_p]),
+    "lb_lp_clear_samples": (ctypes.c_int, [_vp]),
+    "lb_lp_train": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong, _c_double_p]),
 }
 
 _lib = None
@@ -97,6 +112,14 @@ def load():
 
 def dptr(a):
     return a.ctypes.data_as(_c_double_p)
+
+
+def fptr(a):
+    return a.ctypes.data_as(_c_float_p)
+
+
+def as_f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
 
 
 def iptr(a):

@@ -390,6 +390,7 @@ int lb_set_mesh(lb_handle* h, int NE, int NN, const double* rg, const int* node,
     rc = dev_upload(h, &h->d_mat, h->mat.data(), h->mat.size(), "upload materials");
     if (rc) return rc;
     h->mesh_ready = true;
+    ++h->mesh_version;
     h->angle_ready = false;
     h->phys_ready = false;
     return LB_OK;
@@ -569,6 +570,7 @@ int lb_set_xs(lb_handle* h, int Ls, const double* sigt, const double* sigs) {
         if (!(sigt[m] >= 0.0) || !std::isfinite(sigt[m])) return fail(h, LB_ERR_NAN, "lb_set_xs: invalid total cross section");
     h->sigt.assign(sigt, sigt + Nm);
     h->sigs.assign(sigs, sigs + (size_t)Nm * (Ls + 1));
+    ++h->xs_version;
     int nm = (Ls + 1) * (Ls + 1);
     int nmpad = (nm + 15) / 16 * 16;
     bool rebuild = (Ls != h->Ls) || (h->ybuilt_NI != NI);

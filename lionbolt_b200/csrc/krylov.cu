@@ -3,6 +3,7 @@
 // (third_party/SPARSKIT/iters.f: gmres :1901-2206, mgsro :3465-3587) and Main.f90.
 // Reductions are deterministic: fixed grid, per-block partials summed on the host in block order.
 #include "lb_internal.h"
+#include <type_traits>
 
 namespace lb {
 
@@ -19,68 +20,173 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-// partial[b][j] = sum over this block's share of q of V[j][q] * w[q], j < nv.
-// Vectors are read as double2 (n is even: n = nm * NENK with NENK a multiple of 4).
-__global__ void __launch_bounds__(kRedThreads) dots_kernel(const double* __restrict__ V, size_t ldv, int nv,
-                                                          const double* __restrict__ w, size_t n, double* partial) {
-    __shared__ double s[kRedThreads / 32][kMaxDots];
-    double acc[kMaxDots];
-#pragma unroll
-    for (int j = 0; j < kMaxDots; ++j) acc[j] = 0.0;
-    const size_t n2 = n / 2;
-    const double2* w2 = reinterpret_cast<const double2*>(w);
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n2; q += (size_t)gridDim.x * blockDim.x) {
-        const double2 wq = __ldcs(&w2[q]);
-#pragma unroll
-        for (int j = 0; j < kMaxDots; ++j)
-            if (j < nv) {
-                const double2 v = __ldcs(reinterpret_cast<const double2*>(V + (size_t)j * ldv) + q);
-                acc[j] = fma(v.x, wq.x, fma(v.y, wq.y, acc[j]));
-            }
-    }
+constexpr int kPartStride = kMaxDots + 1;   // partial row: NV dots + the squared norm
+
+// Loads in flight per thread: small NV unrolls the element loop instead.
+template <int NV>
+__host__ __device__ constexpr int unroll_for() { return NV < 2 ? 4 : (NV < 6 ? 2 : 1); }
+
+// Block-level reduction of acc[0..NV] into partial[blockIdx.x][0..NV].
+template <int NV>
+__device__ __forceinline__ void block_reduce_store(double (&acc)[NV + 1], double* partial) {
+    __shared__ double s[kRedThreads / 32][NV + 1];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
-    for (int j = 0; j < kMaxDots; ++j) {
-        if (j < nv) {
-            double v = warp_sum(acc[j]);
-            if (lane == 0) s[warp][j] = v;
-        }
+    for (int j = 0; j <= NV; ++j) {
+        const double v = warp_sum(acc[j]);
+        if (lane == 0) s[warp][j] = v;
     }
     __syncthreads();
-    if (threadIdx.x < nv) {
+    if (threadIdx.x <= NV) {
         double v = 0.0;
+#pragma unroll
         for (int k = 0; k < kRedThreads / 32; ++k) v += s[k][threadIdx.x];
-        partial[(size_t)blockIdx.x * kMaxDots + threadIdx.x] = v;
+        partial[(size_t)blockIdx.x * kPartStride + threadIdx.x] = v;
     }
 }
 
-// w -= sum_j c[j] V[j];  partial[b] = sum of w^2 over the block (after the update)
-__global__ void __launch_bounds__(kRedThreads) axpy_norm_kernel(double* w, const double* __restrict__ V, size_t ldv, int nv,
-                                                               Coefs cf, size_t n, double* partial) {
-    __shared__ double s[kRedThreads / 32];
-    double acc = 0.0;
-    const size_t n2 = n / 2;
-    double2* w2 = reinterpret_cast<double2*>(w);
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n2; q += (size_t)gridDim.x * blockDim.x) {
-        double2 v = w2[q];
+// partial[b][j] = V_j . w (j < NV) and partial[b][NV] = w . w over this block's elements.
+// Vectors are read as double2 (n is even: n = nm * NENK with NENK a multiple of 4).
+template <int NV>
+__global__ void __launch_bounds__(kRedThreads) dots_t(const double* __restrict__ V, size_t ldv,
+                                                     const double* __restrict__ w, size_t n2, double* partial) {
+    constexpr int U = unroll_for<NV>();
+    double acc[NV + 1];
 #pragma unroll
-        for (int j = 0; j < kMaxDots; ++j)
-            if (j < nv) {
-                const double2 u = __ldcs(reinterpret_cast<const double2*>(V + (size_t)j * ldv) + q);
-                v.x = fma(-cf.c[j], u.x, v.x);
-                v.y = fma(-cf.c[j], u.y, v.y);
+    for (int j = 0; j <= NV; ++j) acc[j] = 0.0;
+    const double2* w2 = reinterpret_cast<const double2*>(w);
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t q0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q0 < n2; q0 += U * stride) {
+        double2 wq[U], v[U][NV > 0 ? NV : 1];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const size_t q = q0 + u * stride;
+            const bool in = q < n2;
+            wq[u] = in ? __ldcs(w2 + q) : make_double2(0.0, 0.0);
+#pragma unroll
+            for (int j = 0; j < NV; ++j)
+                v[u][j] = in ? __ldcs(reinterpret_cast<const double2*>(V + (size_t)j * ldv) + q) : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+#pragma unroll
+            for (int j = 0; j < NV; ++j) acc[j] = fma(v[u][j].x, wq[u].x, fma(v[u][j].y, wq[u].y, acc[j]));
+            acc[NV] = fma(wq[u].x, wq[u].x, fma(wq[u].y, wq[u].y, acc[NV]));
+        }
+    }
+    block_reduce_store<NV>(acc, partial);
+}
+
+// w <- w - sum_j c_j V_j; partial[b][j] = V_j . w_new (j < NV, when DOTS) and partial[b][NV] =
+// w_new . w_new.  Up to 16 vectors stay in registers between the update and the dots; beyond that
+// the dots re-read the block's elements (L1/L2 hits).
+template <int NV, bool DOTS>
+__global__ void __launch_bounds__(kRedThreads) axpy_dots_t(double* w, const double* __restrict__ V, size_t ldv, Coefs cf,
+                                                          size_t n2, double* partial) {
+    double acc[NV + 1];
+#pragma unroll
+    for (int j = 0; j <= NV; ++j) acc[j] = 0.0;
+    double2* w2 = reinterpret_cast<double2*>(w);
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n2; q += stride) {
+        double2 x = w2[q];
+        if constexpr (NV <= 16) {
+            double2 v[NV > 0 ? NV : 1];
+#pragma unroll
+            for (int j = 0; j < NV; ++j) v[j] = __ldg(reinterpret_cast<const double2*>(V + (size_t)j * ldv) + q);
+#pragma unroll
+            for (int j = 0; j < NV; ++j) {
+                x.x = fma(-cf.c[j], v[j].x, x.x);
+                x.y = fma(-cf.c[j], v[j].y, x.y);
             }
-        w2[q] = v;
-        acc = fma(v.x, v.x, fma(v.y, v.y, acc));
+            w2[q] = x;
+            if constexpr (DOTS) {
+#pragma unroll
+                for (int j = 0; j < NV; ++j) acc[j] = fma(v[j].x, x.x, fma(v[j].y, x.y, acc[j]));
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < NV; ++j) {
+                const double2 v = __ldg(reinterpret_cast<const double2*>(V + (size_t)j * ldv) + q);
+                x.x = fma(-cf.c[j], v.x, x.x);
+                x.y = fma(-cf.c[j], v.y, x.y);
+            }
+            w2[q] = x;
+            if constexpr (DOTS) {
+#pragma unroll
+                for (int j = 0; j < NV; ++j) {
+                    const double2 v = __ldg(reinterpret_cast<const double2*>(V + (size_t)j * ldv) + q);
+                    acc[j] = fma(v.x, x.x, fma(v.y, x.y, acc[j]));
+                }
+            }
+        }
+        acc[NV] = fma(x.x, x.x, fma(x.y, x.y, acc[NV]));
     }
-    acc = warp_sum(acc);
-    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double v = 0.0;
-        for (int k = 0; k < kRedThreads / 32; ++k) v += s[k];
-        partial[blockIdx.x] = v;
+    block_reduce_store<NV>(acc, partial);
+}
+
+// w <- (w - sum_j c_j V_j) * scale
+template <int NV>
+__global__ void __launch_bounds__(kRedThreads) axpy_scale_t(double* w, const double* __restrict__ V, size_t ldv, Coefs cf,
+                                                           double scale, size_t n2) {
+    double2* w2 = reinterpret_cast<double2*>(w);
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n2; q += stride) {
+        double2 x = w2[q];
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            const double2 v = __ldcs(reinterpret_cast<const double2*>(V + (size_t)j * ldv) + q);
+            x.x = fma(-cf.c[j], v.x, x.x);
+            x.y = fma(-cf.c[j], v.y, x.y);
+        }
+        x.x *= scale;
+        x.y *= scale;
+        w2[q] = x;
     }
+}
+
+// y <- a x + b y; partial[b][0] = y . y
+__global__ void __launch_bounds__(kRedThreads) axpby_norm_kernel(double* y, const double* __restrict__ x, double a, double b,
+                                                                size_t n2, double* partial) {
+    double acc[1] = {0.0};
+    double2* y2 = reinterpret_cast<double2*>(y);
+    const double2* x2 = reinterpret_cast<const double2*>(x);
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n2; q += stride) {
+        const double2 u = __ldcs(x2 + q);
+        double2 v = y2[q];
+        v.x = a * u.x + b * v.x;
+        v.y = a * u.y + b * v.y;
+        y2[q] = v;
+        acc[0] = fma(v.x, v.x, fma(v.y, v.y, acc[0]));
+    }
+    block_reduce_store<0>(acc, partial);
+}
+
+// Compile-time dispatch of nv in [0, kMaxDots].
+template <int N>
+struct NvDispatch {
+    template <class F>
+    static void run(int nv, F&& f) {
+        if (nv == N) f(std::integral_constant<int, N>{});
+        else NvDispatch<N - 1>::run(nv, f);
+    }
+};
+template <>
+struct NvDispatch<-1> {
+    template <class F>
+    static void run(int, F&&) {}
+};
+
+// Resident blocks per SM of a kernel (cached per instantiation).
+template <class K>
+int blocks_per_sm(K kernel) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, kRedThreads, 0) != cudaSuccess) {
+        cudaGetLastError();
+        b = 1;
+    }
+    return b < 1 ? 1 : b;
 }
 
 __global__ void axpby_kernel(double* y, const double* x, double a, double b, size_t n) {
@@ -130,6 +236,29 @@ __global__ void unc_source_kernel(double* src, const double* __restrict__ unc, c
     }
 }
 
+// Group source in one pass (Main.f90 PIEISource :544-747 restated in moment space):
+//   src[j][n] = sum_{g' < g} sigma_{g'->g}(mat(n), l(j)) phi_{g'}[j][n]
+//             + sigma_{0->g}(mat(n), l(j)) Y_j(Omega_beam) unc[n]
+// tab = transfer tables [G][G][Nm][nmpad]; phi_all = [G][nm][NENK] solved group moments.
+__global__ void __launch_bounds__(256) group_source_kernel(double* __restrict__ src, const double* __restrict__ phi_all,
+                                                          const float* __restrict__ tab, int G, int g,
+                                                          const double* __restrict__ unc,
+                                                          const double* __restrict__ ybeam, const int* __restrict__ mat,
+                                                          long long NENK, int Nm, int nm, int nmpad) {
+    const size_t nvec = (size_t)nm * NENK;
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < NENK; n += (long long)gridDim.x * blockDim.x) {
+        const int m = mat[n >> 2];
+        const double u = unc ? unc[n] : 0.0;
+        const float* t0 = tab + ((size_t)g * Nm + m) * nmpad;   // (g' = 0, g)
+        for (int j = 0; j < nm; ++j) {
+            double acc = (double)t0[j] * ybeam[j] * u;
+            for (int gp = 0; gp < g; ++gp)
+                acc += (double)tab[(((size_t)gp * G + g) * Nm + m) * nmpad + j] * phi_all[(size_t)gp * nvec + (size_t)j * NENK + n];
+            src[(size_t)j * NENK + n] = acc;
+        }
+    }
+}
+
 // scalar fluence fl = sqrt(4 pi) phi_00 + s*unc; flux = fl; dose += dd[mat] fl (TallyDeposition.f90:19)
 __global__ void dose_kernel(const double* __restrict__ phi00, const double* __restrict__ unc, double unc_scale,
                             const double* __restrict__ dd, const int* __restrict__ mat, double* flux, double* dose,
@@ -151,48 +280,123 @@ inline int grid_for(Handle* h, size_t n) {
 
 }  // namespace
 
-int k_dots(Handle* h, const double* V, size_t ldv, int nv, const double* w, size_t n, double* out) {
-    if (nv > kMaxDots) return fail(h, LB_ERR_ARG, "dots: too many vectors");
-    if (n % 2) return fail(h, LB_ERR_ARG, "dots: odd vector length");
-    const int grid = h->sm_count * 4;
-    Timer t;
-    timer_begin(h, LB_T_KRYLOV, t);
-    dots_kernel<<<grid, kRedThreads, 0, h->stream>>>(V, ldv, nv, w, n, h->d_red);
-    timer_end(h, t);
-    cudaError_t e = cudaMemcpyAsync(h->h_red, h->d_red, sizeof(double) * grid * kMaxDots, cudaMemcpyDeviceToHost, h->stream);
+// Sum of the per-block partials (block order: deterministic) for entries 0..cnt-1.
+static int reduce_partials(Handle* h, int grid, int cnt, double* out) {
+    cudaError_t e = cudaMemcpyAsync(h->h_red, h->d_red, sizeof(double) * (size_t)grid * kPartStride,
+                                    cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    if (e != cudaSuccess) return cuda_fail(h, e, "dots");
-    for (int j = 0; j < nv; ++j) {
+    if (e != cudaSuccess) return cuda_fail(h, e, "Krylov reduction");
+    for (int j = 0; j < cnt; ++j) {
         double s = 0.0;
-        for (int b = 0; b < grid; ++b) s += h->h_red[(size_t)b * kMaxDots + j];
+        for (int b = 0; b < grid; ++b) s += h->h_red[(size_t)b * kPartStride + j];
         out[j] = s;
     }
     return LB_OK;
 }
 
-// w -= sum_j coef[j] V[j]; returns ||w||^2 through *nrm2 (may be null)
-int k_multi_axpy_norm(Handle* h, double* w, const double* V, size_t ldv, int nv, const double* coef, size_t n, double* nrm2) {
-    if (nv > kMaxDots) return fail(h, LB_ERR_ARG, "axpy: too many vectors");
-    if (n % 2) return fail(h, LB_ERR_ARG, "axpy: odd vector length");
-    Coefs cf;
-    for (int j = 0; j < kMaxDots; ++j) cf.c[j] = (j < nv) ? coef[j] : 0.0;
-    const int grid = h->sm_count * 4;
+static bool check_args(Handle* h, int nv, size_t n, const char* what, int* rc) {
+    if (nv < 0 || nv > kMaxDots) { *rc = fail(h, LB_ERR_ARG, std::string(what) + ": too many vectors"); return false; }
+    if (n % 2) { *rc = fail(h, LB_ERR_ARG, std::string(what) + ": odd vector length"); return false; }
+    return true;
+}
+
+// out[j] = V_j . w for j < nv; *wnorm2 = w . w (either output may be null).
+int k_dots_norm(Handle* h, const double* V, size_t ldv, int nv, const double* w, size_t n, double* out, double* wnorm2) {
+    int rc = 0;
+    if (!check_args(h, nv, n, "dots", &rc)) return rc;
+    int grid = 0;
     Timer t;
     timer_begin(h, LB_T_KRYLOV, t);
-    axpy_norm_kernel<<<grid, kRedThreads, 0, h->stream>>>(w, V, ldv, nv, cf, n, h->d_red);
+    NvDispatch<kMaxDots>::run(nv, [&](auto c) {
+        constexpr int NV = decltype(c)::value;
+        static const int occ = blocks_per_sm(dots_t<NV>);
+        grid = h->sm_count * occ;
+        dots_t<NV><<<grid, kRedThreads, 0, h->stream>>>(V, ldv, w, n / 2, h->d_red);
+    });
     timer_end(h, t);
-    if (!nrm2) return LB_OK;
-    cudaError_t e = cudaMemcpyAsync(h->h_red, h->d_red, sizeof(double) * grid, cudaMemcpyDeviceToHost, h->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    if (e != cudaSuccess) return cuda_fail(h, e, "axpy_norm");
-    double s = 0.0;
-    for (int b = 0; b < grid; ++b) s += h->h_red[b];
-    *nrm2 = s;
+    double tmp[kPartStride];
+    if ((rc = reduce_partials(h, grid, nv + 1, tmp))) return rc;
+    for (int j = 0; j < nv; ++j)
+        if (out) out[j] = tmp[j];
+    if (wnorm2) *wnorm2 = tmp[nv];
     return LB_OK;
 }
 
+int k_dots(Handle* h, const double* V, size_t ldv, int nv, const double* w, size_t n, double* out) {
+    return k_dots_norm(h, V, ldv, nv, w, n, out, nullptr);
+}
+
+// w -= sum_j coef[j] V_j; then dots[j] = V_j . w (if dots != null) and *nrm2 = w . w (if non-null).
+int k_axpy_dots(Handle* h, double* w, const double* V, size_t ldv, int nv, const double* coef, size_t n, double* dots,
+                double* nrm2) {
+    int rc = 0;
+    if (!check_args(h, nv, n, "axpy", &rc)) return rc;
+    Coefs cf;
+    for (int j = 0; j < kMaxDots; ++j) cf.c[j] = (j < nv) ? coef[j] : 0.0;
+    int grid = 0;
+    Timer t;
+    timer_begin(h, LB_T_KRYLOV, t);
+    NvDispatch<kMaxDots>::run(nv, [&](auto c) {
+        constexpr int NV = decltype(c)::value;
+        if (dots) {
+            static const int occ = blocks_per_sm(axpy_dots_t<NV, true>);
+            grid = h->sm_count * occ;
+            axpy_dots_t<NV, true><<<grid, kRedThreads, 0, h->stream>>>(w, V, ldv, cf, n / 2, h->d_red);
+        } else {
+            static const int occ = blocks_per_sm(axpy_dots_t<NV, false>);
+            grid = h->sm_count * occ;
+            axpy_dots_t<NV, false><<<grid, kRedThreads, 0, h->stream>>>(w, V, ldv, cf, n / 2, h->d_red);
+        }
+    });
+    timer_end(h, t);
+    if (!dots && !nrm2) return LB_OK;
+    double tmp[kPartStride];
+    if ((rc = reduce_partials(h, grid, nv + 1, tmp))) return rc;
+    if (dots)
+        for (int j = 0; j < nv; ++j) dots[j] = tmp[j];
+    if (nrm2) *nrm2 = tmp[nv];
+    return LB_OK;
+}
+
+// w <- (w - sum_j coef[j] V_j) * scale
+int k_axpy_scale(Handle* h, double* w, const double* V, size_t ldv, int nv, const double* coef, double scale, size_t n) {
+    int rc = 0;
+    if (!check_args(h, nv, n, "axpy", &rc)) return rc;
+    Coefs cf;
+    for (int j = 0; j < kMaxDots; ++j) cf.c[j] = (j < nv) ? coef[j] : 0.0;
+    Timer t;
+    timer_begin(h, LB_T_KRYLOV, t);
+    NvDispatch<kMaxDots>::run(nv, [&](auto c) {
+        constexpr int NV = decltype(c)::value;
+        static const int occ = blocks_per_sm(axpy_scale_t<NV>);
+        axpy_scale_t<NV><<<h->sm_count * occ, kRedThreads, 0, h->stream>>>(w, V, ldv, cf, scale, n / 2);
+    });
+    timer_end(h, t);
+    return LB_OK;
+}
+
+int k_multi_axpy_norm(Handle* h, double* w, const double* V, size_t ldv, int nv, const double* coef, size_t n, double* nrm2) {
+    return k_axpy_dots(h, w, V, ldv, nv, coef, n, nullptr, nrm2);
+}
+
 int k_multi_axpy(Handle* h, double* w, const double* V, size_t ldv, int nv, const double* coef, size_t n) {
-    return k_multi_axpy_norm(h, w, V, ldv, nv, coef, n, nullptr);
+    return k_axpy_scale(h, w, V, ldv, nv, coef, 1.0, n);
+}
+
+// y <- a x + b y and *nrm2 = y . y
+int k_axpby_norm(Handle* h, double* y, const double* x, double a, double b, size_t n, double* nrm2) {
+    int rc = 0;
+    if (!check_args(h, 0, n, "axpby", &rc)) return rc;
+    static const int occ = blocks_per_sm(axpby_norm_kernel);
+    const int grid = h->sm_count * occ;
+    Timer t;
+    timer_begin(h, LB_T_KRYLOV, t);
+    axpby_norm_kernel<<<grid, kRedThreads, 0, h->stream>>>(y, x, a, b, n / 2, h->d_red);
+    timer_end(h, t);
+    double tmp[1];
+    if ((rc = reduce_partials(h, grid, 1, tmp))) return rc;
+    if (nrm2) *nrm2 = tmp[0];
+    return LB_OK;
 }
 
 int k_axpby(Handle* h, double* y, const double* x, double a, double b, size_t n) {
@@ -254,6 +458,16 @@ int k_unc_source(Handle* h, double* src, const double* unc, const double* ybeam,
     Timer t;
     timer_begin(h, LB_T_TALLY, t);
     unc_source_kernel<<<grid_for(h, (size_t)nm * NENK), 256, 0, h->stream>>>(src, unc, ybeam, sigl, mat, NENK, nm, nmpad);
+    timer_end(h, t);
+    return LB_OK;
+}
+
+int k_group_source(Handle* h, double* src, const double* phi_all, const float* tab, int G, int g, const double* unc,
+                   const double* ybeam, const int* mat, long long NENK, int Nm, int nm, int nmpad) {
+    Timer t;
+    timer_begin(h, LB_T_TALLY, t);
+    group_source_kernel<<<grid_for(h, (size_t)NENK), 256, 0, h->stream>>>(src, phi_all, tab, G, g, unc, ybeam, mat, NENK,
+                                                                           Nm, nm, nmpad);
     timer_end(h, t);
     return LB_OK;
 }

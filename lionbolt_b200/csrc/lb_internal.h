@@ -63,6 +63,7 @@ struct Handle {
     std::vector<double> svec;      // [NE][4][3] area*n/volume (FP64)
     std::vector<uint32_t> nbrpack; // [NE][4]
     bool mesh_ready = false;
+    int mesh_version = 0;          // bumped by every lb_set_mesh
 
     // ---- angular ----
     int NI = 0, NIpad = 0;         // directions, and rounded up to a multiple of 16
@@ -80,6 +81,7 @@ struct Handle {
     int Ls = -1, nm = 0, nmpad = 0, ybuilt_NI = -1;
     std::vector<double> sigt, sigs;  // within group: [Nm], [Nm][Ls+1]
     bool phys_ready = false;
+    int xs_version = 0;              // bumped by every lb_set_xs
 
     // ---- device buffers ----
     float4* d_geom = nullptr;      // [NE][4] (snx, sny, snz, nbrpack)
@@ -165,6 +167,8 @@ void real_sh(int Ls, const double* dir, double* Y);
 void mlp_destroy(Handle* h);
 bool mlp_ready(Handle* h);
 int mlp_apply_precond(Handle* h, const double* v, double* z);
+// Appends `count` training samples drawn from the residual r and error err (device moment vectors).
+int mlp_sample(Handle* h, const double* r, const double* err, long long count, unsigned long long seed);
 
 // Allow a kernel the largest dynamic shared memory the device permits next to its static
 // shared memory (227 KB per CTA on sm_100 in total).  Clears the error state it may leave.
@@ -199,6 +203,16 @@ int launch_d2m(Handle* h, const float* psi, const double* xin, double alpha, dou
 
 // FP64 BLAS-1 on device vectors of length n
 int k_dots(Handle* h, const double* V, size_t ldv, int nv, const double* w, size_t n, double* out_host);
+// out[j] = V_j . w (j < nv, nv may be 0) and *wnorm2 = w . w in one pass (outputs may be null)
+int k_dots_norm(Handle* h, const double* V, size_t ldv, int nv, const double* w, size_t n, double* out, double* wnorm2);
+// w -= sum_j coef[j] V_j, then dots[j] = V_j . w and *nrm2 = w . w in the same pass (outputs may be null)
+int k_axpy_dots(Handle* h, double* w, const double* V, size_t ldv, int nv, const double* coef, size_t n, double* dots,
+                double* nrm2);
+// w <- (w - sum_j coef[j] V_j) * scale
+int k_axpy_scale(Handle* h, double* w, const double* V, size_t ldv, int nv, const double* coef, double scale, size_t n);
+int k_multi_axpy_norm(Handle* h, double* w, const double* V, size_t ldv, int nv, const double* coef, size_t n, double* nrm2);
+// y <- a x + b y and *nrm2 = y . y
+int k_axpby_norm(Handle* h, double* y, const double* x, double a, double b, size_t n, double* nrm2);
 int k_multi_axpy(Handle* h, double* w, const double* V, size_t ldv, int nv, const double* coef_host, size_t n);
 int k_axpby(Handle* h, double* y, const double* x, double a, double b, size_t n);   // y = a*x + b*y
 int k_scale(Handle* h, double* y, double a, size_t n);
@@ -210,6 +224,9 @@ int k_dose_tally(Handle* h, const double* phi00, const double* unc, double unc_s
                  const int* mat, double* flux, double* dose, long long NENK);
 int k_moment_source(Handle* h, double* src, const double* phi, const float* sigl, const int* mat, long long NENK,
                     int nm, int nmpad, int accumulate);
+// src = sum_{g'<g} Sigma_{g'->g} phi_{g'} + Sigma_{0->g} Y(beam) unc, one pass (tab: [G][G][Nm][nmpad])
+int k_group_source(Handle* h, double* src, const double* phi_all, const float* tab, int G, int g, const double* unc,
+                   const double* ybeam, const int* mat, long long NENK, int Nm, int nm, int nmpad);
 int k_unc_source(Handle* h, double* src, const double* unc, const double* ybeam, const float* sigl, const int* mat,
                  long long NENK, int nm, int nmpad);
 

@@ -113,9 +113,9 @@ static KrylovResult gmres_device(Handle* h, size_t n, const double* rhs, double*
         // r = rhs - A sol
         if ((rc = matvec(sol, V))) { res.status = rc; return res; }
         ++nmv;
-        k_axpby(h, V, rhs, 1.0, -1.0, n);     // V0 = rhs - V0
-        double alpha = vnorm(h, V, n, &rc);
-        if (rc) { res.status = rc; return res; }
+        double alpha = 0.0;
+        if ((rc = k_axpby_norm(h, V, rhs, 1.0, -1.0, n, &alpha))) { res.status = rc; return res; }   // V0 = rhs - V0
+        alpha = std::sqrt(alpha);
         if (std::isnan(alpha)) { res.status = fail(h, LB_ERR_NAN, "RESIDUAL NORM is NaN."); return res; }
         fpar5 = alpha;
         rs[1] = alpha;
@@ -133,23 +133,34 @@ static KrylovResult gmres_device(Handle* h, size_t n, const double* rhs, double*
             double* vk = V + (size_t)k * n;
             if ((rc = matvec(vin, vk))) { res.status = rc; return res; }
             ++nmv;
-            // orthogonalise vk against V[0..k-1]
-            if ((rc = k_dots(h, V, n, k + 1, vk, n, hh.data()))) { res.status = rc; return res; }
-            double nrm0 = hh[k];
-            double nrm1 = 0.0;
-            if ((rc = k_multi_axpy_norm(h, vk, V, n, k, hh.data(), n, &nrm1))) { res.status = rc; return res; }
-            if (nrm1 < 0.5 * nrm0) {
-                // significant cancellation: orthogonalise once more
-                if ((rc = k_dots(h, V, n, k, vk, n, h2.data()))) { res.status = rc; return res; }
-                if ((rc = k_multi_axpy_norm(h, vk, V, n, k, h2.data(), n, &nrm1))) { res.status = rc; return res; }
-                for (int i = 0; i < k; ++i) hh[i] += h2[i];
+            // Classical Gram-Schmidt with one selective re-orthogonalisation, in three passes over
+            // V[0..k-1]:  (1) hh = V^T vk and |vk|^2;  (2) vk -= V hh, with h2 = V^T vk and |vk|^2 of
+            // the result in the same pass;  (3) either vk = (vk - V h2) / hk when |vk| dropped below
+            // |vk_0| / sqrt(2) (|vk - V h2|^2 = |vk|^2 - |h2|^2 for orthonormal V), or vk /= hk.
+            double nrm0 = 0.0, nrm1 = 0.0;
+            if ((rc = k_dots_norm(h, V, n, k, vk, n, hh.data(), &nrm0))) { res.status = rc; return res; }
+            if ((rc = k_axpy_dots(h, vk, V, n, k, hh.data(), n, h2.data(), &nrm1))) { res.status = rc; return res; }
+            bool reorth = nrm1 < 0.5 * nrm0;
+            double hk2 = nrm1;
+            if (reorth) {
+                double s2 = 0.0;
+                for (int i = 0; i < k; ++i) s2 += h2[i] * h2[i];
+                hk2 = nrm1 - s2;
+                if (!(hk2 > 1e-4 * nrm1)) {
+                    // near breakdown: apply the correction and measure the norm exactly
+                    if ((rc = k_axpy_dots(h, vk, V, n, k, h2.data(), n, nullptr, &hk2))) { res.status = rc; return res; }
+                    reorth = false;
+                    for (int i = 0; i < k; ++i) hh[i] += h2[i];
+                } else {
+                    for (int i = 0; i < k; ++i) hh[i] += h2[i];
+                }
             }
-            double hk = std::sqrt(std::max(0.0, nrm1));
+            double hk = std::sqrt(std::max(0.0, hk2));
             if (std::isnan(hk)) { res.status = fail(h, LB_ERR_NAN, "RESIDUAL NORM is NaN."); return res; }
             for (int i = 0; i < k; ++i) H[k][i + 1] = hh[i];
             H[k][k + 1] = hk;
             if (!(hk > 0.0)) { breakdown = true; --k; break; }
-            k_scale(h, vk, 1.0 / hk, n);
+            if ((rc = k_axpy_scale(h, vk, V, n, reorth ? k : 0, h2.data(), 1.0 / hk, n))) { res.status = rc; return res; }
             for (int i = 1; i <= k - 1; ++i) {
                 double a = H[k][i];
                 H[k][i] = c[i] * a + s[i] * H[k][i + 1];
@@ -237,8 +248,41 @@ static KrylovResult moment_solve(Handle* h, const double* b, double* phi, int so
             // plain GMRES is the fallback when no trained network is loaded
             return gmres_device(h, n, b, phi, m, rtol, atol, maxit, mv, nullptr);
         }
+        // Learned path: FGMRES(m) with the network as right preconditioner, capped at 4m operator
+        // applications when the caller gives no limit.
         DevOp pc = [h](const double* in, double* out) { return mlp_apply_precond(h, in, out); };
-        return gmres_device(h, n, b, phi, m, rtol, atol, maxit, mv, &pc);
+        const int cap = maxit > 0 ? maxit : 4 * m;
+        KrylovResult kr = gmres_device(h, n, b, phi, m, rtol, atol, cap, mv, &pc);
+        if (kr.status != LB_OK && kr.status != LB_ERR_NOCONV && kr.status != LB_ERR_BREAKDOWN &&
+            kr.status != LB_ERR_NAN)
+            return kr;   // CUDA or argument errors end the solve
+        int nmv = kr.nmv;
+        int rc = 0;
+        if (kr.status == LB_ERR_NAN) {
+            k_copy(h, phi, b, n);   // the learned iterate is unusable: restart from the first-flight moments
+        } else {
+            // Plain-operator judge: the true residual ||b - A phi|| of the learned iterate.
+            if ((rc = apply_A(h, phi, h->d_t, sigl))) { kr.status = rc; return kr; }
+            ++nmv;
+            double rn = 0.0;
+            if ((rc = k_axpby_norm(h, h->d_t, b, 1.0, -1.0, n, &rn))) { kr.status = rc; return kr; }
+            rn = std::sqrt(rn);
+            const double bn = vnorm(h, b, n, &rc);
+            if (rc) { kr.status = rc; return kr; }
+            if (rn <= rtol * bn + atol) {
+                h->err.clear();
+                kr.status = LB_OK;
+                kr.nmv = nmv;
+                kr.resid = rn;
+                return kr;
+            }
+        }
+        // Fallback: plain GMRES(m) from the learned iterate, under the caller's limit.
+        h->err.clear();
+        KrylovResult k2 = gmres_device(h, n, b, phi, m, rtol, atol, maxit > 0 ? std::max(1, maxit - nmv) : 0, mv,
+                                       nullptr);
+        k2.nmv += nmv;
+        return k2;
     }
     return gmres_device(h, n, b, phi, m, rtol, atol, maxit, mv, nullptr);
 }
@@ -282,10 +326,45 @@ static int download_angular(Handle* h, const float* d, double* hs) {
     return e == cudaSuccess ? LB_OK : cuda_fail(h, e, "download angular vector");
 }
 
+
 }  // namespace lb
 
 using namespace lb;
 struct lb_handle : public lb::Handle {};
+
+// ---------------------------------------------------------------------------------------------
+//  multigroup helpers (group loop of Main.f90:326-476)
+// ---------------------------------------------------------------------------------------------
+static float* mg_table(Handle* h, int gp, int g) {
+    return h->d_sigl_mg + (((size_t)gp * h->G + g) * h->Nm) * h->nmpad;
+}
+
+// Beam-direction harmonics Y_j(Omega_b) for the first-collision source.
+static void mg_prepare(Handle* h) {
+    std::vector<double> yb(h->nm);
+    real_sh(h->Ls, h->beam_dir.data(), yb.data());
+    cudaMemcpyAsync(h->d_yb, yb.data(), sizeof(double) * h->nm, cudaMemcpyHostToDevice, h->stream);
+    cudaStreamSynchronize(h->stream);
+}
+
+// Source and operator of group g from the solved groups g' < g in d_phi_all:
+// d_src = sum_{g'<g} Sigma_{g'->g} phi_{g'} + first collision of the beam, the within-group cross
+// sections of g set on the handle, and d_b = D T^{-1} M d_src.
+static int mg_group_setup(Handle* h, int g) {
+    const int G = h->G, Nm = h->Nm, Ls = h->Ls, nm = h->nm, nmpad = h->nmpad;
+    const size_t NENK = (size_t)h->NENK, n = h->kry_n;
+    (void)n;
+    k_group_source(h, h->d_src, h->d_phi_all, h->d_sigl_mg, G, g, h->d_unc, h->d_yb, h->d_mat, (long long)NENK, Nm, nm,
+                   nmpad);
+    std::vector<double> st(h->mg_sigt.begin() + (size_t)g * Nm, h->mg_sigt.begin() + (size_t)(g + 1) * Nm);
+    std::vector<double> ss((size_t)Nm * (Ls + 1));
+    for (int mm = 0; mm < Nm; ++mm)
+        for (int l = 0; l <= Ls; ++l)
+            ss[(size_t)mm * (Ls + 1) + l] = h->mg_sigs[(((size_t)g * G + g) * Nm + mm) * (Ls + 1) + l];
+    int rc = lb_set_xs(static_cast<lb_handle*>(h), Ls, st.data(), ss.data());
+    if (rc) return rc;
+    return apply_transport_moments(h, nullptr, nullptr, h->d_src, nullptr, h->d_b);
+}
 
 extern "C" {
 
@@ -427,36 +506,17 @@ int lb_mg_solve(lb_handle* h, int solver, int m, double rtol, double atol, int m
     if (m < 1) m = 10;
     if (m > 30) return fail(h, LB_ERR_ARG, "restart length must be <= 30");
     cudaSetDevice(h->device);
-    const int G = h->G, Nm = h->Nm, Ls = h->Ls;
+    const int G = h->G, Nm = h->Nm;
     int rc = ensure_krylov(h, m, solver == LB_SOLVER_FGMRES_ML);
     if (rc) return rc;
-    const int nm = h->nm, nmpad = h->nmpad;
     const size_t NENK = (size_t)h->NENK, n = h->kry_n;
-    // beam direction harmonics Y_j(Omega_b)
-    std::vector<double> yb(nm);
-    real_sh(Ls, h->beam_dir.data(), yb.data());
-    double* d_yb = h->d_yb;
-    cudaMemcpyAsync(d_yb, yb.data(), sizeof(double) * nm, cudaMemcpyHostToDevice, h->stream);
+    mg_prepare(h);
     cudaMemsetAsync(h->d_dose, 0, sizeof(double) * NENK, h->stream);
-    auto table = [&](int gp, int g) { return h->d_sigl_mg + (((size_t)gp * G + g) * Nm) * nmpad; };
     for (int g = 0; g < G; ++g) {
-        // group source: downscatter of every solved group + first collision of the beam
-        cudaMemsetAsync(h->d_src, 0, sizeof(double) * n, h->stream);
-        for (int gp = 0; gp < g; ++gp)
-            k_moment_source(h, h->d_src, h->d_phi_all + (size_t)gp * n, table(gp, g), h->d_mat, (long long)NENK, nm, nmpad, 1);
-        k_unc_source(h, h->d_src, h->d_unc, d_yb, table(0, g), h->d_mat, (long long)NENK, nm, nmpad);
-        // within-group operator of group g
-        std::vector<double> st(h->mg_sigt.begin() + (size_t)g * Nm, h->mg_sigt.begin() + (size_t)(g + 1) * Nm);
-        std::vector<double> ss((size_t)Nm * (Ls + 1));
-        for (int mm = 0; mm < Nm; ++mm)
-            for (int l = 0; l <= Ls; ++l)
-                ss[(size_t)mm * (Ls + 1) + l] = h->mg_sigs[(((size_t)g * G + g) * Nm + mm) * (Ls + 1) + l];
-        if ((rc = lb_set_xs(h, Ls, st.data(), ss.data()))) break;
-        // b = D T^{-1} M src
-        if ((rc = apply_transport_moments(h, nullptr, nullptr, h->d_src, nullptr, h->d_b))) break;
+        if ((rc = mg_group_setup(h, g))) break;
         double* phi = h->d_phi_all + (size_t)g * n;
         k_copy(h, phi, h->d_b, n);
-        KrylovResult kr = moment_solve(h, h->d_b, phi, solver, m, rtol, atol, maxit, table(g, g));
+        KrylovResult kr = moment_solve(h, h->d_b, phi, solver, m, rtol, atol, maxit, mg_table(h, g, g));
         if (iters) iters[g] = kr.nmv;
         if ((rc = kr.status)) break;
         k_dose_tally(h, phi, h->d_unc, g == 0 ? 1.0 : 0.0, h->d_dd + (size_t)g * Nm, h->d_mat,
@@ -476,6 +536,48 @@ int lb_mg_get_results(lb_handle* h, double* flux, double* dose) {
         e = cudaMemcpyAsync(dose, h->d_dose, sizeof(double) * (size_t)h->NENK, cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     return e == cudaSuccess ? LB_OK : cuda_fail(h, e, "read results");
+}
+
+
+int lb_lp_generate(lb_handle* h, int samples_per_group, int iters, unsigned long long seed, long long* total) {
+    if (!h || h->device < 0 || h->G < 1 || !h->d_phi_all)
+        return h ? fail(h, LB_ERR_STATE, "lb_lp_generate: multigroup problem not set") : LB_ERR_ARG;
+    if (samples_per_group < 0 || iters < 1) return fail(h, LB_ERR_ARG, "lb_lp_generate: bad arguments");
+    cudaSetDevice(h->device);
+    const int G = h->G, m = 30;
+    int rc = ensure_krylov(h, m, false);
+    if (rc) return rc;
+    const size_t n = h->kry_n;
+    mg_prepare(h);
+    double* r = h->d_V;          // residual of the iterate
+    double* err = h->d_V + n;    // its error
+    for (int g = 0; g < G; ++g) {
+        if ((rc = mg_group_setup(h, g))) return rc;
+        // reference solution of the group (also the source of the groups below it)
+        double* phi = h->d_phi_all + (size_t)g * n;
+        k_copy(h, phi, h->d_b, n);
+        const float* sigl = mg_table(h, g, g);
+        DevOp mv = [h, sigl](const double* in, double* out) { return apply_A(h, in, out, sigl); };
+        KrylovResult kr = gmres_device(h, n, h->d_b, phi, m, 1e-10, 0.0, 4000, mv, nullptr);
+        if (kr.status) return kr.status;
+        // source iteration from the first-flight moments: x_{k+1} = x_k + r_k, r_k = b - A x_k = A e_k
+        double* x = h->d_x;
+        k_copy(h, x, h->d_b, n);
+        for (int k = 0; k < iters; ++k) {
+            if ((rc = apply_A(h, x, r, sigl))) return rc;
+            k_axpby(h, r, h->d_b, 1.0, -1.0, n);
+            k_copy(h, err, phi, n);
+            k_axpby(h, err, x, -1.0, 1.0, n);
+            const long long cnt = samples_per_group / iters + (k < samples_per_group % iters ? 1 : 0);
+            const unsigned long long sd = seed ^ (0x9E3779B97F4A7C15ull * (unsigned long long)(g * 1024 + k + 1));
+            if ((rc = mlp_sample(h, r, err, cnt, sd))) return rc;
+            k_axpby(h, x, r, 1.0, 1.0, n);
+        }
+    }
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "lb_lp_generate");
+    if (total) lb_lp_num_samples(h, total);
+    return LB_OK;
 }
 
 }  // extern "C"

@@ -304,6 +304,125 @@ __global__ void __launch_bounds__(1024, MINB) sweep_levels_pf_kernel(SweepArgs a
 }
 
 // ---------------------------------------------------------------------------------------------
+// Staged level schedule: the static inputs of level L+1 are brought on chip while level L is
+// computed, so that after each CTA barrier the only global loads left on an update's critical path
+// are the upstream values written by earlier levels.
+//   * items of level L+2 are loaded into registers during level L (KS slots per thread);
+//   * during level L the items of L+1 (from those registers) go to shared memory, their
+//     neighbour words (16 B of the element record) are copied with cp.async, and their sources and
+//     face vectors are prefetched into L2;
+//   * elements beyond the KS * NT staged slots of a level take the direct path.
+// Shared memory: two buffers of KS * NT (item, neighbour word) pairs = 40 * KS * NT bytes.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p)); }
+
+template <int NT, int KS>
+__global__ void __launch_bounds__(NT, 1) sweep_staged_kernel(SweepArgs a) {
+    constexpr int CAP = NT * KS;
+    extern __shared__ __align__(16) unsigned char s_stage[];
+    int4* s_nbr = reinterpret_cast<int4*>(s_stage);       // [2][CAP]
+    int* s_item = reinterpret_cast<int*>(s_nbr + 2 * CAP);  // [2][CAP]
+    __shared__ float s_sigt[256];
+    load_sigt(a, s_sigt);
+    const int t = threadIdx.x;
+    for (int i = blockIdx.x; i < a.NI; i += gridDim.x) {
+        const int nl = __ldg(&a.nlev[i]);
+        const int lb = __ldg(&a.lvl_base[i]);
+        const float4 dir = __ldg(&a.dirs[i]);
+        const int* it = a.items + (size_t)i * a.NE;
+        float* base = a.psi + (size_t)i * (size_t)a.NENK;
+        int s0 = __ldg(&a.lvl_start[lb]);
+        int s1 = __ldg(&a.lvl_start[lb + 1]);
+        int n0 = s1;
+        int n1 = (nl > 1) ? __ldg(&a.lvl_start[lb + 2]) : s1;
+        int nxt[KS];
+        // stage level 0 into buffer 0 and load the items of level 1
+#pragma unroll
+        for (int k = 0; k < KS; ++k) {
+            const int slot = t + k * NT;
+            if (s0 + slot < s1) {
+                const int itm = __ldcs(&it[s0 + slot]);
+                const int e = itm & 0xFFFFFF;
+                s_item[slot] = itm;
+                cp_async16(&s_nbr[slot], &a.geom[(size_t)e * 4 + 3]);
+            }
+        }
+        cp_async_commit();
+#pragma unroll
+        for (int k = 0; k < KS; ++k) {
+            const int slot = t + k * NT;
+            nxt[k] = (n0 + slot < n1) ? __ldcs(&it[n0 + slot]) : 0;
+        }
+        cp_async_wait_all();
+        __syncthreads();
+        for (int L = 0; L < nl; ++L) {
+            const int b = L & 1;
+            // (1) stage level L+1 into the other buffer
+            int4* nb_dst = s_nbr + (b ^ 1) * CAP;
+            int* it_dst = s_item + (b ^ 1) * CAP;
+#pragma unroll
+            for (int k = 0; k < KS; ++k) {
+                const int slot = t + k * NT;
+                if (n0 + slot < n1) {
+                    const int itm = nxt[k];
+                    const int e = itm & 0xFFFFFF;
+                    it_dst[slot] = itm;
+                    cp_async16(&nb_dst[slot], &a.geom[(size_t)e * 4 + 3]);
+                    prefetch_l2(base + 4 * (size_t)e);
+                    prefetch_l2(&a.geom[(size_t)e * 4]);
+                }
+            }
+            cp_async_commit();
+            // (2) items of level L+2
+            const int m0 = n1;
+            const int m1 = (L + 2 < nl) ? __ldg(&a.lvl_start[lb + L + 3]) : n1;
+#pragma unroll
+            for (int k = 0; k < KS; ++k) {
+                const int slot = t + k * NT;
+                nxt[k] = (m0 + slot < m1) ? __ldcs(&it[m0 + slot]) : 0;
+            }
+            // (3) level L from the staged buffer, then the overflow beyond the staged slots
+            const int4* nb_src = s_nbr + b * CAP;
+            const int* it_src = s_item + b * CAP;
+#pragma unroll
+            for (int k = 0; k < KS; ++k) {
+                const int slot = t + k * NT;
+                if (s0 + slot < s1) {
+                    const int item = it_src[slot];
+                    const int e = item & 0xFFFFFF;
+                    Geom g;
+                    g.gx = __ldg(&a.geom[(size_t)e * 4 + 0]);
+                    g.gy = __ldg(&a.geom[(size_t)e * 4 + 1]);
+                    g.gz = __ldg(&a.geom[(size_t)e * 4 + 2]);
+                    g.gn = nb_src[slot];
+                    Update up;
+                    assemble_g<false>(base, dir, item, g, s_sigt, up, make_float4(0.f, 0.f, 0.f, 0.f));
+                    finish<false>(base, item, up);
+                }
+            }
+            for (int es = s0 + CAP + t; es < s1; es += NT) {
+                const int item = __ldcs(&it[es]);
+                Update up;
+                assemble<false>(a, base, dir, item, s_sigt, up);
+                finish<false>(base, item, up);
+            }
+            cp_async_wait_all();
+            __syncthreads();
+            s0 = n0;
+            s1 = n1;
+            n0 = m0;
+            n1 = m1;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // Element-flag schedule: one CTA per direction, no barriers between levels.  Warps claim 32-element
 // chunks of the direction's padded sweep order (levels padded to multiples of 32, so a chunk's
 // elements are mutually independent) from a shared counter, prefetch the next chunk's items,
@@ -556,7 +675,8 @@ __global__ void __launch_bounds__(256) sweep_dataflow_kernel(SweepArgs a) {
 }
 
 struct Config {
-    int kind;      // 0 levels, 1 dataflow, 2 levels with next-level prefetch, 3 element flags, 4 grouped levels
+    int kind;      // 0 levels, 1 dataflow, 2 levels with next-level prefetch, 3 element flags, 4 grouped levels,
+                   // 5 staged levels (dpc = staged slots per thread)
     int threads;
     int dpc;       // directions per CTA (kind 0); minimum CTAs per SM (kind 2)
     int ilp;
@@ -565,6 +685,7 @@ struct Config {
 const Config kConfigs[] = {
     {4, 1024, 2, 1}, {4, 512, 2, 1}, {4, 512, 3, 1}, {4, 1024, 3, 1}, {4, 512, 6, 1},
     {0, 1024, 1, 1}, {0, 512, 1, 1}, {2, 1024, 1, 1}, {3, 512, 0, 1}, {1, 256, 0, 0},
+    {5, 1024, 5, 1}, {5, 512, 8, 1},
 };
 constexpr int kNumConfigs = sizeof(kConfigs) / sizeof(kConfigs[0]);
 
@@ -636,6 +757,19 @@ cudaError_t launch_flags(const SweepArgs& a, int sm_count, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+template <int NT, int KS>
+cudaError_t launch_staged(const SweepArgs& a, int sm_count, cudaStream_t s) {
+    const size_t smem = (size_t)2 * NT * KS * (sizeof(int4) + sizeof(int));
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(sweep_staged_kernel<NT, KS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    int grid = std::min(a.NI, sm_count);
+    sweep_staged_kernel<NT, KS><<<grid, NT, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
 template <int MINB>
 cudaError_t launch_levels_pf(const SweepArgs& a, int threads, int sm_count, cudaStream_t s) {
     int per_sm = 0;
@@ -699,6 +833,8 @@ int launch_sweep(Handle* h, float* psi) {
         cudaFuncGetAttributes(&fa, sweep_levels_kernel<2, 1>);
         cudaFuncGetAttributes(&fa, sweep_levels_kernel<2, 2>);
         cudaFuncGetAttributes(&fa, sweep_dataflow_kernel);
+        cudaFuncGetAttributes(&fa, sweep_staged_kernel<1024, 5>);
+        cudaFuncGetAttributes(&fa, sweep_staged_kernel<512, 8>);
     }
     Config cfg = kConfigs[cfg_idx];
     // the element-flag schedule keeps one bit per element in shared memory
@@ -719,7 +855,10 @@ int launch_sweep(Handle* h, float* psi) {
     }
     Timer t;
     timer_begin(h, LB_T_SWEEP, t);
-    if (cfg.kind == 4) {
+    if (cfg.kind == 5) {
+        e = cfg.threads == 1024 ? launch_staged<1024, 5>(a, h->sm_count, h->stream)
+                                : launch_staged<512, 8>(a, h->sm_count, h->stream);
+    } else if (cfg.kind == 4) {
         if (cfg.dpc == 2) e = cfg.threads == 1024 ? launch_group<2, 1024>(a, h->d_groups, h->ngroups, h->sm_count, h->stream)
                                                   : launch_group<2, 512>(a, h->d_groups, h->ngroups, h->sm_count, h->stream);
         else if (cfg.dpc == 3) e = cfg.threads == 1024 ? launch_group<3, 1024>(a, h->d_groups, h->ngroups, h->sm_count, h->stream)

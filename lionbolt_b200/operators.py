@@ -111,6 +111,85 @@ class _Op:
     def timers(self):
         return self._h.timers()
 
+    # ---- learned right preconditioner (per-cell MLP, used by solver="FGMRES_ML") ----------------
+    NIN, NOUT = 19, 16
+
+    def lp_nparams(self):
+        return int(self._h.lib.lb_lp_nparams())
+
+    def lp_init(self, seed=0):
+        self._h.call("lb_lp_init", int(seed))
+        return self
+
+    def lp_set_weights(self, w):
+        w = _lib.as_f32(w).ravel()
+        if w.size != self.lp_nparams():
+            raise ValueError(f"expected {self.lp_nparams()} parameters, got {w.size}")
+        self._h.call("lb_lp_set_weights", _lib.fptr(w))
+        return self
+
+    def lp_get_weights(self):
+        w = np.zeros(self.lp_nparams(), dtype=np.float32)
+        self._h.call("lb_lp_get_weights", _lib.fptr(w))
+        return w
+
+    def lp_enable(self, on=True):
+        self._h.call("lb_lp_enable", int(bool(on)))
+        return self
+
+    def lp_forward(self, x):
+        """Network outputs [n, 16] for features x [n, 19] (tensor-core inference kernel)."""
+        x = _lib.as_f32(x).reshape(-1, self.NIN)
+        y = np.zeros((x.shape[0], self.NOUT), dtype=np.float32)
+        self._h.call("lb_lp_forward", int(x.shape[0]), _lib.fptr(x), _lib.fptr(y))
+        return y
+
+    def lp_apply(self, v):
+        """Preconditioner applied to a moment vector v [nm * NENK] (current cross sections)."""
+        v = as_f64(v).ravel()
+        z = np.zeros_like(v)
+        self._h.call("lb_lp_apply", dptr(v), dptr(z))
+        return z
+
+    def lp_loss_grad(self, x, t, w=None):
+        x = _lib.as_f32(x).reshape(-1, self.NIN)
+        t = _lib.as_f32(t).reshape(-1, self.NOUT)
+        wp = None if w is None else _lib.fptr(_lib.as_f32(w).ravel())
+        loss = np.zeros(1)
+        g = np.zeros(self.lp_nparams(), dtype=np.float32)
+        self._h.call("lb_lp_loss_grad", int(x.shape[0]), _lib.fptr(x), _lib.fptr(t), wp, dptr(loss), _lib.fptr(g))
+        return float(loss[0]), g
+
+    def lp_generate(self, samples_per_group=2000, iters=8, seed=0):
+        """Append (residual, error) cell samples from plain-solver runs of the problem set on this
+        operator (MultigroupSolver); returns the size of the training set."""
+        n = np.zeros(1, dtype=np.int64)
+        self._h.call("lb_lp_generate", int(samples_per_group), int(iters), int(seed), n.ctypes.data_as(_lib._c_ll_p))
+        return int(n[0])
+
+    def lp_num_samples(self):
+        n = np.zeros(1, dtype=np.int64)
+        self._h.call("lb_lp_num_samples", n.ctypes.data_as(_lib._c_ll_p))
+        return int(n[0])
+
+    def lp_samples(self):
+        """(features [n, 19], targets [n, 16], loss weights [n]) of the training set."""
+        n = self.lp_num_samples()
+        x = np.zeros((n, self.NIN), dtype=np.float32)
+        t = np.zeros((n, self.NOUT), dtype=np.float32)
+        w = np.zeros(n, dtype=np.float32)
+        self._h.call("lb_lp_get_samples", _lib.fptr(x), _lib.fptr(t), _lib.fptr(w))
+        return x, t, w
+
+    def lp_clear(self):
+        self._h.call("lb_lp_clear_samples")
+
+    def lp_train(self, steps=1500, batch=2048, lr=3e-3, seed=0):
+        """Adam on the device-resident training set; returns the batch loss of every step."""
+        hist = np.zeros(max(int(steps), 1))
+        self._h.call("lb_lp_train", int(steps), int(batch), float(lr), int(seed), dptr(hist))
+        return hist[:steps]
+
     def Destroy(self):
         self._h.close()
 
