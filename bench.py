@@ -44,6 +44,11 @@ def parse():
     p.add_argument("--mesh", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
                    help="hexes per axis of a reduced box with the same physics (profiling cases)")
     p.add_argument("--groups", type=int, default=None, help="energy groups of the reduced box")
+    p.add_argument("--workload", default="dose", choices=["dose", "gemm", "batch"],
+                   help="dose: multigroup dose solve (default); gemm: standalone moment-to-discrete and "
+                        "discrete-to-moment contractions at the 768k-tet size, split-BF16 vs cuBLAS FP32 vs FP64; "
+                        "batch: 64 independent problems (8^3..32^3 hexes, S8/S12/S16, 1-10 groups, P3) solved "
+                        "together")
     p.add_argument("--no-learned", action="store_true",
                    help="skip the learned-preconditioner FGMRES comparison (training + timed solves)")
     p.add_argument("--lp-problems", type=int, default=3, help="training problems (seeded cross sections / slab)")
@@ -253,6 +258,170 @@ def learned_comparison(args, mg, device, barrier, gmres_ms, gmres_dose):
                          "generate_s": t_gen, "train_s": t_train}}
 
 
+def real_sh(Ls, dirs):
+    """Real orthonormal spherical harmonics Y[i][l*l+l+m] (cos for m > 0, sin for m < 0), FP64."""
+    dirs = np.asarray(dirs, dtype=np.float64)
+    ct = dirs[:, 2]
+    st = np.sqrt(np.maximum(0.0, 1.0 - ct * ct))
+    ph = np.arctan2(dirs[:, 1], dirs[:, 0])
+    Pl = {}
+    Pl[(0, 0)] = np.ones_like(ct)
+    for m in range(1, Ls + 1):
+        Pl[(m, m)] = Pl[(m - 1, m - 1)] * (2 * m - 1) * st
+    for m in range(Ls):
+        Pl[(m + 1, m)] = (2 * m + 1) * ct * Pl[(m, m)]
+    for m in range(Ls + 1):
+        for l in range(m + 2, Ls + 1):
+            Pl[(l, m)] = ((2 * l - 1) * ct * Pl[(l - 1, m)] - (l + m - 1) * Pl[(l - 2, m)]) / (l - m)
+    Y = np.zeros((dirs.shape[0], (Ls + 1) ** 2))
+    for l in range(Ls + 1):
+        for m in range(-l, l + 1):
+            am = abs(m)
+            nrm = np.sqrt((2 * l + 1) / (4 * np.pi) * np.prod(1.0 / np.arange(l - am + 1, l + am + 1, dtype=np.float64)))
+            v = nrm * Pl[(l, am)]
+            if m > 0:
+                v = v * np.sqrt(2.0) * np.cos(am * ph)
+            elif m < 0:
+                v = v * np.sqrt(2.0) * np.sin(am * ph)
+            Y[:, l * l + l + m] = v
+    return Y
+
+
+def run_gemm(args):
+    """Standalone scattering contractions (config2 shapes): M2D psi[288][3,072,000] = Y[288][36]
+    phi[36][3,072,000] and D2M phi = (wY)^T psi, on the device.  Split-BF16 tensor-core kernels vs
+    cuBLAS FP32 (TF32 off) vs an FP64 reference on 65,536 sampled node columns."""
+    import ctypes
+    import torch
+    from lionbolt_b200 import AngularClass, ScatteringOp, XSType
+    from lionbolt_b200 import problems as P
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    prob = P.config1()
+    m = prob.mesh
+    NENK, NI, Ls = m.NENK, prob.NI, 5
+    nm = (Ls + 1) ** 2
+    op = ScatteringOp(device=local).Build(m, AngularClass(k=prob.k, w=prob.w),
+                                          XSType(np.ones(m.Nm), np.ones((m.Nm, Ls + 1))))   # sigma_l = 1
+    h = op._h
+    dev = f"cuda:{local}"
+    gen = torch.Generator(device=dev).manual_seed(20261203)
+    lofj = np.concatenate([[l] * (2 * l + 1) for l in range(Ls + 1)])
+    scale = torch.from_numpy(0.8 ** lofj).to(dev)
+    phi = torch.randn(nm, NENK, dtype=torch.float64, device=dev, generator=gen) * scale[:, None]
+    psi = torch.empty(NI, NENK, dtype=torch.float32, device=dev)
+    phi2 = torch.empty(nm, NENK, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    vp = ctypes.c_void_p
+
+    def timed(fn, slot):
+        for _ in range(args.warmup):
+            fn()
+        h.call("lb_synchronize")
+        h.mark(slot)
+        for _ in range(args.steps):
+            fn()
+        h.mark(slot + 1)
+        return h.elapsed_ms(slot, slot + 1) / args.steps
+
+    t_m2d = timed(lambda: h.call("lb_m2d_device", vp(phi.data_ptr()), vp(psi.data_ptr())), 0)
+    t_d2m = timed(lambda: h.call("lb_d2m_device", vp(psi.data_ptr()), vp(phi2.data_ptr())), 2)
+    h.call("lb_synchronize")
+    # cuBLAS FP32 comparators on the same inputs
+    torch.backends.cuda.matmul.allow_tf32 = False
+    Y = torch.from_numpy(real_sh(Ls, prob.k)).to(dev)                   # [NI, nm] FP64
+    D = (Y * torch.from_numpy(prob.w).to(dev)[:, None]).T.contiguous()  # [nm, NI]
+    Y32, D32, phi32 = Y.float(), D.float(), phi.float()
+
+    def tevent(fn):
+        for _ in range(args.warmup):
+            fn()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(args.steps):
+            out = fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / args.steps, out
+
+    t_m2d32, psi32 = tevent(lambda: Y32 @ phi32)
+    t_d2m32, phi2_32 = tevent(lambda: D32 @ psi)
+    # FP64 reference (CPU) on sampled columns; D2M uses the product's psi as input for every path
+    cols = torch.randint(NENK, (65536,), generator=gen, device=dev)
+    Yh, Dh = Y.cpu().numpy(), D.cpu().numpy()
+    ref_m2d = Yh @ phi[:, cols].cpu().numpy()
+    psi_s = psi[:, cols].double().cpu().numpy()
+    ref_d2m = Dh @ psi_s
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    e_m2d = rel(psi[:, cols].double().cpu().numpy(), ref_m2d)
+    e_m2d32 = rel(psi32[:, cols].double().cpu().numpy(), ref_m2d)
+    e_d2m = rel(phi2[:, cols].cpu().numpy(), ref_d2m)
+    e_d2m32 = rel(phi2_32[:, cols].double().cpu().numpy(), ref_d2m)
+    flops = 2.0 * NENK * nm * NI
+    by_m2d = NENK * (nm * 8 + NI * 4)
+    by_d2m = NENK * (NI * 4 + nm * 8)
+    peak, kind = measured_peaks()
+
+    def entry(ms, by, err, ms32, err32):
+        return {"ms": ms, "gbs": by / ms / 1e6, "hbm_frac": by / ms / 1e6 / peak, "useful_tflops": flops / ms / 1e9,
+                "rel_l2_vs_fp64": err, "cublas_fp32": {"ms": ms32, "rel_l2_vs_fp64": err32}}
+
+    line = {"metric": "config2 scattering contractions: split-BF16 (6 products, FP32 accumulate) vs FP32 vs FP64",
+            "workload": f"M2D [{NI} x {nm}] x [{nm} x {NENK}] and D2M [{nm} x {NI}] x [{NI} x {NENK}], "
+                        "phi ~ N(0,1) 0.8^l, seeded",
+            "steps": args.steps, "warmup": args.warmup, "peak_gbs": peak, "peak_source": kind,
+            "m2d": entry(t_m2d, by_m2d, e_m2d, t_m2d32, e_m2d32),
+            "d2m": entry(t_d2m, by_d2m, e_d2m, t_d2m32, e_d2m32),
+            "sample_columns": int(cols.numel()),
+            "algorithmic_bytes": {"m2d": by_m2d, "d2m": by_d2m}}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    op.Destroy()
+    return 0
+
+
+def run_batch(args):
+    """Batched workload: 64 seeded independent dose problems solved together (one step = all 64)."""
+    import torch
+    from lionbolt_b200 import BatchSolver
+    from lionbolt_b200 import problems as P
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    probs = P.batch_problems(count=64, seed=20261203)
+    bs = BatchSolver(device=local)
+    for p in probs:
+        bs.add_problem(p)
+    for _ in range(args.warmup):
+        bs.solve(m=args.m, rtol=args.rtol)
+    torch.cuda.synchronize()
+    ms, it = [], None
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            it = bs.solve(m=args.m, rtol=args.rtol)
+            ms.append(bs.info()["last_ms"])
+    info = bs.info()
+    t = float(np.sum(ms))
+    NE = np.array([p.mesh.NE for p in probs])
+    NI = np.array([p.NI for p in probs])
+    upd = float(sum(int(NE[i]) * int(NI[i]) * int(it[i].sum()) for i in range(len(probs))))
+    line = {"metric": "batched dose solves (config3): 64 independent problems per step", "value": 64 * args.steps / (t / 1e3),
+            "unit": "dose solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t / args.steps, "higher_is_better": True, "dtype": "f32 sweep / split-bf16 moments / f64 Krylov",
+            "data": "synthetic",
+            "config": {"workload": "64 problems: hexes per axis U{8..32} x 6 tets, S8/S12/S16, 1-10 groups, P3, "
+                                   f"GMRES({args.m}) to {args.rtol:g}, seed 20261203",
+                       "tets_total": int(NE.sum()), "groups_total": int(sum(p.G for p in probs))},
+            "updates_per_s": upd / (t / args.steps / 1e3) / args.steps * args.steps,
+            "operator_applications": int(it.sum()), "sweep_threads": info["sweep_threads"],
+            "graph_launches": info["graph_launches"], "sweep_launches": info["sweep_launches"],
+            "clocks": clocks.summary()}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    bs.close()
+    return 0
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -422,6 +591,10 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "gemm":
+        return run_gemm(args)
+    if args.workload == "batch":
+        return run_batch(args)
     return run_ours(args)
 
 

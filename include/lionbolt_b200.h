@@ -114,6 +114,16 @@ int lb_transport_inv(lb_handle* h, double* s);
  * stream capture.  All calls on a device share the array: calls that overlap on the GPU race. */
 int lb_transport_inv_noalloc(lb_handle* h, float* psi);
 
+/* The two halves of K on caller-owned device arrays of the handle's GPU, asynchronous on the
+ * handle's stream (lb_synchronize waits):
+ *   lb_m2d_device: psi[i][n] = sum_j Y_j(k_i) sigma_l(j)(mat(n)) phi[j][n]   (phi FP64 [nm][NENK],
+ *                  psi FP32 [NI][NENK]; moment-to-discrete with the current cross sections)
+ *   lb_d2m_device: phi[j][n] = sum_i w_i Y_j(k_i) psi[i][n]                  (discrete-to-moment)
+ * Both are split-BF16 tensor-core contractions (six BF16 products per term, FP32 accumulation).
+ * With sigma_l = 1 they are the plain GEMMs Y phi and (wY)^T psi of ScatteringAlgebra.f90:13-55. */
+int lb_m2d_device(lb_handle* h, const double* phi, float* psi);
+int lb_d2m_device(lb_handle* h, const float* psi, double* phi);
+
 /* K x in place: replaces ScatteringOp%MatVec (ScatteringOperator.f90:39-70 ->
  * ScatteringAlgebra.f90:13-55).  Evaluated as moment-to-discrete (discrete-to-moment (x)). */
 int lb_scatter_apply(lb_handle* h, double* x);
@@ -156,8 +166,9 @@ int lb_reset_timers(lb_handle* h);
 /* Algorithmic traffic of one full sweep (bytes) and its update count (NE*NI). */
 int lb_sweep_stats(lb_handle* h, double* bytes_per_sweep, double* updates_per_sweep, long long* upstream_faces);
 int lb_synchronize(lb_handle* h);
-/* Sweep launch shape picked by the autotuner: cfg[0] schedule (0 levels, 1 dataflow), cfg[1]
- * threads per CTA, cfg[2] directions per CTA, cfg[3] updates in flight per thread.  Returns
+/* Sweep launch shape picked by the autotuner: cfg[0] schedule (0 levels, 1 dataflow, 2 levels with
+ * next-level prefetch, 3 element flags, 4 grouped directions), cfg[1] threads per CTA, cfg[2]
+ * directions per CTA, cfg[3] updates in flight per thread.  Returns
  * LB_ERR_STATE while candidates are still being timed (the first sweeps of a handle). */
 int lb_get_sweep_config(lb_handle* h, int* cfg);
 
@@ -199,6 +210,32 @@ int lb_lp_clear_samples(lb_handle* h);
 /* `steps` Adam steps (cosine-decayed learning rate from lr to lr/20) on batches of `batch` samples
  * drawn from the training set; loss_hist[steps] (optional) receives the batch losses. */
 int lb_lp_train(lb_handle* h, int steps, int batch, double lr, unsigned long long seed, double* loss_hist);
+
+
+/* ---- Batched dose solves (no counterpart in the reference, which runs one problem per process) ---
+ * Many independent multigroup problems -- own mesh, quadrature, cross sections and beam each -- on
+ * one GPU.  Groups and GMRES(m) steps advance in lock step over the problems; one persistent sweep
+ * launch covers every (problem, direction) pair; the matrix-vector product of an Arnoldi step is
+ * replayed from a CUDA graph; converged problems drop out through a device-side mask. */
+typedef struct lb_batch lb_batch;
+int lb_batch_create(int device, lb_batch** out);
+int lb_batch_destroy(lb_batch* b);
+int lb_batch_last_error(const lb_batch* b, char* buf, int len);
+/* Adds a problem (arguments as lb_set_mesh + lb_set_quadrature + lb_mg_set_problem); *id = index. */
+int lb_batch_add_problem(lb_batch* b, int NE, int NN, const double* rg, const int* node, const int* neighbors,
+                         const int* mat, int Nm, int NI, const double* k, const double* w, int G, int Ls,
+                         const double* sigt, const double* sigs, const double* dd, const double* unc,
+                         const double* beam_dir, int* id);
+/* GMRES(m) dose solve of every problem; iters[P][Gmax] (optional) receives operator applications
+ * per problem and group (0 for groups a problem does not have).  Returns the first nonzero Krylov
+ * status of any problem (all problems are still solved). */
+int lb_batch_solve(lb_batch* b, int m, double rtol, double atol, int maxit, int* iters);
+/* flux[G][NENK], dose[NENK] of problem id (either may be NULL). */
+int lb_batch_get_results(lb_batch* b, int id, double* flux, double* dose);
+/* Problem count, largest group count, device time of the last solve (ms), sweep threads picked by
+ * the tuner, graph replays and batched sweep launches so far.  Any pointer may be NULL. */
+int lb_batch_info(lb_batch* b, int* nproblems, int* max_groups, double* last_ms, int* sweep_threads,
+                  long long* graph_launches, long long* sweep_launches);
 
 #ifdef __cplusplus
 }

@@ -67,6 +67,18 @@ SIGNATURES = {
     "lb_mark": (ctypes.c_int, [_vp, ctypes.c_int]),
     "lb_transport_inv_noalloc": (ctypes.c_int, [_vp, ctypes.c_void_p]),
     "lb_elapsed_ms": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _c_double_p]),
+    "lb_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp)]),
+    "lb_batch_destroy": (ctypes.c_int, [_vp]),
+    "lb_batch_last_error": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_int]),
+    "lb_batch_add_problem": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _c_double_p, _c_int_p, _c_int_p, _c_int_p,
+                                            ctypes.c_int, ctypes.c_int, _c_double_p, _c_double_p, ctypes.c_int,
+                                            ctypes.c_int, _c_double_p, _c_double_p, _c_double_p, _c_double_p,
+                                            _c_double_p, _c_int_p]),
+    "lb_batch_solve": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, _c_int_p]),
+    "lb_batch_get_results": (ctypes.c_int, [_vp, ctypes.c_int, _c_double_p, _c_double_p]),
+    "lb_batch_info": (ctypes.c_int, [_vp, _c_int_p, _c_int_p, _c_double_p, _c_int_p, _c_ll_p, _c_ll_p]),
+    "lb_m2d_device": (ctypes.c_int, [_vp, ctypes.c_void_p, ctypes.c_void_p]),
+    "lb_d2m_device": (ctypes.c_int, [_vp, ctypes.c_void_p, ctypes.c_void_p]),
     "lb_lp_nparams": (ctypes.c_int, []),
     "lb_lp_init": (ctypes.c_int, [_vp, ctypes.c_ulonglong]),
     "lb_lp_set_weights": (ctypes.c_int, [_vp, _c_float_p]),
@@ -179,8 +191,10 @@ class Handle:
         st = self.lib.lb_get_sweep_config(self.h, iptr(cfg))
         if st != LB_OK:
             return None
-        return dict(schedule=("levels", "dataflow")[int(cfg[0])], threads=int(cfg[1]), dirs_per_cta=int(cfg[2]),
-                    ilp=int(cfg[3]))
+        names = ("levels", "dataflow", "levels+prefetch", "element flags", "grouped directions")
+        kind = int(cfg[0])
+        return dict(schedule=names[kind] if 0 <= kind < len(names) else str(kind), threads=int(cfg[1]),
+                    dirs_per_cta=int(cfg[2]), ilp=int(cfg[3]))
 
     def mark(self, slot):
         self.call("lb_mark", int(slot))

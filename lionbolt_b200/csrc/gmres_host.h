@@ -1,0 +1,82 @@
+// Host-side bookkeeping of restarted GMRES / FGMRES: Hessenberg columns, Givens rotations and the
+// back-substitution, following SPARSKIT gmres/fgmres (third_party/SPARSKIT/iters.f:1901-2206,
+// 2511-2795; givens :3225-3262).  The device does the vector work; one instance per problem.
+#pragma once
+#include <cmath>
+#include <vector>
+
+namespace lb {
+
+struct GmresHost {
+    int m = 0;
+    std::vector<std::vector<double>> H;   // H[col][row], 1-based rows as in SPARSKIT
+    std::vector<double> c, s, rs;
+
+    explicit GmresHost(int m_ = 0) { resize(m_); }
+
+    void resize(int m_) {
+        m = m_;
+        H.assign(m + 2, std::vector<double>(m + 2, 0.0));
+        c.assign(m + 2, 0.0);
+        s.assign(m + 2, 0.0);
+        rs.assign(m + 2, 0.0);
+    }
+
+    // start of a cycle with residual norm alpha
+    void start(double alpha) { rs[1] = alpha; }
+
+    // Column k (1-based) with projections hh[0..k-1] on v_1..v_k and subdiagonal hk: applies the
+    // previous rotations, forms the new one (SPARSKIT givens) and returns |rs[k+1]|, the residual
+    // estimate after k steps.
+    double add_column(int k, const double* hh, double hk) {
+        for (int i = 0; i < k; ++i) H[k][i + 1] = hh[i];
+        H[k][k + 1] = hk;
+        for (int i = 1; i <= k - 1; ++i) {
+            const double a = H[k][i];
+            H[k][i] = c[i] * a + s[i] * H[k][i + 1];
+            H[k][i + 1] = c[i] * H[k][i + 1] - s[i] * a;
+        }
+        double x = H[k][k], y = H[k][k + 1], cc, ss;
+        if (x == 0.0 && y == 0.0) {
+            cc = 1.0;
+            ss = 0.0;
+        } else if (std::fabs(y) > std::fabs(x)) {
+            const double t = x / y;
+            x = std::sqrt(1.0 + t * t);
+            ss = std::copysign(1.0 / x, y);
+            cc = t * ss;
+        } else {
+            const double t = y / x;
+            y = std::sqrt(1.0 + t * t);
+            cc = std::copysign(1.0 / y, x);
+            ss = t * cc;
+        }
+        H[k][k] = std::fabs(x * y);
+        H[k][k + 1] = 0.0;
+        c[k] = cc;
+        s[k] = ss;
+        const double a = -ss * rs[k];
+        rs[k] = cc * rs[k];
+        rs[k + 1] = a;
+        return std::fabs(a);
+    }
+
+    // Back-substitution over the first k columns, dropping trailing columns with a zero diagonal.
+    // Returns the number of columns kept (0: nothing to update) and the solution-update
+    // coefficients coef[i] = -y_i (for the multi-axpy x -= sum coef_i v_i).
+    int solve(int k, std::vector<double>& coef) {
+        while (k > 0 && H[k][k] == 0.0) --k;
+        coef.clear();
+        if (k == 0) return 0;
+        rs[k] = rs[k] / H[k][k];
+        for (int i = k - 1; i >= 1; --i) {
+            for (int ii = 1; ii <= i; ++ii) rs[ii] = rs[ii] - rs[i + 1] * H[i + 1][ii];
+            rs[i] = rs[i] / H[i][i];
+        }
+        coef.resize(k);
+        for (int i = 0; i < k; ++i) coef[i] = -rs[i + 1];
+        return k;
+    }
+};
+
+}  // namespace lb

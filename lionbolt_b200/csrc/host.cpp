@@ -72,16 +72,18 @@ void real_sh(int Ls, const double* dir, double* Y) {
 }
 
 void timer_begin(Handle* h, int kind, Timer& t) {
-    if (!h->free_timers.empty()) { t = h->free_timers.back(); h->free_timers.pop_back(); }
-    else { cudaEventCreate(&t.a); cudaEventCreate(&t.b); }
     t.kind = kind;
+    if (!h->timing) { t.a = t.b = nullptr; return; }
+    if (!h->free_timers.empty()) { t = h->free_timers.back(); h->free_timers.pop_back(); t.kind = kind; }
+    else { cudaEventCreate(&t.a); cudaEventCreate(&t.b); }
     cudaEventRecord(t.a, h->stream);
 }
 
 void timer_end(Handle* h, Timer& t) {
+    h->launches[t.kind] += 1;
+    if (!t.a) return;
     cudaEventRecord(t.b, h->stream);
     h->timers.push_back(t);
-    h->launches[t.kind] += 1;
 }
 
 void timers_flush(Handle* h) {
@@ -125,6 +127,8 @@ static void free_all(Handle* h) {
                     h->d_sigl_mg, h->d_yb, h->d_dd};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (h->h_red) cudaFreeHost(h->h_red);
+    if (h->d_seg) cudaFree(h->d_seg);
+    if (h->h_seg) cudaFreeHost(h->h_seg);
     for (auto& t : h->timers) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
     for (auto& t : h->free_timers) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
     for (auto& m : h->marks) if (m) cudaEventDestroy(m);

@@ -3,6 +3,9 @@
 // (third_party/SPARSKIT/iters.f: gmres :1901-2206, mgsro :3465-3587) and Main.f90.
 // Reductions are deterministic: fixed grid, per-block partials summed on the host in block order.
 #include "lb_internal.h"
+#include <algorithm>
+#include <cmath>
+#include <cstring>
 #include <type_traits>
 
 namespace lb {
@@ -272,6 +275,110 @@ __global__ void dose_kernel(const double* __restrict__ phi00, const double* __re
     }
 }
 
+// ---- segmented (per-problem) versions for batches: block b belongs to the segment whose
+// [blk0, blk0 + nblk) contains it; the segment table is small (one entry per problem).
+__device__ __forceinline__ int seg_of_block(const SegVec* segs, int nseg) {
+    int s = 0;
+    while (s + 1 < nseg && (int)blockIdx.x >= segs[s + 1].blk0) ++s;
+    return s;
+}
+
+template <int NV>
+__global__ void __launch_bounds__(kRedThreads) seg_dots_t(const SegVec* __restrict__ segs, int nseg, double* partial) {
+    const SegVec S = segs[seg_of_block(segs, nseg)];
+    double acc[NV + 1];
+#pragma unroll
+    for (int j = 0; j <= NV; ++j) acc[j] = 0.0;
+    const double2* w2 = reinterpret_cast<const double2*>(S.w);
+    const size_t stride = (size_t)S.nblk * blockDim.x;
+    for (size_t q = (size_t)(blockIdx.x - S.blk0) * blockDim.x + threadIdx.x; q < S.n2; q += stride) {
+        const double2 wq = __ldcs(w2 + q);
+        double2 v[NV > 0 ? NV : 1];
+#pragma unroll
+        for (int j = 0; j < NV; ++j) v[j] = __ldcs(reinterpret_cast<const double2*>(S.V + (size_t)j * S.ldv) + q);
+#pragma unroll
+        for (int j = 0; j < NV; ++j) acc[j] = fma(v[j].x, wq.x, fma(v[j].y, wq.y, acc[j]));
+        acc[NV] = fma(wq.x, wq.x, fma(wq.y, wq.y, acc[NV]));
+    }
+    block_reduce_store<NV>(acc, partial);
+}
+
+template <int NV, bool DOTS>
+__global__ void __launch_bounds__(kRedThreads) seg_axpy_dots_t(const SegVec* __restrict__ segs, int nseg,
+                                                              const double* __restrict__ coef, double* partial) {
+    const SegVec S = segs[seg_of_block(segs, nseg)];
+    double c[NV > 0 ? NV : 1];
+#pragma unroll
+    for (int j = 0; j < NV; ++j) c[j] = coef[S.coef + j];
+    double acc[NV + 1];
+#pragma unroll
+    for (int j = 0; j <= NV; ++j) acc[j] = 0.0;
+    double2* w2 = reinterpret_cast<double2*>(S.w);
+    const size_t stride = (size_t)S.nblk * blockDim.x;
+    for (size_t q = (size_t)(blockIdx.x - S.blk0) * blockDim.x + threadIdx.x; q < S.n2; q += stride) {
+        double2 x = w2[q];
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            const double2 v = __ldg(reinterpret_cast<const double2*>(S.V + (size_t)j * S.ldv) + q);
+            x.x = fma(-c[j], v.x, x.x);
+            x.y = fma(-c[j], v.y, x.y);
+        }
+        w2[q] = x;
+        if constexpr (DOTS) {
+#pragma unroll
+            for (int j = 0; j < NV; ++j) {
+                const double2 v = __ldg(reinterpret_cast<const double2*>(S.V + (size_t)j * S.ldv) + q);
+                acc[j] = fma(v.x, x.x, fma(v.y, x.y, acc[j]));
+            }
+        }
+        acc[NV] = fma(x.x, x.x, fma(x.y, x.y, acc[NV]));
+    }
+    block_reduce_store<NV>(acc, partial);
+}
+
+template <int NV>
+__global__ void __launch_bounds__(kRedThreads) seg_axpy_scale_t(const SegVec* __restrict__ segs, int nseg,
+                                                               const double* __restrict__ coef) {
+    const SegVec S = segs[seg_of_block(segs, nseg)];
+    double c[NV > 0 ? NV : 1];
+#pragma unroll
+    for (int j = 0; j < NV; ++j) c[j] = coef[S.coef + j];
+    double2* w2 = reinterpret_cast<double2*>(S.w);
+    double2* o2 = reinterpret_cast<double2*>(S.w2);
+    const size_t stride = (size_t)S.nblk * blockDim.x;
+    for (size_t q = (size_t)(blockIdx.x - S.blk0) * blockDim.x + threadIdx.x; q < S.n2; q += stride) {
+        double2 x = w2[q];
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            const double2 v = __ldcs(reinterpret_cast<const double2*>(S.V + (size_t)j * S.ldv) + q);
+            x.x = fma(-c[j], v.x, x.x);
+            x.y = fma(-c[j], v.y, x.y);
+        }
+        x.x *= S.scale;
+        x.y *= S.scale;
+        w2[q] = x;
+        if (o2) o2[q] = x;
+    }
+}
+
+__global__ void __launch_bounds__(kRedThreads) seg_axpby_norm_kernel(const SegVec* __restrict__ segs, int nseg,
+                                                                    double* partial) {
+    const SegVec S = segs[seg_of_block(segs, nseg)];
+    double acc[1] = {0.0};
+    double2* y2 = reinterpret_cast<double2*>(S.w);
+    const double2* x2 = reinterpret_cast<const double2*>(S.x);
+    const size_t stride = (size_t)S.nblk * blockDim.x;
+    for (size_t q = (size_t)(blockIdx.x - S.blk0) * blockDim.x + threadIdx.x; q < S.n2; q += stride) {
+        const double2 u = __ldcs(x2 + q);
+        double2 v = y2[q];
+        v.x = S.a * u.x + S.b * v.x;
+        v.y = S.a * u.y + S.b * v.y;
+        y2[q] = v;
+        acc[0] = fma(v.x, v.x, fma(v.y, v.y, acc[0]));
+    }
+    block_reduce_store<0>(acc, partial);
+}
+
 inline int grid_for(Handle* h, size_t n) {
     size_t g = (n + 255) / 256;
     size_t cap = (size_t)h->sm_count * 8;
@@ -479,6 +586,127 @@ int k_dose_tally(Handle* h, const double* phi00, const double* unc, double unc_s
     dose_kernel<<<grid_for(h, (size_t)NENK), 256, 0, h->stream>>>(phi00, unc, unc_scale, dd_mat, mat, flux, dose, NENK);
     timer_end(h, t);
     return LB_OK;
+}
+
+
+// ---------------------------------------------------------------------------------------------
+//  segmented operations of a batch
+// ---------------------------------------------------------------------------------------------
+int seg_assign_blocks(std::vector<SegVec>& segs, int blocks) {
+    double tot = 0.0;
+    for (auto& sg : segs) tot += (double)sg.n2;
+    int b0 = 0;
+    for (auto& sg : segs) {
+        int nb = (int)std::floor((double)blocks * (double)sg.n2 / std::max(tot, 1.0));
+        nb = std::max(nb, 1);
+        sg.blk0 = b0;
+        sg.nblk = nb;
+        b0 += nb;
+    }
+    return b0;
+}
+
+// Uploads the segment table (and coefficients) through the handle's pinned staging area.
+static int seg_upload(Handle* h, const std::vector<SegVec>& segs, const std::vector<double>* coef, SegVec** dsegs,
+                      double** dcoef) {
+    const size_t sb = sizeof(SegVec) * segs.size();
+    const size_t cb = coef ? sizeof(double) * coef->size() : 0;
+    const size_t need = sb + cb + 64;
+    if (need > h->seg_bytes) {
+        if (h->d_seg) cudaFree(h->d_seg);
+        if (h->h_seg) cudaFreeHost(h->h_seg);
+        h->d_seg = nullptr;
+        h->h_seg = nullptr;
+        h->seg_bytes = 0;
+        const size_t cap = std::max<size_t>(need * 2, 1 << 16);
+        if (cudaMalloc(&h->d_seg, cap) != cudaSuccess || cudaMallocHost(&h->h_seg, cap) != cudaSuccess)
+            return fail(h, LB_ERR_OOM, "segment tables");
+        h->seg_bytes = cap;
+    }
+    // the staging buffer is reused by the next call: wait for the previous upload to be consumed
+    cudaStreamSynchronize(h->stream);
+    unsigned char* hb = reinterpret_cast<unsigned char*>(h->h_seg);
+    std::memcpy(hb, segs.data(), sb);
+    const size_t coff = (sb + 15) / 16 * 16;
+    if (cb) std::memcpy(hb + coff, coef->data(), cb);
+    cudaError_t e = cudaMemcpyAsync(h->d_seg, hb, coff + cb, cudaMemcpyHostToDevice, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "segment upload");
+    *dsegs = reinterpret_cast<SegVec*>(h->d_seg);
+    if (dcoef) *dcoef = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(h->d_seg) + coff);
+    return LB_OK;
+}
+
+static int seg_reduce(Handle* h, const std::vector<SegVec>& segs, int cnt, std::vector<double>& out) {
+    const int grid = segs.back().blk0 + segs.back().nblk;
+    cudaError_t e = cudaMemcpyAsync(h->h_red, h->d_red, sizeof(double) * (size_t)grid * kPartStride,
+                                    cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "segmented reduction");
+    out.assign(segs.size() * (size_t)cnt, 0.0);
+    for (size_t si = 0; si < segs.size(); ++si)
+        for (int j = 0; j < cnt; ++j) {
+            double acc = 0.0;
+            for (int b = segs[si].blk0; b < segs[si].blk0 + segs[si].nblk; ++b) acc += h->h_red[(size_t)b * kPartStride + j];
+            out[si * cnt + j] = acc;
+        }
+    return LB_OK;
+}
+
+int seg_dots_norm(Handle* h, const std::vector<SegVec>& segs, int nv, std::vector<double>& out) {
+    if (segs.empty()) { out.clear(); return LB_OK; }
+    if (nv < 0 || nv > kMaxDots) return fail(h, LB_ERR_ARG, "segmented dots: too many vectors");
+    SegVec* ds = nullptr;
+    int rc = seg_upload(h, segs, nullptr, &ds, nullptr);
+    if (rc) return rc;
+    const int grid = segs.back().blk0 + segs.back().nblk;
+    NvDispatch<kMaxDots>::run(nv, [&](auto c) {
+        constexpr int NV = decltype(c)::value;
+        seg_dots_t<NV><<<grid, kRedThreads, 0, h->stream>>>(ds, (int)segs.size(), h->d_red);
+    });
+    return seg_reduce(h, segs, nv + 1, out);
+}
+
+int seg_axpy_dots(Handle* h, const std::vector<SegVec>& segs, int nv, const std::vector<double>& coef, bool dots,
+                  std::vector<double>& out) {
+    if (segs.empty()) { out.clear(); return LB_OK; }
+    if (nv < 0 || nv > kMaxDots) return fail(h, LB_ERR_ARG, "segmented axpy: too many vectors");
+    SegVec* ds = nullptr;
+    double* dc = nullptr;
+    int rc = seg_upload(h, segs, &coef, &ds, &dc);
+    if (rc) return rc;
+    const int grid = segs.back().blk0 + segs.back().nblk;
+    NvDispatch<kMaxDots>::run(nv, [&](auto c) {
+        constexpr int NV = decltype(c)::value;
+        if (dots) seg_axpy_dots_t<NV, true><<<grid, kRedThreads, 0, h->stream>>>(ds, (int)segs.size(), dc, h->d_red);
+        else seg_axpy_dots_t<NV, false><<<grid, kRedThreads, 0, h->stream>>>(ds, (int)segs.size(), dc, h->d_red);
+    });
+    return seg_reduce(h, segs, nv + 1, out);
+}
+
+int seg_axpy_scale(Handle* h, const std::vector<SegVec>& segs, int nv, const std::vector<double>& coef) {
+    if (segs.empty()) return LB_OK;
+    if (nv < 0 || nv > kMaxDots) return fail(h, LB_ERR_ARG, "segmented axpy: too many vectors");
+    SegVec* ds = nullptr;
+    double* dc = nullptr;
+    int rc = seg_upload(h, segs, &coef, &ds, &dc);
+    if (rc) return rc;
+    const int grid = segs.back().blk0 + segs.back().nblk;
+    NvDispatch<kMaxDots>::run(nv, [&](auto c) {
+        constexpr int NV = decltype(c)::value;
+        seg_axpy_scale_t<NV><<<grid, kRedThreads, 0, h->stream>>>(ds, (int)segs.size(), dc);
+    });
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? LB_OK : cuda_fail(h, e, "segmented axpy");
+}
+
+int seg_axpby_norm(Handle* h, const std::vector<SegVec>& segs, std::vector<double>& out) {
+    if (segs.empty()) { out.clear(); return LB_OK; }
+    SegVec* ds = nullptr;
+    int rc = seg_upload(h, segs, nullptr, &ds, nullptr);
+    if (rc) return rc;
+    const int grid = segs.back().blk0 + segs.back().nblk;
+    seg_axpby_norm_kernel<<<grid, kRedThreads, 0, h->stream>>>(ds, (int)segs.size(), h->d_red);
+    return seg_reduce(h, segs, 1, out);
 }
 
 }  // namespace lb

@@ -156,6 +156,15 @@ struct Handle {
 
     // learned preconditioner state (mlp.cu)
     void* mlp = nullptr;
+
+    // batched solves (batch.cpp): a problem of a batch records no CUDA events (its launches may be
+    // captured into graphs) and its moment kernels skip their work while *d_active == 0
+    bool timing = true;
+    const int* d_active = nullptr;
+    // staging of segment tables for the segmented vector operations (krylov.cu)
+    void* d_seg = nullptr;
+    void* h_seg = nullptr;
+    size_t seg_bytes = 0;
 };
 
 // ---- host helpers (host.cpp) ----
@@ -183,6 +192,62 @@ inline void allow_max_dynamic_smem(K kernel) {
     if (dyn > 0) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
     cudaGetLastError();
 }
+
+// Squared norm of an Arnoldi vector after classical Gram-Schmidt with selective re-orthogonalisation
+// (solve.cpp); a negative value asks for an exact norm.
+double cgs2_norm(double nrm0, double nrm1, const double* h2, int k, bool* reorth);
+
+// Krylov workspace of a handle for restart length m (solve.cpp)
+int ensure_krylov(Handle* h, int m, bool flexible);
+// multigroup helpers (solve.cpp): transfer table sigma_l(j) of g' -> g, beam harmonics, and the
+// group source + within-group cross sections of group g (from the solved groups below it)
+float* mg_table(Handle* h, int gp, int g);
+void mg_prepare(Handle* h);
+int mg_group_sources(Handle* h, int g);
+
+// ---- batched solves ----
+// One work item of the batched sweep: one direction of one problem of a batch.
+struct BatchWork {
+    const int* items;       // [NE] packed schedule items of the direction
+    const int* lvl_start;   // [nlev + 1] level starts of the direction
+    const float4* geom;     // the problem's element records
+    const float* sigt;      // the problem's per-material total cross sections (device, FP32)
+    float* psi;             // the problem's angular vector, block of this direction
+    float4 dir;             // (kx, ky, kz, w)
+    int nlev;
+    int Nm;
+    int problem;
+    int pad;
+};
+// Sweeps every work item whose problem has active[problem] != 0, CTAs claiming items in order from
+// *counter (reset before the launch).  threads: 1024 or 512.
+int launch_sweep_batch(cudaStream_t s, const BatchWork* work, int nwork, int* counter, const int* active,
+                       int threads, int sm_count);
+
+// Segmented (per-problem) FP64 vector operations of a batch: one launch for all problems.
+struct SegVec {
+    double* w;              // target vector (updated / dotted)
+    const double* V;        // nv basis vectors, stride ldv
+    const double* x;        // second operand of axpby
+    double* w2;             // optional second destination of axpy_scale
+    size_t ldv;
+    size_t n2;              // vector length / 2
+    int blk0, nblk;         // blocks of the launch assigned to this problem
+    int coef;               // offset of this problem's coefficients
+    int pad;
+    double scale, a, b;
+};
+// Builds block ranges proportional to the vector lengths for a grid of `blocks`.
+int seg_assign_blocks(std::vector<SegVec>& segs, int blocks);
+// out[s][j] = V_j . w (j < nv) and out[s][nv] = w . w, for every segment s
+int seg_dots_norm(Handle* h, const std::vector<SegVec>& segs, int nv, std::vector<double>& out);
+// w -= sum_j c[s][j] V_j; out[s][j] = V_j . w (if dots) and out[s][nv] = w . w
+int seg_axpy_dots(Handle* h, const std::vector<SegVec>& segs, int nv, const std::vector<double>& coef, bool dots,
+                  std::vector<double>& out);
+// w = (w - sum_j c[s][j] V_j) * scale (also written to w2 when non-null)
+int seg_axpy_scale(Handle* h, const std::vector<SegVec>& segs, int nv, const std::vector<double>& coef);
+// w = a x + b w and out[s] = w . w
+int seg_axpby_norm(Handle* h, const std::vector<SegVec>& segs, std::vector<double>& out);
 
 // ---- timers ----
 void timer_begin(Handle* h, int kind, Timer& t);

@@ -58,11 +58,12 @@ __host__ __device__ __forceinline__ int smem_stride_words(int kpad) {
 // A = Y planes [3][NIpad][nmpad] (global, L1-resident), B = xt tile in smem as [3][n][j].
 // Warp w computes all direction tiles for the 8 nodes of n8 tile w.
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) m2d_kernel(const double* __restrict__ x, const float* __restrict__ sigl,
+__global__ void __launch_bounds__(kThreads) m2d_kernel(const int* __restrict__ active, const double* __restrict__ x, const float* __restrict__ sigl,
                                                       const double* __restrict__ add, const float* __restrict__ qadd,
                                                       const int* __restrict__ mat, const __nv_bfloat16* __restrict__ Y,
                                                       float* __restrict__ q, long long NENK, int NI, int NIpad,
                                                       int nm, int nmpad, long long ntiles) {
+    if (active && *active == 0) return;   // problem of a batch that has converged
     extern __shared__ __align__(16) uint32_t smem[];
     const int sw = smem_stride_words(nmpad);            // words per node row
     uint32_t* Bs = smem;                                  // [3][kTileN][sw]
@@ -134,10 +135,11 @@ __global__ void __launch_bounds__(kThreads) m2d_kernel(const double* __restrict_
 // A = Dw planes [3][nmpad][NIpad] (global), B = psi tile split into smem as [3][n][i].
 // ---------------------------------------------------------------------------------------------
 template <int MT>
-__global__ void __launch_bounds__(kThreads) d2m_kernel(const float* __restrict__ psi, const __nv_bfloat16* __restrict__ Dw,
+__global__ void __launch_bounds__(kThreads) d2m_kernel(const int* __restrict__ active, const float* __restrict__ psi, const __nv_bfloat16* __restrict__ Dw,
                                                       const double* __restrict__ xin, double alpha, double beta,
                                                       double* __restrict__ out, long long NENK, int NI, int NIpad,
                                                       int nm, int nmpad, long long ntiles) {
+    if (active && *active == 0) return;   // problem of a batch that has converged
     extern __shared__ __align__(16) uint32_t smem[];
     const int sw = smem_stride_words(NIpad);
     uint32_t* Bs = smem;                                  // [3][kTileN][sw]
@@ -256,11 +258,12 @@ __device__ __forceinline__ void stage_planes(const __nv_bfloat16* __restrict__ g
 // M2D: q[i][n] = sum_j Y[i][j] xt[j][n] (+ qadd),  xt = sigl[mat(n)][j] x[j][n] + a[j][n].
 // Warp w owns nodes n0 + 8w .. +7 of the 64-node tile; its B fragments for all K stay in registers.
 template <int KT>
-__global__ void __launch_bounds__(kThreads) m2d_stream_kernel(const double* __restrict__ x, const float* __restrict__ sigl,
+__global__ void __launch_bounds__(kThreads) m2d_stream_kernel(const int* __restrict__ active, const double* __restrict__ x, const float* __restrict__ sigl,
                                                              const double* __restrict__ add, const float* __restrict__ qadd,
                                                              const int* __restrict__ mat, const __nv_bfloat16* __restrict__ Y,
                                                              float* __restrict__ q, long long NENK, int NI, int NIpad,
                                                              int nm, int nmpad, long long ntiles) {
+    if (active && *active == 0) return;   // problem of a batch that has converged
     extern __shared__ __align__(16) __nv_bfloat16 ys[];     // [3][NIpad][nmpad + 8]
     stage_planes(Y, ys, NIpad, nmpad);
     const int rs = nmpad + 8;
@@ -320,10 +323,11 @@ __global__ void __launch_bounds__(kThreads) m2d_stream_kernel(const double* __re
 // D2M: z[j][n] = sum_i Dw[j][i] psi[i][n];  out = alpha * xin + beta * z.
 // Warp w owns nodes n0 + 8w .. +7; psi fragments stream from HBM one k-step ahead of the MMAs.
 template <int MT>
-__global__ void __launch_bounds__(kThreads) d2m_stream_kernel(const float* __restrict__ psi, const __nv_bfloat16* __restrict__ Dw,
+__global__ void __launch_bounds__(kThreads) d2m_stream_kernel(const int* __restrict__ active, const float* __restrict__ psi, const __nv_bfloat16* __restrict__ Dw,
                                                              const double* xin, double alpha, double beta, double* out,
                                                              long long NENK, int NI, int NIpad, int nm, int nmpad,
                                                              long long ntiles) {
+    if (active && *active == 0) return;   // problem of a batch that has converged
     extern __shared__ __align__(16) __nv_bfloat16 ds[];     // [3][nmpad][NIpad + 8]
     stage_planes(Dw, ds, nmpad, NIpad);
     const int rs = NIpad + 8;
@@ -393,7 +397,7 @@ int run_d2m(Handle* h, const float* psi, const double* xin, double alpha, double
         allow_max_dynamic_smem(d2m_kernel<MT>);
         attr = true;
     }
-    d2m_kernel<MT><<<grid, kThreads, smem, h->stream>>>(psi, h->d_Yd2m, xin, alpha, beta, out, h->NENK, h->NI,
+    d2m_kernel<MT><<<grid, kThreads, smem, h->stream>>>(h->d_active, psi, h->d_Yd2m, xin, alpha, beta, out, h->NENK, h->NI,
                                                         h->NIpad, h->nm, h->nmpad, ntiles);
     return LB_OK;
 }
@@ -409,7 +413,7 @@ cudaError_t run_m2d_stream(Handle* h, const double* x, const float* sigl, const 
         if (per_sm < 1) per_sm = 1;
     }
     long long grid = std::min<long long>(ntiles, (long long)h->sm_count * per_sm);
-    m2d_stream_kernel<KT><<<(int)grid, kThreads, smem, h->stream>>>(x, sigl, a, qadd, h->d_mat, h->d_Ym2d, q, h->NENK,
+    m2d_stream_kernel<KT><<<(int)grid, kThreads, smem, h->stream>>>(h->d_active, x, sigl, a, qadd, h->d_mat, h->d_Ym2d, q, h->NENK,
                                                                     h->NI, h->NIpad, h->nm, h->nmpad, ntiles);
     return cudaGetLastError();
 }
@@ -424,7 +428,7 @@ cudaError_t run_d2m_stream(Handle* h, const float* psi, const double* xin, doubl
         if (per_sm < 1) per_sm = 1;
     }
     long long grid = std::min<long long>(ntiles, (long long)h->sm_count * per_sm);
-    d2m_stream_kernel<MT><<<(int)grid, kThreads, smem, h->stream>>>(psi, h->d_Yd2m, xin, alpha, beta, out, h->NENK,
+    d2m_stream_kernel<MT><<<(int)grid, kThreads, smem, h->stream>>>(h->d_active, psi, h->d_Yd2m, xin, alpha, beta, out, h->NENK,
                                                                     h->NI, h->NIpad, h->nm, h->nmpad, ntiles);
     return cudaGetLastError();
 }
@@ -464,7 +468,7 @@ int launch_m2d(Handle* h, const double* x, const float* sigl, const double* a, c
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, m2d_kernel, kThreads, smem);
         if (per_sm < 1) per_sm = 1;
         long long grid = std::min<long long>(ntiles, (long long)h->sm_count * per_sm);
-        m2d_kernel<<<(int)grid, kThreads, smem, h->stream>>>(x, sigl, a, qadd, h->d_mat, h->d_Ym2d, q, h->NENK, h->NI,
+        m2d_kernel<<<(int)grid, kThreads, smem, h->stream>>>(h->d_active, x, sigl, a, qadd, h->d_mat, h->d_Ym2d, q, h->NENK, h->NI,
                                                              h->NIpad, h->nm, h->nmpad, ntiles);
         e = cudaGetLastError();
     }

@@ -11,6 +11,7 @@
 // the reference's SPARSKIT gmres/fgmres; orthogonalisation is classical Gram-Schmidt with
 // selective re-orthogonalisation (one fused multi-dot and one fused multi-axpy per pass).
 #include "lb_internal.h"
+#include "gmres_host.h"
 #include <cmath>
 #include <cstring>
 #include <functional>
@@ -27,7 +28,7 @@ static int need_ready(Handle* h, bool phys = true) {
     return LB_OK;
 }
 
-static int ensure_krylov(Handle* h, int m, bool flexible) {
+int ensure_krylov(Handle* h, int m, bool flexible) {
     size_t n = (size_t)h->nm * (size_t)h->NENK;
     bool realloc_v = (h->kry_n != n) || (h->kry_m < m) || !h->d_V;
     if (realloc_v) {
@@ -95,6 +96,21 @@ struct KrylovResult {
 
 using DevOp = std::function<int(const double* in, double* out)>;
 
+// Squared norm of the Arnoldi vector after the second Gram-Schmidt pass.  nrm0 = |w|^2 before the
+// first projection, nrm1 = |w - V hh|^2, h2 = V^T (w - V hh).  When the first pass cancelled more
+// than half of |w|^2, the second pass is applied (*reorth = true) and |w - V hh - V h2|^2 =
+// nrm1 - |h2|^2 for orthonormal V; a negative return asks for an exact norm (near breakdown).
+double cgs2_norm(double nrm0, double nrm1, const double* h2, int k, bool* reorth) {
+    *reorth = false;
+    if (!(nrm1 < 0.5 * nrm0)) return nrm1;
+    double s2 = 0.0;
+    for (int i = 0; i < k; ++i) s2 += h2[i] * h2[i];
+    const double hk2 = nrm1 - s2;
+    if (!(hk2 > 1e-4 * nrm1)) return -1.0;
+    *reorth = true;
+    return hk2;
+}
+
 // Restarted GMRES(m) / FGMRES(m) (right preconditioner `prec`), SPARSKIT semantics.
 static KrylovResult gmres_device(Handle* h, size_t n, const double* rhs, double* sol, int m, double rtol, double atol,
                                  int maxit, const DevOp& matvec, const DevOp* prec) {
@@ -102,8 +118,8 @@ static KrylovResult gmres_device(Handle* h, size_t n, const double* rhs, double*
     int rc = 0;
     double* V = h->d_V;
     double* Z = h->d_Z;
-    std::vector<std::vector<double>> H(m + 2, std::vector<double>(m + 2, 0.0));   // H[col][row]
-    std::vector<double> c(m + 2), s(m + 2), rs(m + 2), hh(m + 2), h2(m + 2);
+    GmresHost gh(m);
+    std::vector<double> hh(m + 2), h2(m + 2), coef;
     double rn = vnorm(h, rhs, n, &rc);
     if (rc) { res.status = rc; return res; }
     const double fpar4 = rtol * rn + atol;
@@ -118,7 +134,7 @@ static KrylovResult gmres_device(Handle* h, size_t n, const double* rhs, double*
         alpha = std::sqrt(alpha);
         if (std::isnan(alpha)) { res.status = fail(h, LB_ERR_NAN, "RESIDUAL NORM is NaN."); return res; }
         fpar5 = alpha;
-        rs[1] = alpha;
+        gh.start(alpha);
         if (alpha <= fpar4) { res.status = LB_OK; res.nmv = nmv; res.resid = alpha; return res; }
         k_scale(h, V, 1.0 / alpha, n);
         int k = 0;
@@ -140,63 +156,38 @@ static KrylovResult gmres_device(Handle* h, size_t n, const double* rhs, double*
             double nrm0 = 0.0, nrm1 = 0.0;
             if ((rc = k_dots_norm(h, V, n, k, vk, n, hh.data(), &nrm0))) { res.status = rc; return res; }
             if ((rc = k_axpy_dots(h, vk, V, n, k, hh.data(), n, h2.data(), &nrm1))) { res.status = rc; return res; }
-            bool reorth = nrm1 < 0.5 * nrm0;
-            double hk2 = nrm1;
+            bool reorth = false;
+            double hk2 = cgs2_norm(nrm0, nrm1, h2.data(), k, &reorth);
             if (reorth) {
-                double s2 = 0.0;
-                for (int i = 0; i < k; ++i) s2 += h2[i] * h2[i];
-                hk2 = nrm1 - s2;
-                if (!(hk2 > 1e-4 * nrm1)) {
-                    // near breakdown: apply the correction and measure the norm exactly
-                    if ((rc = k_axpy_dots(h, vk, V, n, k, h2.data(), n, nullptr, &hk2))) { res.status = rc; return res; }
-                    reorth = false;
-                    for (int i = 0; i < k; ++i) hh[i] += h2[i];
-                } else {
-                    for (int i = 0; i < k; ++i) hh[i] += h2[i];
-                }
+                for (int i = 0; i < k; ++i) hh[i] += h2[i];
+            } else if (hk2 < 0.0) {
+                // near breakdown: apply the correction and measure the norm exactly
+                if ((rc = k_axpy_dots(h, vk, V, n, k, h2.data(), n, nullptr, &hk2))) { res.status = rc; return res; }
+                for (int i = 0; i < k; ++i) hh[i] += h2[i];
             }
-            double hk = std::sqrt(std::max(0.0, hk2));
+            const double hk = std::sqrt(std::max(0.0, hk2));
             if (std::isnan(hk)) { res.status = fail(h, LB_ERR_NAN, "RESIDUAL NORM is NaN."); return res; }
-            for (int i = 0; i < k; ++i) H[k][i + 1] = hh[i];
-            H[k][k + 1] = hk;
-            if (!(hk > 0.0)) { breakdown = true; --k; break; }
-            if ((rc = k_axpy_scale(h, vk, V, n, reorth ? k : 0, h2.data(), 1.0 / hk, n))) { res.status = rc; return res; }
-            for (int i = 1; i <= k - 1; ++i) {
-                double a = H[k][i];
-                H[k][i] = c[i] * a + s[i] * H[k][i + 1];
-                H[k][i + 1] = c[i] * H[k][i + 1] - s[i] * a;
+            if (!(hk > 0.0)) {
+                for (int i = 0; i < k; ++i) gh.H[k][i + 1] = hh[i];
+                gh.H[k][k + 1] = hk;
+                breakdown = true;
+                --k;
+                break;
             }
-            // SPARSKIT givens (iters.f:3225-3262)
-            double x = H[k][k], y = H[k][k + 1], cc, ss;
-            if (x == 0.0 && y == 0.0) { cc = 1.0; ss = 0.0; }
-            else if (std::fabs(y) > std::fabs(x)) { double t = x / y; x = std::sqrt(1.0 + t * t); ss = std::copysign(1.0 / x, y); cc = t * ss; }
-            else { double t = y / x; y = std::sqrt(1.0 + t * t); cc = std::copysign(1.0 / y, x); ss = t * cc; }
-            H[k][k] = std::fabs(x * y);
-            H[k][k + 1] = 0.0;
-            c[k] = cc; s[k] = ss;
-            double a = -ss * rs[k];
-            rs[k] = cc * rs[k];
-            rs[k + 1] = a;
-            alpha = std::fabs(a);
+            if ((rc = k_axpy_scale(h, vk, V, n, reorth ? k : 0, h2.data(), 1.0 / hk, n))) { res.status = rc; return res; }
+            alpha = gh.add_column(k, hh.data(), hk);
             fpar5 = alpha;
             if (k < m && !(alpha <= fpar4) && (maxit <= 0 || nmv < maxit)) continue;
             break;
         }
-        while (k > 0 && H[k][k] == 0.0) --k;
-        if (k == 0) {
+        const int kk = gh.solve(k, coef);
+        if (kk == 0) {
             if (breakdown) continue;   // nothing new in the basis: recompute the true residual
             res.status = fail(h, LB_ERR_BREAKDOWN, "GMRES : Anticipated breakdown / division by zero.");
             return res;
         }
-        rs[k] = rs[k] / H[k][k];
-        for (int i = k - 1; i >= 1; --i) {
-            for (int ii = 1; ii <= i; ++ii) rs[ii] = rs[ii] - rs[i + 1] * H[i + 1][ii];
-            rs[i] = rs[i] / H[i][i];
-        }
         // sol += sum_i y_i V_i (or Z_i): multi-axpy with negated coefficients
-        std::vector<double> coef(k);
-        for (int i = 0; i < k; ++i) coef[i] = -rs[i + 1];
-        if ((rc = k_multi_axpy(h, sol, prec ? Z : V, n, k, coef.data(), n))) { res.status = rc; return res; }
+        if ((rc = k_multi_axpy(h, sol, prec ? Z : V, n, kk, coef.data(), n))) { res.status = rc; return res; }
         if (breakdown) continue;
         if ((nmv < maxit || maxit <= 0) && fpar5 > fpar4) continue;
         res.nmv = nmv;
@@ -329,18 +320,19 @@ static int download_angular(Handle* h, const float* d, double* hs) {
 
 }  // namespace lb
 
-using namespace lb;
 struct lb_handle : public lb::Handle {};
+
+namespace lb {
 
 // ---------------------------------------------------------------------------------------------
 //  multigroup helpers (group loop of Main.f90:326-476)
 // ---------------------------------------------------------------------------------------------
-static float* mg_table(Handle* h, int gp, int g) {
+float* mg_table(Handle* h, int gp, int g) {
     return h->d_sigl_mg + (((size_t)gp * h->G + g) * h->Nm) * h->nmpad;
 }
 
 // Beam-direction harmonics Y_j(Omega_b) for the first-collision source.
-static void mg_prepare(Handle* h) {
+void mg_prepare(Handle* h) {
     std::vector<double> yb(h->nm);
     real_sh(h->Ls, h->beam_dir.data(), yb.data());
     cudaMemcpyAsync(h->d_yb, yb.data(), sizeof(double) * h->nm, cudaMemcpyHostToDevice, h->stream);
@@ -348,23 +340,30 @@ static void mg_prepare(Handle* h) {
 }
 
 // Source and operator of group g from the solved groups g' < g in d_phi_all:
-// d_src = sum_{g'<g} Sigma_{g'->g} phi_{g'} + first collision of the beam, the within-group cross
-// sections of g set on the handle, and d_b = D T^{-1} M d_src.
-static int mg_group_setup(Handle* h, int g) {
+// d_src = sum_{g'<g} Sigma_{g'->g} phi_{g'} + first collision of the beam, and the within-group
+// cross sections of g set on the handle.
+int mg_group_sources(Handle* h, int g) {
     const int G = h->G, Nm = h->Nm, Ls = h->Ls, nm = h->nm, nmpad = h->nmpad;
-    const size_t NENK = (size_t)h->NENK, n = h->kry_n;
-    (void)n;
-    k_group_source(h, h->d_src, h->d_phi_all, h->d_sigl_mg, G, g, h->d_unc, h->d_yb, h->d_mat, (long long)NENK, Nm, nm,
+    k_group_source(h, h->d_src, h->d_phi_all, h->d_sigl_mg, G, g, h->d_unc, h->d_yb, h->d_mat, h->NENK, Nm, nm,
                    nmpad);
     std::vector<double> st(h->mg_sigt.begin() + (size_t)g * Nm, h->mg_sigt.begin() + (size_t)(g + 1) * Nm);
     std::vector<double> ss((size_t)Nm * (Ls + 1));
     for (int mm = 0; mm < Nm; ++mm)
         for (int l = 0; l <= Ls; ++l)
             ss[(size_t)mm * (Ls + 1) + l] = h->mg_sigs[(((size_t)g * G + g) * Nm + mm) * (Ls + 1) + l];
-    int rc = lb_set_xs(static_cast<lb_handle*>(h), Ls, st.data(), ss.data());
+    return lb_set_xs(static_cast<lb_handle*>(h), Ls, st.data(), ss.data());
+}
+
+// ... and d_b = D T^{-1} M d_src.
+static int mg_group_setup(Handle* h, int g) {
+    int rc = mg_group_sources(h, g);
     if (rc) return rc;
     return apply_transport_moments(h, nullptr, nullptr, h->d_src, nullptr, h->d_b);
 }
+
+}  // namespace lb
+
+using namespace lb;
 
 extern "C" {
 
@@ -377,6 +376,22 @@ int lb_transport_inv(lb_handle* h, double* s) {
     if ((rc = upload_angular(h, s, h->d_psi))) return rc;
     if ((rc = launch_sweep(h, h->d_psi))) return rc;
     return download_angular(h, h->d_psi, s);
+}
+
+int lb_m2d_device(lb_handle* h, const double* phi, float* psi) {
+    if (!h || !phi || !psi) return LB_ERR_ARG;
+    int rc = need_ready(h);
+    if (rc) return rc;
+    cudaSetDevice(h->device);
+    return launch_m2d(h, phi, h->d_sigl, nullptr, nullptr, psi);
+}
+
+int lb_d2m_device(lb_handle* h, const float* psi, double* phi) {
+    if (!h || !phi || !psi) return LB_ERR_ARG;
+    int rc = need_ready(h);
+    if (rc) return rc;
+    cudaSetDevice(h->device);
+    return launch_d2m(h, psi, nullptr, 0.0, 1.0, phi);
 }
 
 int lb_scatter_apply(lb_handle* h, double* x) {

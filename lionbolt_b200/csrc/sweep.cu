@@ -61,18 +61,18 @@ struct SweepArgs {
     long long spin_limit;
 };
 
-__device__ __forceinline__ int ld_acquire(const int* p) {
-    int v;
-    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
 __device__ __forceinline__ float pick(const float4& v, int idx) {
     float r = v.x;
     r = (idx == 1) ? v.y : r;
     r = (idx == 2) ? v.z : r;
     r = (idx == 3) ? v.w : r;
     return r;
+}
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
 }
 
 // Loads of one element-direction update.  kCG selects L2-only loads (data written by other SMs).
@@ -181,10 +181,10 @@ __device__ __forceinline__ void solve_rank2(Update& u) {
     const float v1 = fmaf(u.b[0], u.r[0], fmaf(u.b[1], u.r[1], fmaf(u.b[2], u.r[2], u.b[3] * u.r[3])));
     const float e00 = u.d + sa, e11 = u.d + sb;
     const float det = fmaf(e00, e11, -4.0f * ba);
-    const float idet = __frcp_rn(det);
+    const float idet = __fdividef(1.0f, det);
     const float z0 = fmaf(e11, v0, -4.0f * v1) * idet;
     const float z1 = fmaf(e00, v1, -ba * v0) * idet;
-    const float id = __frcp_rn(u.d);
+    const float id = __fdividef(1.0f, u.d);
 #pragma unroll
     for (int k = 0; k < 4; ++k) u.r[k] = (u.r[k] - fmaf(u.a[k], z0, z1)) * id;
 }
@@ -304,120 +304,48 @@ __global__ void __launch_bounds__(1024, MINB) sweep_levels_pf_kernel(SweepArgs a
 }
 
 // ---------------------------------------------------------------------------------------------
-// Staged level schedule: the static inputs of level L+1 are brought on chip while level L is
-// computed, so that after each CTA barrier the only global loads left on an update's critical path
-// are the upstream values written by earlier levels.
-//   * items of level L+2 are loaded into registers during level L (KS slots per thread);
-//   * during level L the items of L+1 (from those registers) go to shared memory, their
-//     neighbour words (16 B of the element record) are copied with cp.async, and their sources and
-//     face vectors are prefetched into L2;
-//   * elements beyond the KS * NT staged slots of a level take the direct path.
-// Shared memory: two buffers of KS * NT (item, neighbour word) pairs = 40 * KS * NT bytes.
+// Batched level schedule: one persistent launch over the directions of many independent problems
+// (meshes, quadratures and cross sections differ).  CTAs claim work items in order from a global
+// counter, so items sorted by decreasing cost give a longest-first list schedule; each item is a
+// whole direction walked level by level with a CTA barrier between levels, exactly like the
+// single-problem level kernel (same element update, bit-identical results).
 // ---------------------------------------------------------------------------------------------
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p)); }
-
-template <int NT, int KS>
-__global__ void __launch_bounds__(NT, 1) sweep_staged_kernel(SweepArgs a) {
-    constexpr int CAP = NT * KS;
-    extern __shared__ __align__(16) unsigned char s_stage[];
-    int4* s_nbr = reinterpret_cast<int4*>(s_stage);       // [2][CAP]
-    int* s_item = reinterpret_cast<int*>(s_nbr + 2 * CAP);  // [2][CAP]
+template <int NT>
+__global__ void __launch_bounds__(NT) sweep_batch_kernel(const BatchWork* __restrict__ work, int nwork, int* counter,
+                                                        const int* __restrict__ active) {
     __shared__ float s_sigt[256];
-    load_sigt(a, s_sigt);
-    const int t = threadIdx.x;
-    for (int i = blockIdx.x; i < a.NI; i += gridDim.x) {
-        const int nl = __ldg(&a.nlev[i]);
-        const int lb = __ldg(&a.lvl_base[i]);
-        const float4 dir = __ldg(&a.dirs[i]);
-        const int* it = a.items + (size_t)i * a.NE;
-        float* base = a.psi + (size_t)i * (size_t)a.NENK;
-        int s0 = __ldg(&a.lvl_start[lb]);
-        int s1 = __ldg(&a.lvl_start[lb + 1]);
-        int n0 = s1;
-        int n1 = (nl > 1) ? __ldg(&a.lvl_start[lb + 2]) : s1;
-        int nxt[KS];
-        // stage level 0 into buffer 0 and load the items of level 1
-#pragma unroll
-        for (int k = 0; k < KS; ++k) {
-            const int slot = t + k * NT;
-            if (s0 + slot < s1) {
-                const int itm = __ldcs(&it[s0 + slot]);
-                const int e = itm & 0xFFFFFF;
-                s_item[slot] = itm;
-                cp_async16(&s_nbr[slot], &a.geom[(size_t)e * 4 + 3]);
-            }
+    __shared__ int s_w;
+    for (;;) {
+        if (threadIdx.x == 0) s_w = atomicAdd(counter, 1);
+        __syncthreads();
+        const int w = s_w;
+        if (w >= nwork) return;
+        const BatchWork* W = work + w;
+        const int prob = __ldg(&W->problem);
+        if (active && __ldg(&active[prob]) == 0) {
+            __syncthreads();
+            continue;
         }
-        cp_async_commit();
-#pragma unroll
-        for (int k = 0; k < KS; ++k) {
-            const int slot = t + k * NT;
-            nxt[k] = (n0 + slot < n1) ? __ldcs(&it[n0 + slot]) : 0;
-        }
-        cp_async_wait_all();
+        const int Nm = __ldg(&W->Nm);
+        const float* sg = W->sigt;
+        for (int m = threadIdx.x; m < 256; m += NT) s_sigt[m] = (m < Nm) ? __ldg(&sg[m]) : 0.f;
+        const int nl = __ldg(&W->nlev);
+        const int* ls = W->lvl_start;
+        const int* it = W->items;
+        const float4* geom = W->geom;
+        float* base = W->psi;
+        const float4 dir = __ldg(&W->dir);
         __syncthreads();
         for (int L = 0; L < nl; ++L) {
-            const int b = L & 1;
-            // (1) stage level L+1 into the other buffer
-            int4* nb_dst = s_nbr + (b ^ 1) * CAP;
-            int* it_dst = s_item + (b ^ 1) * CAP;
-#pragma unroll
-            for (int k = 0; k < KS; ++k) {
-                const int slot = t + k * NT;
-                if (n0 + slot < n1) {
-                    const int itm = nxt[k];
-                    const int e = itm & 0xFFFFFF;
-                    it_dst[slot] = itm;
-                    cp_async16(&nb_dst[slot], &a.geom[(size_t)e * 4 + 3]);
-                    prefetch_l2(base + 4 * (size_t)e);
-                    prefetch_l2(&a.geom[(size_t)e * 4]);
-                }
-            }
-            cp_async_commit();
-            // (2) items of level L+2
-            const int m0 = n1;
-            const int m1 = (L + 2 < nl) ? __ldg(&a.lvl_start[lb + L + 3]) : n1;
-#pragma unroll
-            for (int k = 0; k < KS; ++k) {
-                const int slot = t + k * NT;
-                nxt[k] = (m0 + slot < m1) ? __ldcs(&it[m0 + slot]) : 0;
-            }
-            // (3) level L from the staged buffer, then the overflow beyond the staged slots
-            const int4* nb_src = s_nbr + b * CAP;
-            const int* it_src = s_item + b * CAP;
-#pragma unroll
-            for (int k = 0; k < KS; ++k) {
-                const int slot = t + k * NT;
-                if (s0 + slot < s1) {
-                    const int item = it_src[slot];
-                    const int e = item & 0xFFFFFF;
-                    Geom g;
-                    g.gx = __ldg(&a.geom[(size_t)e * 4 + 0]);
-                    g.gy = __ldg(&a.geom[(size_t)e * 4 + 1]);
-                    g.gz = __ldg(&a.geom[(size_t)e * 4 + 2]);
-                    g.gn = nb_src[slot];
-                    Update up;
-                    assemble_g<false>(base, dir, item, g, s_sigt, up, make_float4(0.f, 0.f, 0.f, 0.f));
-                    finish<false>(base, item, up);
-                }
-            }
-            for (int es = s0 + CAP + t; es < s1; es += NT) {
+            const int s0 = __ldg(&ls[L]), s1 = __ldg(&ls[L + 1]);
+            for (int es = s0 + threadIdx.x; es < s1; es += NT) {
                 const int item = __ldcs(&it[es]);
+                const Geom g = load_geom(geom, item & 0xFFFFFF);
                 Update up;
-                assemble<false>(a, base, dir, item, s_sigt, up);
+                assemble_g<false>(base, dir, item, g, s_sigt, up, make_float4(0.f, 0.f, 0.f, 0.f));
                 finish<false>(base, item, up);
             }
-            cp_async_wait_all();
             __syncthreads();
-            s0 = n0;
-            s1 = n1;
-            n0 = m0;
-            n1 = m1;
         }
     }
 }
@@ -675,8 +603,7 @@ __global__ void __launch_bounds__(256) sweep_dataflow_kernel(SweepArgs a) {
 }
 
 struct Config {
-    int kind;      // 0 levels, 1 dataflow, 2 levels with next-level prefetch, 3 element flags, 4 grouped levels,
-                   // 5 staged levels (dpc = staged slots per thread)
+    int kind;      // 0 levels, 1 dataflow, 2 levels with next-level prefetch, 3 element flags, 4 grouped levels
     int threads;
     int dpc;       // directions per CTA (kind 0); minimum CTAs per SM (kind 2)
     int ilp;
@@ -685,7 +612,7 @@ struct Config {
 const Config kConfigs[] = {
     {4, 1024, 2, 1}, {4, 512, 2, 1}, {4, 512, 3, 1}, {4, 1024, 3, 1}, {4, 512, 6, 1},
     {0, 1024, 1, 1}, {0, 512, 1, 1}, {2, 1024, 1, 1}, {3, 512, 0, 1}, {1, 256, 0, 0},
-    {5, 1024, 5, 1}, {5, 512, 8, 1},
+    {4, 768, 2, 1},
 };
 constexpr int kNumConfigs = sizeof(kConfigs) / sizeof(kConfigs[0]);
 
@@ -757,19 +684,6 @@ cudaError_t launch_flags(const SweepArgs& a, int sm_count, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-template <int NT, int KS>
-cudaError_t launch_staged(const SweepArgs& a, int sm_count, cudaStream_t s) {
-    const size_t smem = (size_t)2 * NT * KS * (sizeof(int4) + sizeof(int));
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(sweep_staged_kernel<NT, KS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
-    }
-    int grid = std::min(a.NI, sm_count);
-    sweep_staged_kernel<NT, KS><<<grid, NT, smem, s>>>(a);
-    return cudaGetLastError();
-}
-
 template <int MINB>
 cudaError_t launch_levels_pf(const SweepArgs& a, int threads, int sm_count, cudaStream_t s) {
     int per_sm = 0;
@@ -781,6 +695,28 @@ cudaError_t launch_levels_pf(const SweepArgs& a, int threads, int sm_count, cuda
 }
 
 }  // namespace
+
+int launch_sweep_batch(cudaStream_t st, const BatchWork* work, int nwork, int* counter, const int* active, int threads,
+                       int sm_count) {
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
+    if (e != cudaSuccess) return LB_ERR_CUDA;
+    if (threads == 512) {
+        static int per_sm = -1;
+        if (per_sm < 0) {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_batch_kernel<512>, 512, 0);
+            if (per_sm < 1) per_sm = 1;
+        }
+        sweep_batch_kernel<512><<<std::min(nwork, sm_count * per_sm), 512, 0, st>>>(work, nwork, counter, active);
+    } else {
+        static int per_sm = -1;
+        if (per_sm < 0) {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_batch_kernel<1024>, 1024, 0);
+            if (per_sm < 1) per_sm = 1;
+        }
+        sweep_batch_kernel<1024><<<std::min(nwork, sm_count * per_sm), 1024, 0, st>>>(work, nwork, counter, active);
+    }
+    return cudaGetLastError() == cudaSuccess ? LB_OK : LB_ERR_CUDA;
+}
 
 int launch_sweep(Handle* h, float* psi) {
     SweepArgs a;
@@ -833,8 +769,7 @@ int launch_sweep(Handle* h, float* psi) {
         cudaFuncGetAttributes(&fa, sweep_levels_kernel<2, 1>);
         cudaFuncGetAttributes(&fa, sweep_levels_kernel<2, 2>);
         cudaFuncGetAttributes(&fa, sweep_dataflow_kernel);
-        cudaFuncGetAttributes(&fa, sweep_staged_kernel<1024, 5>);
-        cudaFuncGetAttributes(&fa, sweep_staged_kernel<512, 8>);
+        cudaFuncGetAttributes(&fa, sweep_group_kernel<2, 768>);
     }
     Config cfg = kConfigs[cfg_idx];
     // the element-flag schedule keeps one bit per element in shared memory
@@ -855,12 +790,10 @@ int launch_sweep(Handle* h, float* psi) {
     }
     Timer t;
     timer_begin(h, LB_T_SWEEP, t);
-    if (cfg.kind == 5) {
-        e = cfg.threads == 1024 ? launch_staged<1024, 5>(a, h->sm_count, h->stream)
-                                : launch_staged<512, 8>(a, h->sm_count, h->stream);
-    } else if (cfg.kind == 4) {
+    if (cfg.kind == 4) {
         if (cfg.dpc == 2) e = cfg.threads == 1024 ? launch_group<2, 1024>(a, h->d_groups, h->ngroups, h->sm_count, h->stream)
-                                                  : launch_group<2, 512>(a, h->d_groups, h->ngroups, h->sm_count, h->stream);
+                            : cfg.threads == 768 ? launch_group<2, 768>(a, h->d_groups, h->ngroups, h->sm_count, h->stream)
+                                                 : launch_group<2, 512>(a, h->d_groups, h->ngroups, h->sm_count, h->stream);
         else if (cfg.dpc == 3) e = cfg.threads == 1024 ? launch_group<3, 1024>(a, h->d_groups, h->ngroups, h->sm_count, h->stream)
                                                        : launch_group<3, 512>(a, h->d_groups, h->ngroups, h->sm_count, h->stream);
         else e = launch_group<6, 512>(a, h->d_groups, h->ngroups, h->sm_count, h->stream);

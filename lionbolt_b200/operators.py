@@ -9,6 +9,8 @@ Vectors are FP64 numpy arrays in the reference layout v[i*NENK + 4e + k]; operat
 place ("enters as source, leaves as solution", TransportAlgebra.f90:44).  Every call goes through
 the C ABI to the CUDA library; errors raise LionboltError (the reference calls stophere).
 """
+import ctypes
+
 import numpy as np
 
 from . import _lib
@@ -268,3 +270,69 @@ class MultigroupSolver(_Op):
         dose = np.zeros(NENK)
         self._h.call("lb_mg_get_results", dptr(flux), dptr(dose))
         return flux, dose
+
+
+class BatchSolver:
+    """Many independent multigroup dose problems solved together on one GPU (lb_batch_* C ABI):
+    one persistent sweep launch over every (problem, direction) pair, lock-step GMRES with a
+    device-side activity mask, and the Arnoldi matrix-vector product replayed from a CUDA graph."""
+
+    def __init__(self, device=0):
+        self.lib = _lib.load()
+        b = _lib._vp()
+        st = self.lib.lb_batch_create(int(device), ctypes.byref(b))
+        if st != _lib.LB_OK:
+            raise _lib.LionboltError(st, "lb_batch_create failed: " + self.lib.lb_status_string(st).decode())
+        self.b = b
+        self.problems = []
+
+    def _check(self, st):
+        if st != _lib.LB_OK:
+            buf = ctypes.create_string_buffer(512)
+            self.lib.lb_batch_last_error(self.b, buf, 512)
+            raise _lib.LionboltError(st, buf.value.decode() or self.lib.lb_status_string(st).decode())
+
+    def add_problem(self, prob):
+        m = prob.mesh
+        pid = ctypes.c_int(-1)
+        self._check(self.lib.lb_batch_add_problem(
+            self.b, m.NE, m.NN, dptr(as_f64(m.rg)), iptr(as_i32(m.node)), iptr(as_i32(m.neighbors)),
+            iptr(as_i32(m.mat)), int(m.Nm), int(prob.k.shape[0]), dptr(as_f64(prob.k)), dptr(as_f64(prob.w)),
+            int(prob.G), int(prob.Ls), dptr(as_f64(prob.sigt)), dptr(as_f64(prob.sigs)), dptr(as_f64(prob.dd)),
+            dptr(as_f64(prob.unc)), dptr(as_f64(prob.beam_dir)), ctypes.byref(pid)))
+        self.problems.append(prob)
+        return pid.value
+
+    def solve(self, m=20, rtol=1e-6, atol=0.0, maxit=0):
+        """Operator applications per problem and group, [P, Gmax] (0 where a problem has no group)."""
+        Gmax = max(p.G for p in self.problems)
+        it = np.zeros((len(self.problems), Gmax), dtype=np.int32)
+        self._check(self.lib.lb_batch_solve(self.b, int(m), float(rtol), float(atol), int(maxit), iptr(it)))
+        return it
+
+    def results(self, pid):
+        prob = self.problems[pid]
+        flux = np.zeros((prob.G, prob.mesh.NENK))
+        dose = np.zeros(prob.mesh.NENK)
+        self._check(self.lib.lb_batch_get_results(self.b, int(pid), dptr(flux), dptr(dose)))
+        return flux, dose
+
+    def info(self):
+        n, g, th = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        ms = ctypes.c_double()
+        gl, sl = ctypes.c_longlong(), ctypes.c_longlong()
+        self._check(self.lib.lb_batch_info(self.b, ctypes.byref(n), ctypes.byref(g), ctypes.byref(ms), ctypes.byref(th),
+                                           ctypes.byref(gl), ctypes.byref(sl)))
+        return dict(problems=n.value, max_groups=g.value, last_ms=ms.value, sweep_threads=th.value,
+                    graph_launches=gl.value, sweep_launches=sl.value)
+
+    def close(self):
+        if self.b:
+            self.lib.lb_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

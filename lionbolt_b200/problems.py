@@ -146,3 +146,40 @@ def config1():
 def config1_small(n=(8, 8, 16), G=4, Ng=6, Nc=12):
     """config1 physics on a coarse mesh with fewer groups and directions (oracle-sized)."""
     return multigroup_box(n=n, G=G, Ng=Ng, Nc=Nc, name=f"config1_small{n}")
+
+
+SN_ORDERS = {8: (8, 10), 12: (12, 14), 16: (16, 18)}   # S_N -> (polar Ng, azimuthal Nc): N(N+2) directions
+
+
+def batch_problem(rng, idx, hmin=8, hmax=32, cell=0.5, groups=(1, 10), orders=(8, 12, 16), Ls=3):
+    """One problem of a batched workload: hexes per axis ~ U{hmin..hmax} (x6 tets), S_N mixed,
+    1-10 groups, P3, cross sections drawn like config1 (log-uniform water + a slab x2.7), beam
+    direction uniform on the upper hemisphere and width U[1, 8] cm."""
+    n = tuple(int(v) for v in rng.integers(hmin, hmax + 1, size=3))
+    size = tuple(cell * v for v in n)
+    G = int(rng.integers(groups[0], groups[1] + 1))
+    N = int(rng.choice(orders))
+    Ng, Nc = SN_ORDERS[N]
+    depth = size[2]
+    z0 = float(rng.uniform(0.15, 0.6)) * depth
+    slab = (z0, min(depth, z0 + 0.1 * depth))
+    u = rng.uniform(0.0, 1.0)                      # uniform on the upper hemisphere: cos(theta) ~ U[0, 1]
+    ct = max(u, 0.05)
+    ph = rng.uniform(0.0, 2 * np.pi)
+    st = np.sqrt(1 - ct * ct)
+    width = float(rng.uniform(1.0, 8.0))
+    seed = int(rng.integers(0, 2 ** 31 - 1))
+    prob = multigroup_box(n=n, size=size, Ng=Ng, Nc=Nc, G=G, Ls=Ls, seed=seed, slab=slab,
+                          beam_deg=0.0, name=f"batch{idx}")
+    bdir = np.array([st * np.cos(ph), st * np.sin(ph), ct])
+    layers = [(0.0, slab[0], prob.sigt[0, 0]), (slab[0], slab[1], prob.sigt[0, 1]), (slab[1], depth, prob.sigt[0, 0])]
+    beam = (min(width, size[0]), min(width, size[1]))
+    prob.beam_dir = bdir
+    prob.unc = beam_uncollided(prob.mesh, bdir, (0.5 * size[0], 0.5 * size[1]), beam, layers)
+    return prob
+
+
+def batch_problems(count=64, seed=20261203, **kw):
+    """config3: `count` independent problems with seeded uneven sizes (8^3 to 32^3 hexes)."""
+    rng = np.random.default_rng(seed)
+    return [batch_problem(rng, i, **kw) for i in range(count)]

@@ -58,10 +58,10 @@ def test_transport_inverse_matches_oracle(case):
     assert T.timers()["sweep"][1] >= 1
 
 
-@pytest.mark.parametrize("cfg", range(10))
+@pytest.mark.parametrize("cfg", range(11))
 def test_every_sweep_schedule_matches_oracle(cfg, monkeypatch):
     """Each launch candidate of the sweep autotuner (levels, prefetching levels, element flags,
-    dataflow) reproduces the oracle's T^{-1} on a two-material mesh."""
+    grouped directions, dataflow) reproduces the oracle's T^{-1} on a two-material mesh."""
     monkeypatch.setenv("LB_SWEEP_CONFIG", str(cfg))
     m, (k, w), sigt, sigs = SWEEP_CASES["two_material"]()
     o, ang, xs = _pair(m, k, w, sigt, sigs)
