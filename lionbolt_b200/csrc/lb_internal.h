@@ -266,6 +266,14 @@ int launch_m2d(Handle* h, const double* x, const float* sigl, const double* a, c
 // (xin may be null: out = beta * z).
 int launch_d2m(Handle* h, const float* psi, const double* xin, double alpha, double beta, double* out);
 
+// tcgen05 versions of the two contractions (moments_tc.cu); LB_ERR_ARG when a shape does not fit them.
+// LB_MOMENTS_TC=0 selects the mma.sync kernels.
+bool moments_tc_enabled();
+int launch_m2d_tc(Handle* h, const double* x, const float* sigl, const double* a, const float* qadd, float* q);
+int launch_d2m_tc(Handle* h, const float* psi, const double* xin, double alpha, double beta, double* out);
+// Reads and clears the tensor-core kernels' bounded-wait timeout flag.
+int moments_tc_status(Handle* h);
+
 // FP64 BLAS-1 on device vectors of length n
 int k_dots(Handle* h, const double* V, size_t ldv, int nv, const double* w, size_t n, double* out_host);
 // out[j] = V_j . w (j < nv, nv may be 0) and *wnorm2 = w . w in one pass (outputs may be null)

@@ -11,6 +11,7 @@
 // whose magnitude exceeds 2^-24 of the leading term are accumulated (hi.hi, hi.mid, mid.hi,
 // hi.lo, mid.mid, lo.hi), which reproduces an FP32 GEMM on the BF16 tensor pipe.
 #include "lb_internal.h"
+#include <cstdlib>
 
 namespace lb {
 
@@ -28,7 +29,7 @@ __device__ __forceinline__ void split3(float v, __nv_bfloat16& a, __nv_bfloat16&
 }
 
 __device__ __forceinline__ void mma16816(float* d, const uint32_t* a, const uint32_t* b) {
-    asm volatile(
+    asm(
         "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
         "{%0,%1,%2,%3};\n"
         : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
@@ -256,9 +257,10 @@ __device__ __forceinline__ void stage_planes(const __nv_bfloat16* __restrict__ g
 }
 
 // M2D: q[i][n] = sum_j Y[i][j] xt[j][n] (+ qadd),  xt = sigl[mat(n)][j] x[j][n] + a[j][n].
-// Warp w owns nodes n0 + 8w .. +7 of the 64-node tile; its B fragments for all K stay in registers.
-template <int KT>
-__global__ void __launch_bounds__(kThreads) m2d_stream_kernel(const int* __restrict__ active, const double* __restrict__ x, const float* __restrict__ sigl,
+// NW warps per CTA; warp w owns nodes n0 + 8w .. +7 of the 8*NW-node tile; its B fragments for all
+// K stay in registers.  Direction tiles are processed in pairs: two independent accumulator chains.
+template <int KT, int NW>
+__global__ void __launch_bounds__(NW * 32, 1) m2d_stream_kernel(const int* __restrict__ active, const double* __restrict__ x, const float* __restrict__ sigl,
                                                              const double* __restrict__ add, const float* __restrict__ qadd,
                                                              const int* __restrict__ mat, const __nv_bfloat16* __restrict__ Y,
                                                              float* __restrict__ q, long long NENK, int NI, int NIpad,
@@ -266,13 +268,14 @@ __global__ void __launch_bounds__(kThreads) m2d_stream_kernel(const int* __restr
     if (active && *active == 0) return;   // problem of a batch that has converged
     extern __shared__ __align__(16) __nv_bfloat16 ys[];     // [3][NIpad][nmpad + 8]
     stage_planes(Y, ys, NIpad, nmpad);
+    constexpr int TN = NW * 8;
     const int rs = nmpad + 8;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
     const int mi = lane >> 3, rr = lane & 7;                // ldmatrix: matrix index, row in matrix
     const int arow = rr + 8 * (mi & 1), acol = 8 * (mi >> 1);
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const long long n = tile * kTileN + warp * 8 + g;   // node of this thread's B column
+        const long long n = tile * TN + warp * 8 + g;       // node of this thread's B column
         const bool nok = n < NENK;
         const int m = nok ? __ldg(&mat[n >> 2]) : 0;
         uint32_t bf[KT][3][2];
@@ -292,8 +295,39 @@ __global__ void __launch_bounds__(kThreads) m2d_stream_kernel(const int* __restr
             split_pair(v[0], v[1], bf[kt][0][0], bf[kt][1][0], bf[kt][2][0]);
             split_pair(v[2], v[3], bf[kt][0][1], bf[kt][1][1], bf[kt][2][1]);
         }
-        const long long nc = tile * kTileN + warp * 8 + 2 * t;   // output column pair of this thread
-        for (int m0 = 0; m0 < NIpad; m0 += 16) {
+        const long long nc = tile * TN + warp * 8 + 2 * t;   // output column pair of this thread
+        auto store = [&](int m0, const float* acc) {
+            if (nc >= NENK) return;
+            const int r0 = m0 + g, r1 = m0 + g + 8;
+            if (r0 < NI) {
+                float2 v = make_float2(acc[0], acc[1]);
+                if (qadd) { float2 u = *reinterpret_cast<const float2*>(&qadd[(size_t)r0 * NENK + nc]); v.x += u.x; v.y += u.y; }
+                __stcs(reinterpret_cast<float2*>(&q[(size_t)r0 * NENK + nc]), v);
+            }
+            if (r1 < NI) {
+                float2 v = make_float2(acc[2], acc[3]);
+                if (qadd) { float2 u = *reinterpret_cast<const float2*>(&qadd[(size_t)r1 * NENK + nc]); v.x += u.x; v.y += u.y; }
+                __stcs(reinterpret_cast<float2*>(&q[(size_t)r1 * NENK + nc]), v);
+            }
+        };
+        int m0 = 0;
+        for (; m0 + 16 < NIpad; m0 += 32) {
+            float acc0[4] = {0.f, 0.f, 0.f, 0.f}, acc1[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int kt = 0; kt < KT; ++kt) {
+                uint32_t a0[3][4], a1[3][4];
+#pragma unroll
+                for (int p = 0; p < 3; ++p) {
+                    ldsm_x4(a0[p], ys + ((size_t)p * NIpad + m0 + arow) * rs + kt * 16 + acol);
+                    ldsm_x4(a1[p], ys + ((size_t)p * NIpad + m0 + 16 + arow) * rs + kt * 16 + acol);
+                }
+                mma_split6(acc0, a0, bf[kt]);
+                mma_split6(acc1, a1, bf[kt]);
+            }
+            store(m0, acc0);
+            store(m0 + 16, acc1);
+        }
+        if (m0 < NIpad) {
             float acc[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
             for (int kt = 0; kt < KT; ++kt) {
@@ -303,27 +337,16 @@ __global__ void __launch_bounds__(kThreads) m2d_stream_kernel(const int* __restr
                     ldsm_x4(af[p], ys + ((size_t)p * NIpad + m0 + arow) * rs + kt * 16 + acol);
                 mma_split6(acc, af, bf[kt]);
             }
-            if (nc < NENK) {
-                const int r0 = m0 + g, r1 = m0 + g + 8;
-                if (r0 < NI) {
-                    float2 v = make_float2(acc[0], acc[1]);
-                    if (qadd) { float2 u = *reinterpret_cast<const float2*>(&qadd[(size_t)r0 * NENK + nc]); v.x += u.x; v.y += u.y; }
-                    __stcs(reinterpret_cast<float2*>(&q[(size_t)r0 * NENK + nc]), v);
-                }
-                if (r1 < NI) {
-                    float2 v = make_float2(acc[2], acc[3]);
-                    if (qadd) { float2 u = *reinterpret_cast<const float2*>(&qadd[(size_t)r1 * NENK + nc]); v.x += u.x; v.y += u.y; }
-                    __stcs(reinterpret_cast<float2*>(&q[(size_t)r1 * NENK + nc]), v);
-                }
-            }
+            store(m0, acc);
         }
     }
 }
 
 // D2M: z[j][n] = sum_i Dw[j][i] psi[i][n];  out = alpha * xin + beta * z.
-// Warp w owns nodes n0 + 8w .. +7; psi fragments stream from HBM one k-step ahead of the MMAs.
-template <int MT>
-__global__ void __launch_bounds__(kThreads) d2m_stream_kernel(const int* __restrict__ active, const float* __restrict__ psi, const __nv_bfloat16* __restrict__ Dw,
+// NW warps per CTA; warp w owns nodes n0 + 8w .. +7; psi fragments stream from HBM one k-step ahead
+// of the MMAs.
+template <int MT, int NW>
+__global__ void __launch_bounds__(NW * 32, 1) d2m_stream_kernel(const int* __restrict__ active, const float* __restrict__ psi, const __nv_bfloat16* __restrict__ Dw,
                                                              const double* xin, double alpha, double beta, double* out,
                                                              long long NENK, int NI, int NIpad, int nm, int nmpad,
                                                              long long ntiles) {
@@ -337,7 +360,7 @@ __global__ void __launch_bounds__(kThreads) d2m_stream_kernel(const int* __restr
     const int arow = rr + 8 * (mi & 1), acol = 8 * (mi >> 1);
     const int mtiles = nmpad / 16;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const long long n = tile * kTileN + warp * 8 + g;
+        const long long n = tile * (NW * 8) + warp * 8 + g;
         const bool nok = n < NENK;
         float acc[MT][4];
 #pragma unroll
@@ -368,7 +391,7 @@ __global__ void __launch_bounds__(kThreads) d2m_stream_kernel(const int* __restr
 #pragma unroll
             for (int h = 0; h < 4; ++h) cur[h] = nxt[h];
         }
-        const long long nc = tile * kTileN + warp * 8 + 2 * t;
+        const long long nc = tile * (NW * 8) + warp * 8 + 2 * t;
         if (nc < NENK) {
 #pragma unroll
             for (int mt = 0; mt < MT; ++mt) {
@@ -403,34 +426,47 @@ int run_d2m(Handle* h, const float* psi, const double* xin, double alpha, double
 }
 
 
-template <int KT>
+template <int KT, int NW>
 cudaError_t run_m2d_stream(Handle* h, const double* x, const float* sigl, const double* a, const float* qadd, float* q,
-                           long long ntiles, size_t smem) {
+                           size_t smem) {
     static int per_sm = -1;
     if (per_sm < 0) {
-        allow_max_dynamic_smem(m2d_stream_kernel<KT>);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, m2d_stream_kernel<KT>, kThreads, smem);
+        allow_max_dynamic_smem(m2d_stream_kernel<KT, NW>);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, m2d_stream_kernel<KT, NW>, NW * 32, smem);
         if (per_sm < 1) per_sm = 1;
     }
+    const long long ntiles = (h->NENK + NW * 8 - 1) / (NW * 8);
     long long grid = std::min<long long>(ntiles, (long long)h->sm_count * per_sm);
-    m2d_stream_kernel<KT><<<(int)grid, kThreads, smem, h->stream>>>(h->d_active, x, sigl, a, qadd, h->d_mat, h->d_Ym2d, q, h->NENK,
-                                                                    h->NI, h->NIpad, h->nm, h->nmpad, ntiles);
+    m2d_stream_kernel<KT, NW><<<(int)grid, NW * 32, smem, h->stream>>>(h->d_active, x, sigl, a, qadd, h->d_mat, h->d_Ym2d, q,
+                                                                        h->NENK, h->NI, h->NIpad, h->nm, h->nmpad, ntiles);
     return cudaGetLastError();
 }
 
-template <int MT>
+template <int MT, int NW>
 cudaError_t run_d2m_stream(Handle* h, const float* psi, const double* xin, double alpha, double beta, double* out,
-                           long long ntiles, size_t smem) {
+                           size_t smem) {
     static int per_sm = -1;
     if (per_sm < 0) {
-        allow_max_dynamic_smem(d2m_stream_kernel<MT>);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, d2m_stream_kernel<MT>, kThreads, smem);
+        allow_max_dynamic_smem(d2m_stream_kernel<MT, NW>);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, d2m_stream_kernel<MT, NW>, NW * 32, smem);
         if (per_sm < 1) per_sm = 1;
     }
+    const long long ntiles = (h->NENK + NW * 8 - 1) / (NW * 8);
     long long grid = std::min<long long>(ntiles, (long long)h->sm_count * per_sm);
-    d2m_stream_kernel<MT><<<(int)grid, kThreads, smem, h->stream>>>(h->d_active, psi, h->d_Yd2m, xin, alpha, beta, out, h->NENK,
-                                                                    h->NI, h->NIpad, h->nm, h->nmpad, ntiles);
+    d2m_stream_kernel<MT, NW><<<(int)grid, NW * 32, smem, h->stream>>>(h->d_active, psi, h->d_Yd2m, xin, alpha, beta, out,
+                                                                        h->NENK, h->NI, h->NIpad, h->nm, h->nmpad, ntiles);
     return cudaGetLastError();
+}
+
+// Warps per CTA of the streaming contractions: 32 (one CTA and one copy of the constant operand per
+// SM) unless LB_MOMENTS_WARPS=8 asks for four 256-thread CTAs.
+int moments_warps() {
+    static int nw = -1;
+    if (nw < 0) {
+        const char* e = std::getenv("LB_MOMENTS_WARPS");
+        nw = (e && std::atoi(e) == 8) ? 8 : 32;
+    }
+    return nw;
 }
 
 constexpr size_t kStreamSmemLimit = 200 * 1024;
@@ -439,6 +475,13 @@ constexpr size_t kStreamSmemLimit = 200 * 1024;
 
 int launch_m2d(Handle* h, const double* x, const float* sigl, const double* a, const float* qadd, float* q) {
     if (!sigl) sigl = h->d_sigl;
+    if (moments_tc_enabled()) {
+        Timer tt;
+        timer_begin(h, LB_T_M2D, tt);
+        const int rc = launch_m2d_tc(h, x, sigl, a, qadd, q);
+        timer_end(h, tt);
+        if (rc != LB_ERR_ARG) return rc;
+    }
     const long long ntiles = (h->NENK + kTileN - 1) / kTileN;
     const int KT = h->nmpad / 16;
     const size_t smem_stream = (size_t)3 * h->NIpad * (h->nmpad + 8) * 2;
@@ -446,16 +489,20 @@ int launch_m2d(Handle* h, const double* x, const float* sigl, const double* a, c
     timer_begin(h, LB_T_M2D, t);
     cudaError_t e = cudaSuccess;
     if (KT <= 8 && smem_stream <= kStreamSmemLimit) {
+        const bool w32 = moments_warps() == 32;
+#define LB_M2D(K) e = w32 ? run_m2d_stream<K, 32>(h, x, sigl, a, qadd, q, smem_stream) \
+                          : run_m2d_stream<K, 8>(h, x, sigl, a, qadd, q, smem_stream)
         switch (KT) {
-            case 1: e = run_m2d_stream<1>(h, x, sigl, a, qadd, q, ntiles, smem_stream); break;
-            case 2: e = run_m2d_stream<2>(h, x, sigl, a, qadd, q, ntiles, smem_stream); break;
-            case 3: e = run_m2d_stream<3>(h, x, sigl, a, qadd, q, ntiles, smem_stream); break;
-            case 4: e = run_m2d_stream<4>(h, x, sigl, a, qadd, q, ntiles, smem_stream); break;
-            case 5: e = run_m2d_stream<5>(h, x, sigl, a, qadd, q, ntiles, smem_stream); break;
-            case 6: e = run_m2d_stream<6>(h, x, sigl, a, qadd, q, ntiles, smem_stream); break;
-            case 7: e = run_m2d_stream<7>(h, x, sigl, a, qadd, q, ntiles, smem_stream); break;
-            default: e = run_m2d_stream<8>(h, x, sigl, a, qadd, q, ntiles, smem_stream); break;
+            case 1: LB_M2D(1); break;
+            case 2: LB_M2D(2); break;
+            case 3: LB_M2D(3); break;
+            case 4: LB_M2D(4); break;
+            case 5: LB_M2D(5); break;
+            case 6: LB_M2D(6); break;
+            case 7: LB_M2D(7); break;
+            default: LB_M2D(8); break;
         }
+#undef LB_M2D
     } else {
         static bool attr = false;
         if (!attr) {
@@ -478,6 +525,13 @@ int launch_m2d(Handle* h, const double* x, const float* sigl, const double* a, c
 }
 
 int launch_d2m(Handle* h, const float* psi, const double* xin, double alpha, double beta, double* out) {
+    if (moments_tc_enabled()) {
+        Timer tt;
+        timer_begin(h, LB_T_D2M, tt);
+        const int rc = launch_d2m_tc(h, psi, xin, alpha, beta, out);
+        timer_end(h, tt);
+        if (rc != LB_ERR_ARG) return rc;
+    }
     const long long ntiles = (h->NENK + kTileN - 1) / kTileN;
     const int mtiles = h->nmpad / 16;
     const size_t smem_stream = (size_t)3 * h->nmpad * (h->NIpad + 8) * 2;
@@ -486,10 +540,14 @@ int launch_d2m(Handle* h, const float* psi, const double* xin, double alpha, dou
     cudaError_t e = cudaSuccess;
     int rc = LB_OK;
     if (smem_stream <= kStreamSmemLimit) {
-        if (mtiles <= 1) e = run_d2m_stream<1>(h, psi, xin, alpha, beta, out, ntiles, smem_stream);
-        else if (mtiles <= 3) e = run_d2m_stream<3>(h, psi, xin, alpha, beta, out, ntiles, smem_stream);
-        else if (mtiles <= 7) e = run_d2m_stream<7>(h, psi, xin, alpha, beta, out, ntiles, smem_stream);
-        else e = run_d2m_stream<16>(h, psi, xin, alpha, beta, out, ntiles, smem_stream);
+        const bool w32 = moments_warps() == 32;
+#define LB_D2M(M) e = w32 ? run_d2m_stream<M, 32>(h, psi, xin, alpha, beta, out, smem_stream) \
+                          : run_d2m_stream<M, 8>(h, psi, xin, alpha, beta, out, smem_stream)
+        if (mtiles <= 1) LB_D2M(1);
+        else if (mtiles <= 3) LB_D2M(3);
+        else if (mtiles <= 7) LB_D2M(7);
+        else LB_D2M(16);
+#undef LB_D2M
     } else {
         const size_t smem = (size_t)3 * kTileN * smem_stride_words(h->NIpad) * 4;
         if (smem > 227 * 1024) { timer_end(h, t); return fail(h, LB_ERR_ARG, "d2m: too many directions for the shared-memory tile"); }
