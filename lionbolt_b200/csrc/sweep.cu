@@ -100,12 +100,24 @@ struct Geom {
     int4 gn;
 };
 
+// The 64-byte element record is read with two 256-bit loads (32-byte aligned): half the load
+// instructions and L1 sector accesses of four 128-bit loads.
+__device__ __forceinline__ void ld_nc_v8(const float* p, float (&r)[8]) {
+    asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=f"(r[0]), "=f"(r[1]), "=f"(r[2]), "=f"(r[3]), "=f"(r[4]), "=f"(r[5]), "=f"(r[6]), "=f"(r[7])
+        : "l"(p));
+}
+
 __device__ __forceinline__ Geom load_geom(const float4* __restrict__ geom, int e) {
+    const float* p = reinterpret_cast<const float*>(geom + (size_t)e * 4);
+    float a[8], b[8];
+    ld_nc_v8(p, a);
+    ld_nc_v8(p + 8, b);
     Geom g;
-    g.gx = __ldg(&geom[(size_t)e * 4 + 0]);
-    g.gy = __ldg(&geom[(size_t)e * 4 + 1]);
-    g.gz = __ldg(&geom[(size_t)e * 4 + 2]);
-    g.gn = __ldg(reinterpret_cast<const int4*>(&geom[(size_t)e * 4 + 3]));
+    g.gx = make_float4(a[0], a[1], a[2], a[3]);
+    g.gy = make_float4(a[4], a[5], a[6], a[7]);
+    g.gz = make_float4(b[0], b[1], b[2], b[3]);
+    g.gn = make_int4(__float_as_int(b[4]), __float_as_int(b[5]), __float_as_int(b[6]), __float_as_int(b[7]));
     return g;
 }
 
