@@ -14,8 +14,10 @@
 // the rows are contiguous 16-byte lines (8 rows = one 128-byte core matrix, SBO = 128 B) and
 // consecutive K chunks are LBO bytes apart.  A (data) is produced by the CTA's threads (FP64 / FP32
 // loads, scale, BF16 split, st.shared) and handed to the tensor core with fence.proxy.async; B (the
-// constant Y planes) is staged once per CTA.  One thread issues the MMAs and commits them to an
-// mbarrier; every wait is bounded and sets an error flag instead of hanging.
+// constant Y planes) is staged once per CTA.  Each kernel is warp-specialised (producer warps, an MMA
+// warp whose lane 0 issues every tcgen05.mma, epilogue warps) with double-buffered operands and
+// accumulators synchronised by mbarriers; every wait is bounded and sets an error flag instead of
+// hanging.
 #include "lb_internal.h"
 #include <algorithm>
 #include <cstdlib>
@@ -96,16 +98,6 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
 }
 
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
-    uint32_t r[8];
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-                 : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = __uint_as_float(r[k]);
-}
-
 // The warp calling this allocates ncols TMEM columns (power of two >= 32) and publishes the base.
 __device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)), "r"(ncols)
@@ -158,107 +150,125 @@ __device__ void stage_kmajor(const __nv_bfloat16* __restrict__ g, int rows, int 
     }
 }
 
+__device__ __forceinline__ void bar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 // ---------------------------------------------------------------------------------------------
 // M2D: q[i][n] = sum_j Y[i][j] xt[j][n] (+ qadd[i][n]),  xt[j][n] = sigl[mat(n)][j] x[j][n] + a[j][n].
-// CTA = 128 threads (thread t owns node tile*128 + t), directions [half*NH, half*NH + NH).
+// One CTA per SM, warp-specialised, directions [half*NH, half*NH + NH) of every tile it takes:
+//   warps 0-7   producers: threads t and t + 128 read node tile*128 + (t & 127), half of its moments
+//               each, split them into BF16 planes and write the A buffer (two buffers);
+//   warps 8-15  epilogue: warps 8+e and 12+e read TMEM lanes 32e.. (the tile's nodes), half of the
+//               direction columns each, and write q rows (two accumulators);
+//   warp 16     lane 0 issues the MMAs; the warp owns the TMEM allocation.
+// Barriers per buffer b: full[b] (producers -> MMA), done[b] (MMA commit -> producers, epilogue),
+// empty[b] (epilogue -> MMA).  The k-th use of a buffer waits on phase parity k & 1.
 // ---------------------------------------------------------------------------------------------
 template <int KT>
-__global__ void __launch_bounds__(128, 2) m2d_tc_kernel(const int* __restrict__ active, const double* __restrict__ x,
+__global__ void __launch_bounds__(544, 1) m2d_tc_kernel(const int* __restrict__ active, const double* __restrict__ x,
                                                       const float* __restrict__ sigl, const double* __restrict__ add,
                                                       const float* __restrict__ qadd, const int* __restrict__ mat,
                                                       const __nv_bfloat16* __restrict__ Y, float* __restrict__ q,
                                                       long long NENK, int NI, int NIpad, int nm, int nmpad, int NH,
-                                                      int nhalves, uint32_t tmem_cols, long long ntiles, int* err) {
+                                                      int nhalves, long long ntiles, int* err) {
     if (active && *active == 0) return;
     extern __shared__ __align__(1024) unsigned char sm[];
+    constexpr int NMP = KT * 16;
     const int tid = threadIdx.x, warp = tid >> 5;
-    const size_t bplane = (size_t)NH * nmpad * 2;     // bytes per B plane
-    const size_t aplane = (size_t)kTM * nmpad * 2;    // bytes per A plane
+    const size_t bplane = (size_t)NH * nmpad * 2;
+    const size_t aplane = (size_t)kTM * nmpad * 2;
+    const size_t abuf = ((3 * aplane + 1023) / 1024) * 1024;
     unsigned char* sB = sm;
-    unsigned char* sA = sm + ((3 * bplane + 1023) / 1024) * 1024;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sA + 3 * aplane);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+    unsigned char* sA = sm + ((3 * bplane + 1023) / 1024) * 1024;   // [2] buffers of 3 planes
+    uint64_t* full = reinterpret_cast<uint64_t*>(sA + 2 * abuf);
+    uint64_t* done = full + 2;
+    uint64_t* empty = full + 4;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(full + 6);
     const int half = blockIdx.x % nhalves;
     stage_kmajor(Y, NIpad, nmpad, half * NH, NH, sB, bplane);
-    if (tid == 0) bar_init(bar, 1);
-    if (warp == 0) tmem_alloc(tslot, tmem_cols);
+    if (tid == 0)
+        for (int k = 0; k < 2; ++k) {
+            bar_init(&full[k], 256);
+            bar_init(&done[k], 1);
+            bar_init(&empty[k], 256);
+        }
+    if (warp == 16) tmem_alloc(tslot, 512);
     fence_async_smem();
     tc_before_sync();
     __syncthreads();
     tc_after_sync();
     const uint32_t tmem = *tslot;
-    const uint32_t idesc = idesc_bf16(kTM, NH);
-    const uint32_t lboA = kTM * 16, lboB = (uint32_t)NH * 16;
-    const uint32_t aBase = smem_u32(sA), bBase = smem_u32(sB);
-    constexpr int NMP = KT * 16;
-    uint32_t phase = 0;
-    bool ok = true;
-    const long long tstep = gridDim.x / nhalves;
-    // raw inputs of the current tile, loaded one tile ahead: x (or the additive source) per moment
-    double cur[NMP];
-    auto fetch = [&](long long tl, double (&r)[NMP]) {
-        const long long nn = tl * kTM + tid;
+    const long long t0 = blockIdx.x / nhalves, tstep = gridDim.x / nhalves;
+    if (warp < 8) {
+        // ---- producers: threads t and t + 128 share node tile*128 + (t & 127), each half the moments ----
+        constexpr int HM = NMP / 2;
+        const int r = tid & 127, side = tid >> 7;
         const double* src = x ? x : add;
+        int it = 0;
+        for (long long tile = t0; tile < ntiles; tile += tstep, ++it) {
+            const int b = it & 1;
+            const uint32_t u = (uint32_t)(it >> 1);
+            const long long n = tile * kTM + r;
+            const bool valid = n < NENK;
+            double raw[HM];
 #pragma unroll
-        for (int j = 0; j < NMP; ++j) r[j] = (tl < ntiles && nn < NENK && j < nm) ? __ldcs(&src[(size_t)j * NENK + nn]) : 0.0;
-    };
-    fetch(blockIdx.x / nhalves, cur);
-    for (long long tile = blockIdx.x / nhalves; tile < ntiles && ok; tile += tstep) {
-        const long long n = tile * kTM + tid;
-        const bool valid = n < NENK;
-        const int m = valid ? __ldg(&mat[n >> 2]) : 0;
-        // A: xt rows of this tile, split into BF16 planes
-#pragma unroll
-        for (int c = 0; c < NMP / 8; ++c) {
-            float v[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const int j = c * 8 + k;
-                double s = 0.0;
-                if (valid && j < nm) {
-                    if (x) {
-                        s = (double)__ldg(&sigl[(size_t)m * nmpad + j]) * cur[j];
-                        if (add) s += __ldcs(&add[(size_t)j * NENK + n]);
-                    } else {
-                        s = cur[j];
-                    }
-                }
-                v[k] = (float)s;
+            for (int k = 0; k < HM; ++k) {
+                const int j = side * HM + k;
+                raw[k] = (valid && j < nm) ? __ldcs(&src[(size_t)j * NENK + n]) : 0.0;
             }
-            uint4 hi, mid, lo;
-            split8(v, hi, mid, lo);
-            unsigned char* row = sA + (size_t)c * kTM * 16 + (size_t)tid * 16;
-            *reinterpret_cast<uint4*>(row) = hi;
-            *reinterpret_cast<uint4*>(row + aplane) = mid;
-            *reinterpret_cast<uint4*>(row + 2 * aplane) = lo;
-        }
-        // next tile's inputs are requested now and arrive during this tile's MMAs and epilogue
-        fetch(tile + tstep, cur);
-        fence_async_smem();
-        __syncthreads();
-        if (tid == 0) {
-            tc_after_sync();
-            for (int ks = 0; ks < KT; ++ks)
-                for (int pr = 0; pr < 6; ++pr) {
-                    const uint64_t da = sdesc(aBase + kProdA[pr] * (uint32_t)aplane + ks * 2 * lboA, lboA, 128);
-                    const uint64_t db = sdesc(bBase + kProdB[pr] * (uint32_t)bplane + ks * 2 * lboB, lboB, 128);
-                    mma_bf16_ss(tmem, da, db, idesc, (ks | pr) ? 1u : 0u);
+            const int m = valid ? __ldg(&mat[n >> 2]) : 0;
+            if (u > 0 && !bar_wait(&done[b], (u - 1) & 1u, err)) break;
+            unsigned char* A = sA + b * abuf;
+#pragma unroll
+            for (int cl = 0; cl < HM / 8; ++cl) {
+                float v[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const int j = side * HM + cl * 8 + k;
+                    double sv = 0.0;
+                    if (valid && j < nm) {
+                        if (x) {
+                            sv = (double)__ldg(&sigl[(size_t)m * nmpad + j]) * raw[cl * 8 + k];
+                            if (add) sv += __ldcs(&add[(size_t)j * NENK + n]);
+                        } else {
+                            sv = raw[cl * 8 + k];
+                        }
+                    }
+                    v[k] = (float)sv;
                 }
-            mma_commit(bar);
+                uint4 hi, mid, lo;
+                split8(v, hi, mid, lo);
+                unsigned char* row = A + (size_t)(side * (HM / 8) + cl) * kTM * 16 + (size_t)r * 16;
+                *reinterpret_cast<uint4*>(row) = hi;
+                *reinterpret_cast<uint4*>(row + aplane) = mid;
+                *reinterpret_cast<uint4*>(row + 2 * aplane) = lo;
+            }
+            fence_async_smem();
+            bar_arrive(&full[b]);
         }
-        ok = __syncthreads_and(bar_wait(bar, phase, err));
-        phase ^= 1u;
-        tc_after_sync();
-        if (ok) {
-            // epilogue: warp w reads TMEM lanes 32w..32w+31 = its threads' nodes
-            const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-            for (int c0 = 0; c0 < NH; c0 += 16) {
+    } else if (warp < 16) {
+        // ---- epilogue: warps w and w + 4 share TMEM lanes 32(w%4).. and split the columns ----
+        const int e = warp - 8;
+        const int r = (e & 3) * 32 + (tid & 31);
+        const int ngr = NH / 16, per = (ngr + 1) / 2;
+        const int g0 = (e >> 2) * per, g1 = min(ngr, g0 + per);
+        const uint32_t lane_base = tmem + ((uint32_t)((e & 3) * 32) << 16);
+        int it = 0;
+        for (long long tile = t0; tile < ntiles; tile += tstep, ++it) {
+            const int b = it & 1;
+            const uint32_t u = (uint32_t)(it >> 1);
+            if (!bar_wait(&done[b], u & 1u, err)) break;
+            tc_after_sync();
+            const long long n = tile * kTM + r;
+            const bool valid = n < NENK;
+            for (int g = g0; g < g1; ++g) {
                 float v[16];
-                tmem_ld16(lane_base + (uint32_t)c0, v);
+                tmem_ld16(lane_base + (uint32_t)(b * 256 + g * 16), v);
                 if (valid) {
 #pragma unroll
                     for (int k = 0; k < 16; ++k) {
-                        const int i = half * NH + c0 + k;
+                        const int i = half * NH + g * 16 + k;
                         if (i < NI) {
                             float o = v[k];
                             if (qadd) o += qadd[(size_t)i * NENK + n];
@@ -267,43 +277,68 @@ __global__ void __launch_bounds__(128, 2) m2d_tc_kernel(const int* __restrict__ 
                     }
                 }
             }
+            tc_before_sync();
+            bar_arrive(&empty[b]);
         }
-        tc_before_sync();
-        ok = __syncthreads_and(ok && !*(volatile int*)err);
-        tc_after_sync();
+    } else if ((tid & 31) == 0) {
+        // ---- MMA issue ----
+        const uint32_t idesc = idesc_bf16(kTM, NH);
+        const uint32_t lboA = kTM * 16, lboB = (uint32_t)NH * 16;
+        const uint32_t aBase = smem_u32(sA), bBase = smem_u32(sB);
+        int it = 0;
+        for (long long tile = t0; tile < ntiles; tile += tstep, ++it) {
+            const int b = it & 1;
+            const uint32_t u = (uint32_t)(it >> 1);
+            if (!bar_wait(&full[b], u & 1u, err)) break;
+            if (u > 0 && !bar_wait(&empty[b], (u - 1) & 1u, err)) break;
+            tc_after_sync();
+            const uint32_t a0 = aBase + b * (uint32_t)abuf;
+            for (int ks = 0; ks < KT; ++ks)
+                for (int pr = 0; pr < 6; ++pr) {
+                    const uint64_t da = sdesc(a0 + kProdA[pr] * (uint32_t)aplane + ks * 2 * lboA, lboA, 128);
+                    const uint64_t db = sdesc(bBase + kProdB[pr] * (uint32_t)bplane + ks * 2 * lboB, lboB, 128);
+                    mma_bf16_ss(tmem + b * 256, da, db, idesc, (ks | pr) ? 1u : 0u);
+                }
+            mma_commit(&done[b]);
+        }
     }
     tc_before_sync();
     __syncthreads();
-    if (warp == 0) tmem_free(tmem, tmem_cols);
+    if (warp == 16) tmem_free(tmem, 512);
 }
 
 // ---------------------------------------------------------------------------------------------
-// D2M: z[j][n] = sum_i Dw[j][i] psi[i][n];  out = alpha * xin + beta * z.
-// CTA = 256 threads; psi is streamed in K chunks of 48 directions (double-buffered A planes):
-// threads t and t + 128 share node tile*128 + (t & 127) and split the chunk's directions, and in the
-// epilogue the moments, in halves.  KT = nmpad / 16.
+// D2M: z[j][n] = sum_i Dw[j][i] psi[i][n];  out = alpha * xin + beta * z.  KT = nmpad / 16.
+// One CTA per SM, warp-specialised; psi streams in K chunks of 48 directions through a ring of
+// kStages A buffers:
+//   warps 0-7   producers: threads t and t + 128 share node tile*128 + (t & 127), each loads and
+//               splits 24 directions of the chunk;
+//   warps 8-11  epilogue (TMEM lanes 32(w%4)..): out rows of the tile (two accumulators);
+//   warp 12     lane 0 issues the MMAs; the warp owns the TMEM allocation.
 // ---------------------------------------------------------------------------------------------
-constexpr int kKC = 48;   // directions per K chunk (3 MMA K-steps)
+constexpr int kKC = 48;       // directions per K chunk (3 MMA K-steps)
+constexpr int kStages = 3;    // A ring depth
 
 template <int KT>
-__global__ void __launch_bounds__(256, 1) d2m_tc_kernel(const int* __restrict__ active, const float* __restrict__ psi,
+__global__ void __launch_bounds__(416, 1) d2m_tc_kernel(const int* __restrict__ active, const float* __restrict__ psi,
                                                       const __nv_bfloat16* __restrict__ Dw, const double* xin,
                                                       double alpha, double beta, double* out, long long NENK, int NI,
                                                       int NIpad, int nm, int nmpad, long long ntiles, int* err) {
     if (active && *active == 0) return;
     extern __shared__ __align__(1024) unsigned char sm[];
     const int tid = threadIdx.x, warp = tid >> 5;
-    const int row = tid & 127, side = tid >> 7;
-    const int NKpad = (NIpad + kKC - 1) / kKC * kKC;         // directions padded to whole chunks
-    const size_t bplane = (size_t)nmpad * NKpad * 2;         // B: [3][K chunks][nmpad rows][16 B]
-    const size_t aplane = (size_t)kTM * kKC * 2;             // A chunk: [3][6 K chunks][128 rows][16 B]
+    const int NKpad = (NIpad + kKC - 1) / kKC * kKC;
+    const size_t bplane = (size_t)nmpad * NKpad * 2;
+    const size_t aplane = (size_t)kTM * kKC * 2;
+    const size_t abuf = ((3 * aplane + 1023) / 1024) * 1024;
     unsigned char* sB = sm;
-    unsigned char* sA0 = sm + ((3 * bplane + 1023) / 1024) * 1024;
-    unsigned char* sA1 = sA0 + ((3 * aplane + 1023) / 1024) * 1024;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sA1 + 3 * aplane);   // [2]
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 2);
-    // B = Dw planes [3][nmpad][NIpad] (row-major) staged K-major: rows = moments, K = directions
-    {
+    unsigned char* sA = sm + ((3 * bplane + 1023) / 1024) * 1024;   // [kStages] buffers
+    uint64_t* full = reinterpret_cast<uint64_t*>(sA + kStages * abuf);   // [kStages]
+    uint64_t* done = full + kStages;                                     // [kStages]
+    uint64_t* dfull = done + kStages;                                    // [2]
+    uint64_t* dempty = dfull + 2;                                        // [2]
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(dempty + 2);
+    {   // B = Dw planes [3][nmpad][NIpad] staged K-major: rows = moments, K = directions
         const int cc = NKpad / 8;
         const int total = 3 * nmpad * cc;
         for (int u = tid; u < total; u += blockDim.x) {
@@ -316,127 +351,140 @@ __global__ void __launch_bounds__(256, 1) d2m_tc_kernel(const int* __restrict__ 
         }
     }
     if (tid == 0) {
-        bar_init(&bar[0], 1);
-        bar_init(&bar[1], 1);
+        for (int k = 0; k < kStages; ++k) {
+            bar_init(&full[k], 256);
+            bar_init(&done[k], 1);
+        }
+        for (int k = 0; k < 2; ++k) {
+            bar_init(&dfull[k], 1);
+            bar_init(&dempty[k], 128);
+        }
     }
-    if (warp == 0) tmem_alloc(tslot, 64);
+    if (warp == 12) tmem_alloc(tslot, 128);
     fence_async_smem();
     tc_before_sync();
     __syncthreads();
     tc_after_sync();
     const uint32_t tmem = *tslot;
-    const uint32_t idesc = idesc_bf16(kTM, nmpad);
-    const uint32_t lboA = kTM * 16, lboB = (uint32_t)nmpad * 16;
-    const uint32_t bBase = smem_u32(sB);
     const int nchunks = NKpad / kKC;
-    uint32_t uses[2] = {0u, 0u};   // completed commits per buffer
-    bool ok = true;
-    // this thread's 24 psi values of a chunk (3 K lines of 8 directions), loaded one chunk ahead
-    float cur[24];
-    auto fetch = [&](long long tl, int chk, float (&r)[24]) {
-        const long long nn = tl * kTM + row;
-        const bool vv = tl < ntiles && nn < NENK;
+    if (warp < 8) {
+        // ---- producers ----
+        const int row = tid & 127, side = tid >> 7;
+        long long c = 0;   // chunk sequence number of this CTA
+        bool ok = true;
+        for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+            const long long n = tile * kTM + row;
+            const bool valid = n < NENK;
+            for (int ch = 0; ch < nchunks; ++ch, ++c) {
+                const int s = (int)(c % kStages);
+                const uint32_t u = (uint32_t)(c / kStages);
+                float v[24];
 #pragma unroll
-        for (int u = 0; u < 24; ++u) {
-            const int i = chk * kKC + side * 24 + u;
-            r[u] = (vv && i < NI) ? __ldcs(&psi[(size_t)i * NENK + nn]) : 0.f;
-        }
-    };
-    fetch(blockIdx.x, 0, cur);
-    for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-        const long long n = tile * kTM + row;
-        const bool valid = n < NENK;
-        for (int ch = 0; ch < nchunks && ok; ++ch) {
-            const int b = ch & 1;
-            unsigned char* sA = b ? sA1 : sA0;
-            float nxt[24];
-            if (ch + 1 < nchunks) fetch(tile, ch + 1, nxt);
-            else fetch(tile + gridDim.x, 0, nxt);
-            // the buffer's previous MMAs must be done before it is overwritten
-            if (uses[b] > 0) {
-                ok = __syncthreads_and(bar_wait(&bar[b], (uses[b] - 1) & 1u, err));
-                if (!ok) break;
+                for (int k = 0; k < 24; ++k) {
+                    const int i = ch * kKC + side * 24 + k;
+                    v[k] = (valid && i < NI) ? __ldcs(&psi[(size_t)i * NENK + n]) : 0.f;
+                }
+                if (u > 0 && !bar_wait(&done[s], (u - 1) & 1u, err)) {
+                    ok = false;
+                    break;
+                }
+                unsigned char* A = sA + s * abuf;
+#pragma unroll
+                for (int cl = 0; cl < 3; ++cl) {
+                    float w[8];
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) w[k] = v[cl * 8 + k];
+                    uint4 hi, mid, lo;
+                    split8(w, hi, mid, lo);
+                    unsigned char* rp = A + (size_t)(side * 3 + cl) * kTM * 16 + (size_t)row * 16;
+                    *reinterpret_cast<uint4*>(rp) = hi;
+                    *reinterpret_cast<uint4*>(rp + aplane) = mid;
+                    *reinterpret_cast<uint4*>(rp + 2 * aplane) = lo;
+                }
+                fence_async_smem();
+                bar_arrive(&full[s]);
             }
-#pragma unroll
-            for (int cl = 0; cl < 3; ++cl) {
-                const int c = side * 3 + cl;
-                float v[8];
-#pragma unroll
-                for (int k = 0; k < 8; ++k) v[k] = cur[cl * 8 + k];
-                uint4 hi, mid, lo;
-                split8(v, hi, mid, lo);
-                unsigned char* r = sA + (size_t)c * kTM * 16 + (size_t)row * 16;
-                *reinterpret_cast<uint4*>(r) = hi;
-                *reinterpret_cast<uint4*>(r + aplane) = mid;
-                *reinterpret_cast<uint4*>(r + 2 * aplane) = lo;
-            }
-#pragma unroll
-            for (int u = 0; u < 24; ++u) cur[u] = nxt[u];
-            fence_async_smem();
-            __syncthreads();
-            if (tid == 0) {
-                tc_after_sync();
-                const uint32_t aBase = smem_u32(sA);
-                for (int ks = 0; ks < kKC / 16; ++ks)
-                    for (int pr = 0; pr < 6; ++pr) {
-                        const uint64_t da = sdesc(aBase + kProdA[pr] * (uint32_t)aplane + ks * 2 * lboA, lboA, 128);
-                        const uint64_t db = sdesc(bBase + kProdB[pr] * (uint32_t)bplane +
-                                                      (uint32_t)(ch * (kKC / 8) + ks * 2) * lboB, lboB, 128);
-                        mma_bf16_ss(tmem, da, db, idesc, (ch | ks | pr) ? 1u : 0u);
-                    }
-                mma_commit(&bar[b]);
-            }
-            ++uses[b];
         }
-        if (!ok) break;
-        // epilogue operands: this thread's half of the moments (side * KT*8 ..), requested before
-        // the wait so that their latency overlaps the last MMAs
-        constexpr int CPS = KT * 8;   // columns per side
-        double xv[CPS];
+    } else if (warp < 12) {
+        // ---- epilogue ----
+        const int r = tid - 256;
+        const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+        constexpr int NMP = KT * 16;
+        int it = 0;
+        for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+            const int b = it & 1;
+            const uint32_t u = (uint32_t)(it >> 1);
+            const long long n = tile * kTM + r;
+            const bool valid = n < NENK;
+            double xv[NMP];
 #pragma unroll
-        for (int u = 0; u < CPS; ++u) {
-            const int j = side * CPS + u;
-            xv[u] = (xin && valid && j < nm) ? xin[(size_t)j * NENK + n] : 0.0;
-        }
-        // all chunks of the tile: wait for the last commit of each buffer
-        for (int b = 0; b < 2 && ok; ++b)
-            if (uses[b] > 0) ok = __syncthreads_and(bar_wait(&bar[b], (uses[b] - 1) & 1u, err));
-        tc_after_sync();
-        if (ok) {
-            // warps w and w + 4 share TMEM lanes 32(w%4)..; each reads its side's columns
-            const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+            for (int j = 0; j < NMP; ++j) xv[j] = (xin && valid && j < nm) ? xin[(size_t)j * NENK + n] : 0.0;
+            if (!bar_wait(&dfull[b], u & 1u, err)) break;
+            tc_after_sync();
 #pragma unroll
             for (int g = 0; g < KT; ++g) {
-                float v[8];
-                tmem_ld8(lane_base + (uint32_t)(side * CPS + g * 8), v);
+                float v[16];
+                tmem_ld16(lane_base + (uint32_t)(b * 64 + g * 16), v);
                 if (valid) {
 #pragma unroll
-                    for (int k = 0; k < 8; ++k) {
-                        const int j = side * CPS + g * 8 + k;
-                        if (j < nm) out[(size_t)j * NENK + n] = beta * (double)v[k] + alpha * xv[g * 8 + k];
+                    for (int k = 0; k < 16; ++k) {
+                        const int j = g * 16 + k;
+                        if (j < nm) out[(size_t)j * NENK + n] = beta * (double)v[k] + alpha * xv[j];
                     }
                 }
             }
+            tc_before_sync();
+            bar_arrive(&dempty[b]);
         }
-        tc_before_sync();
-        ok = __syncthreads_and(ok && !*(volatile int*)err);
-        tc_after_sync();
+    } else if ((tid & 31) == 0) {
+        // ---- MMA issue ----
+        const uint32_t idesc = idesc_bf16(kTM, nmpad);
+        const uint32_t lboA = kTM * 16, lboB = (uint32_t)nmpad * 16;
+        const uint32_t aBase = smem_u32(sA), bBase = smem_u32(sB);
+        long long c = 0;
+        int it = 0;
+        bool ok = true;
+        for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++it) {
+            const int b = it & 1;
+            const uint32_t ut = (uint32_t)(it >> 1);
+            if (ut > 0 && !bar_wait(&dempty[b], (ut - 1) & 1u, err)) break;
+            for (int ch = 0; ch < nchunks; ++ch, ++c) {
+                const int s = (int)(c % kStages);
+                const uint32_t u = (uint32_t)(c / kStages);
+                if (!bar_wait(&full[s], u & 1u, err)) {
+                    ok = false;
+                    break;
+                }
+                tc_after_sync();
+                const uint32_t a0 = aBase + s * (uint32_t)abuf;
+                for (int ks = 0; ks < kKC / 16; ++ks)
+                    for (int pr = 0; pr < 6; ++pr) {
+                        const uint64_t da = sdesc(a0 + kProdA[pr] * (uint32_t)aplane + ks * 2 * lboA, lboA, 128);
+                        const uint64_t db = sdesc(bBase + kProdB[pr] * (uint32_t)bplane +
+                                                      (uint32_t)(ch * (kKC / 8) + ks * 2) * lboB, lboB, 128);
+                        mma_bf16_ss(tmem + b * 64, da, db, idesc, (ch | ks | pr) ? 1u : 0u);
+                    }
+                mma_commit(&done[s]);
+                if (ch == nchunks - 1) mma_commit(&dfull[b]);
+            }
+        }
     }
     tc_before_sync();
     __syncthreads();
-    if (warp == 0) tmem_free(tmem, 64);
+    if (warp == 12) tmem_free(tmem, 128);
 }
 
 size_t m2d_tc_smem(int NH, int nmpad) {
     const size_t b = ((3 * (size_t)NH * nmpad * 2 + 1023) / 1024) * 1024;
-    return b + 3 * (size_t)kTM * nmpad * 2 + 64;
+    const size_t a = ((3 * (size_t)kTM * nmpad * 2 + 1023) / 1024) * 1024;
+    return b + 2 * a + 64;
 }
 
 size_t d2m_tc_smem(int NIpad, int nmpad) {
     const int NKpad = (NIpad + kKC - 1) / kKC * kKC;
     const size_t b = ((3 * (size_t)nmpad * NKpad * 2 + 1023) / 1024) * 1024;
     const size_t a = ((3 * (size_t)kTM * kKC * 2 + 1023) / 1024) * 1024;
-    return b + a + 3 * (size_t)kTM * kKC * 2 + 64;
+    return b + kStages * a + 128;
 }
 
 int* tc_error_flag() {
@@ -461,28 +509,27 @@ int launch_m2d_tc(Handle* h, const double* x, const float* sigl, const double* a
     const int nhalves = h->NIpad > 256 ? 2 : 1;
     const int NH = ((h->NIpad + nhalves - 1) / nhalves + 15) / 16 * 16;
     if (NH > 256 || h->nmpad % 16 || h->nmpad > 64 || h->NIpad % 8) return LB_ERR_ARG;
-    const uint32_t cols = NH <= 32 ? 32 : NH <= 64 ? 64 : NH <= 128 ? 128 : 256;
-    // at most two CTAs per SM: their TMEM (<= 2 x 256 columns) always fits, so no allocation waits
-    const size_t smem = std::max<size_t>(m2d_tc_smem(NH, h->nmpad), 80 * 1024);
-    if (smem > 113 * 1024) return LB_ERR_ARG;
+    // one CTA per SM (it holds all 512 TMEM columns: two accumulators of up to 256)
+    const size_t smem = std::max<size_t>(m2d_tc_smem(NH, h->nmpad), 116 * 1024);
+    if (smem > 227 * 1024) return LB_ERR_ARG;
     int* err = tc_error_flag();
     if (!err) return LB_ERR_OOM;
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(m2d_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 113 * 1024);
-        cudaFuncSetAttribute(m2d_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 113 * 1024);
-        cudaFuncSetAttribute(m2d_tc_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 113 * 1024);
-        cudaFuncSetAttribute(m2d_tc_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 113 * 1024);
+        cudaFuncSetAttribute(m2d_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(m2d_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(m2d_tc_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(m2d_tc_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
         attr = true;
     }
     const long long ntiles = (h->NENK + kTM - 1) / kTM;
-    long long grid = std::min<long long>(ntiles * nhalves, (long long)h->sm_count * 2);
+    long long grid = std::min<long long>(ntiles * nhalves, (long long)h->sm_count);
     grid = std::max<long long>(nhalves, grid / nhalves * nhalves);
-    const int KT = h->nmpad / 16;
-#define LB_M2DTC(K)                                                                                               \
-    m2d_tc_kernel<K><<<(int)grid, 128, smem, h->stream>>>(h->d_active, x, sigl, a, qadd, h->d_mat, h->d_Ym2d, q, h->NENK, \
-                                                           h->NI, h->NIpad, h->nm, h->nmpad, NH, nhalves, cols, ntiles, err)
-    switch (KT) {
+#define LB_M2DTC(K)                                                                                                \
+    m2d_tc_kernel<K><<<(int)grid, 544, smem, h->stream>>>(h->d_active, x, sigl, a, qadd, h->d_mat, h->d_Ym2d, q,   \
+                                                           h->NENK, h->NI, h->NIpad, h->nm, h->nmpad, NH, nhalves, \
+                                                           ntiles, err)
+    switch (h->nmpad / 16) {
         case 1: LB_M2DTC(1); break;
         case 2: LB_M2DTC(2); break;
         case 3: LB_M2DTC(3); break;
@@ -495,8 +542,8 @@ int launch_m2d_tc(Handle* h, const double* x, const float* sigl, const double* a
 
 int launch_d2m_tc(Handle* h, const float* psi, const double* xin, double alpha, double beta, double* out) {
     if (h->nmpad > 64 || h->nmpad % 16 || h->NIpad % 8) return LB_ERR_ARG;
-    // at most two CTAs per SM (2 x 64 TMEM columns)
-    const size_t smem = std::max<size_t>(d2m_tc_smem(h->NIpad, h->nmpad), 80 * 1024);
+    // one CTA per SM (two accumulators of up to 64 columns in a 128-column allocation)
+    const size_t smem = std::max<size_t>(d2m_tc_smem(h->NIpad, h->nmpad), 116 * 1024);
     if (smem > 227 * 1024) return LB_ERR_ARG;
     int* err = tc_error_flag();
     if (!err) return LB_ERR_OOM;
@@ -510,8 +557,8 @@ int launch_d2m_tc(Handle* h, const float* psi, const double* xin, double alpha, 
     }
     const long long ntiles = (h->NENK + kTM - 1) / kTM;
     const long long grid = std::min<long long>(ntiles, (long long)h->sm_count);
-#define LB_D2MTC(K)                                                                                        \
-    d2m_tc_kernel<K><<<(int)grid, 256, smem, h->stream>>>(h->d_active, psi, h->d_Yd2m, xin, alpha, beta, out, \
+#define LB_D2MTC(K)                                                                                         \
+    d2m_tc_kernel<K><<<(int)grid, 416, smem, h->stream>>>(h->d_active, psi, h->d_Yd2m, xin, alpha, beta, out, \
                                                            h->NENK, h->NI, h->NIpad, h->nm, h->nmpad, ntiles, err)
     switch (h->nmpad / 16) {
         case 1: LB_D2MTC(1); break;
