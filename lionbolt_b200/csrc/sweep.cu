@@ -59,6 +59,9 @@ struct SweepArgs {
     int Nm;
     SweepStatus* status;
     long long spin_limit;
+    const int4* __restrict__ rec;     // 32-byte element records (when ngeom > 0)
+    const float4* __restrict__ gtab;  // [ngeom][3] face vectors of the distinct element shapes
+    int ngeom;
 };
 
 __device__ __forceinline__ float pick(const float4& v, int idx) {
@@ -125,10 +128,33 @@ template <bool kCG, bool kHaveQ = false>
 __device__ __forceinline__ void assemble_g(const float* base, float4 dir, int item, const Geom& G, const float* s_sigt,
                                            Update& u, float4 qpre);
 
+// Element record from the 32-byte record and the shape table in shared memory (one 256-bit load).
+__device__ __forceinline__ Geom load_geom_tab(const int4* __restrict__ rec, const float4* s_gtab, int e) {
+    float r[8];
+    ld_nc_v8(reinterpret_cast<const float*>(rec + (size_t)e * 2), r);
+    Geom g;
+    g.gn = make_int4(__float_as_int(r[0]), __float_as_int(r[1]), __float_as_int(r[2]), __float_as_int(r[3]));
+    const int s = __float_as_int(r[4]);
+    g.gx = s_gtab[3 * s + 0];
+    g.gy = s_gtab[3 * s + 1];
+    g.gz = s_gtab[3 * s + 2];
+    return g;
+}
+
+// Copies the shape table into shared memory (kernels launched with 48 * ngeom bytes of dynamic
+// shared memory); returns the table, or nullptr when the mesh has none.
+__device__ __forceinline__ const float4* load_gtab(const SweepArgs& a, float4* s_gtab) {
+    if (a.ngeom <= 0) return nullptr;
+    for (int k = threadIdx.x; k < 3 * a.ngeom; k += blockDim.x) s_gtab[k] = __ldg(&a.gtab[k]);
+    __syncthreads();
+    return s_gtab;
+}
+
 template <bool kCG, bool kHaveQ = false>
 __device__ __forceinline__ void assemble(const SweepArgs& a, const float* base, float4 dir, int item,
-                                         const float* s_sigt, Update& u, float4 qpre = make_float4(0.f, 0.f, 0.f, 0.f)) {
-    const Geom G = load_geom(a.geom, item & 0xFFFFFF);
+                                         const float* s_sigt, Update& u, float4 qpre = make_float4(0.f, 0.f, 0.f, 0.f),
+                                         const float4* s_gtab = nullptr) {
+    const Geom G = s_gtab ? load_geom_tab(a.rec, s_gtab, item & 0xFFFFFF) : load_geom(a.geom, item & 0xFFFFFF);
     assemble_g<kCG, kHaveQ>(base, dir, item, G, s_sigt, u, qpre);
 }
 
@@ -219,9 +245,11 @@ __device__ __forceinline__ void load_sigt(const SweepArgs& a, float* s_sigt) {
 // Level-synchronous schedule: CTA-owned directions, barrier between wavefront levels.
 // ---------------------------------------------------------------------------------------------
 template <int DPC, int ILP>
-__global__ void __launch_bounds__(ILP == 1 ? 1024 : 512) sweep_levels_kernel(SweepArgs a) {
+__global__ void __launch_bounds__(1024) sweep_levels_kernel(SweepArgs a) {
     __shared__ float s_sigt[256];
+    extern __shared__ float4 s_gtab_dyn[];
     load_sigt(a, s_sigt);
+    const float4* s_gtab = load_gtab(a, s_gtab_dyn);
     const int nt = blockDim.x;
     for (int d0 = blockIdx.x * DPC; d0 < a.NI; d0 += gridDim.x * DPC) {
         int nl[DPC], lb[DPC];
@@ -255,7 +283,8 @@ __global__ void __launch_bounds__(ILP == 1 ? 1024 : 512) sweep_levels_kernel(Swe
                     Update up[ILP];
 #pragma unroll
                     for (int u = 0; u < ILP; ++u)
-                        if (has[u]) assemble<false>(a, base, dir[d], item[u], s_sigt, up[u]);
+                        if (has[u]) assemble<false>(a, base, dir[d], item[u], s_sigt, up[u],
+                                                    make_float4(0.f, 0.f, 0.f, 0.f), s_gtab);
 #pragma unroll
                     for (int u = 0; u < ILP; ++u)
                         if (has[u]) finish<false>(base, item[u], up[u]);
@@ -272,7 +301,9 @@ __global__ void __launch_bounds__(ILP == 1 ? 1024 : 512) sweep_levels_kernel(Swe
 template <int MINB>
 __global__ void __launch_bounds__(1024, MINB) sweep_levels_pf_kernel(SweepArgs a) {
     __shared__ float s_sigt[256];
+    extern __shared__ float4 s_gtab_dyn[];
     load_sigt(a, s_sigt);
+    const float4* s_gtab = load_gtab(a, s_gtab_dyn);
     const int nt = blockDim.x;
     for (int i = blockIdx.x; i < a.NI; i += gridDim.x) {
         const int nl = __ldg(&a.nlev[i]);
@@ -299,13 +330,13 @@ __global__ void __launch_bounds__(1024, MINB) sweep_levels_pf_kernel(SweepArgs a
             }
             if (es0 < s1) {
                 Update up;
-                assemble<false, true>(a, base, dir, cur_item, s_sigt, up, cur_q);
+                assemble<false, true>(a, base, dir, cur_item, s_sigt, up, cur_q, s_gtab);
                 finish<false>(base, cur_item, up);
             }
             for (int es = es0 + nt; es < s1; es += nt) {
                 const int item = __ldcs(&it[es]);
                 Update up;
-                assemble<false>(a, base, dir, item, s_sigt, up);
+                assemble<false>(a, base, dir, item, s_sigt, up, make_float4(0.f, 0.f, 0.f, 0.f), s_gtab);
                 finish<false>(base, item, up);
             }
             s0 = n0;
@@ -624,18 +655,19 @@ struct Config {
 const Config kConfigs[] = {
     {4, 1024, 2, 1}, {4, 512, 2, 1}, {4, 512, 3, 1}, {4, 1024, 3, 1}, {4, 512, 6, 1},
     {0, 1024, 1, 1}, {0, 512, 1, 1}, {2, 1024, 1, 1}, {3, 512, 0, 1}, {1, 256, 0, 0},
-    {4, 768, 2, 1},
+    {4, 768, 2, 1}, {0, 1024, 1, 2}, {0, 1024, 1, 3}, {0, 768, 1, 3},
 };
 constexpr int kNumConfigs = sizeof(kConfigs) / sizeof(kConfigs[0]);
 
 template <int DPC, int ILP>
 cudaError_t launch_levels(const SweepArgs& a, int threads, int sm_count, cudaStream_t s) {
+    const size_t smem = sizeof(float4) * 3 * (size_t)a.ngeom;
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_levels_kernel<DPC, ILP>, threads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_levels_kernel<DPC, ILP>, threads, smem);
     if (per_sm < 1) per_sm = 1;
     int ctas = (a.NI + DPC - 1) / DPC;
     int grid = std::min(ctas, sm_count * per_sm);
-    sweep_levels_kernel<DPC, ILP><<<grid, threads, 0, s>>>(a);
+    sweep_levels_kernel<DPC, ILP><<<grid, threads, smem, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -698,11 +730,12 @@ cudaError_t launch_flags(const SweepArgs& a, int sm_count, cudaStream_t s) {
 
 template <int MINB>
 cudaError_t launch_levels_pf(const SweepArgs& a, int threads, int sm_count, cudaStream_t s) {
+    const size_t smem = sizeof(float4) * 3 * (size_t)a.ngeom;
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_levels_pf_kernel<MINB>, threads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_levels_pf_kernel<MINB>, threads, smem);
     if (per_sm < 1) per_sm = 1;
     int grid = std::min(a.NI, sm_count * per_sm);
-    sweep_levels_pf_kernel<MINB><<<grid, threads, 0, s>>>(a);
+    sweep_levels_pf_kernel<MINB><<<grid, threads, smem, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -731,7 +764,7 @@ int launch_sweep_batch(cudaStream_t st, const BatchWork* work, int nwork, int* c
 }
 
 int launch_sweep(Handle* h, float* psi) {
-    SweepArgs a;
+    SweepArgs a{};
     a.items = h->d_items;
     a.pitems = h->d_pitems;
     a.pbase = h->d_pbase;
@@ -752,6 +785,9 @@ int launch_sweep(Handle* h, float* psi) {
     a.status = h->d_status;
     // about a second of polling with 64-ns naps before a wait is declared stuck
     a.spin_limit = 1LL << 24;
+    a.rec = h->d_rec;
+    a.gtab = h->d_gtab;
+    a.ngeom = h->ngeom;
 
     if (h->sweep_cfg_forced < 0) {
         const char* env = std::getenv("LB_SWEEP_CONFIG");
@@ -778,6 +814,7 @@ int launch_sweep(Handle* h, float* psi) {
         cudaFuncGetAttributes(&fa, sweep_levels_pf_kernel<2>);
         cudaFuncGetAttributes(&fa, sweep_levels_kernel<1, 1>);
         cudaFuncGetAttributes(&fa, sweep_levels_kernel<1, 2>);
+        cudaFuncGetAttributes(&fa, sweep_levels_kernel<1, 3>);
         cudaFuncGetAttributes(&fa, sweep_levels_kernel<2, 1>);
         cudaFuncGetAttributes(&fa, sweep_levels_kernel<2, 2>);
         cudaFuncGetAttributes(&fa, sweep_dataflow_kernel);
@@ -826,6 +863,7 @@ int launch_sweep(Handle* h, float* psi) {
         e = cudaGetLastError();
     } else if (cfg.dpc == 1 && cfg.ilp == 1) e = launch_levels<1, 1>(a, cfg.threads, h->sm_count, h->stream);
     else if (cfg.dpc == 1 && cfg.ilp == 2) e = launch_levels<1, 2>(a, cfg.threads, h->sm_count, h->stream);
+    else if (cfg.dpc == 1 && cfg.ilp == 3) e = launch_levels<1, 3>(a, cfg.threads, h->sm_count, h->stream);
     else if (cfg.dpc == 2 && cfg.ilp == 1) e = launch_levels<2, 1>(a, cfg.threads, h->sm_count, h->stream);
     else e = launch_levels<2, 2>(a, cfg.threads, h->sm_count, h->stream);
     timer_end(h, t);
@@ -933,7 +971,7 @@ extern "C" int lb_transport_inv_noalloc(lb_handle* hh, float* psi) {
         g_noalloc_ptr[h->device] = p;
     }
     int* base = static_cast<int*>(g_noalloc_ptr[h->device]);
-    SweepArgs a;
+    SweepArgs a{};
     a.items = h->d_items;
     a.pitems = h->d_pitems;
     a.pbase = h->d_pbase;

@@ -58,7 +58,7 @@ def test_transport_inverse_matches_oracle(case):
     assert T.timers()["sweep"][1] >= 1
 
 
-@pytest.mark.parametrize("cfg", range(11))
+@pytest.mark.parametrize("cfg", range(14))
 def test_every_sweep_schedule_matches_oracle(cfg, monkeypatch):
     """Each launch candidate of the sweep autotuner (levels, prefetching levels, element flags,
     grouped directions, dataflow) reproduces the oracle's T^{-1} on a two-material mesh."""
