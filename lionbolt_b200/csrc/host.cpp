@@ -122,7 +122,7 @@ static int dev_upload(Handle* h, T** p, const T* src, size_t count, const char* 
 }
 
 static void free_all(Handle* h) {
-    void* ptrs[] = {h->d_geom, h->d_rec, h->d_gtab, h->d_mat, h->d_items, h->d_groups, h->d_pitems, h->d_pbase, h->d_chunks, h->d_lvl_start, h->d_lvl_base, h->d_nlev, h->d_done, h->d_status, h->d_dirs, h->d_sigt,
+    void* ptrs[] = {h->d_geom, h->d_rec, h->d_gtab, h->d_tmat, h->d_mat, h->d_items, h->d_groups, h->d_pitems, h->d_pbase, h->d_chunks, h->d_lvl_start, h->d_lvl_base, h->d_nlev, h->d_done, h->d_status, h->d_dirs, h->d_sigt,
                     h->d_psi, h->d_qext, h->d_Ym2d, h->d_Yd2m, h->d_sigl, h->d_lofj, h->d_V, h->d_Z, h->d_x,
                     h->d_b, h->d_t, h->d_red, h->d_unc, h->d_phi_all, h->d_src, h->d_dose, h->d_flux,
                     h->d_sigl_mg, h->d_yb, h->d_dd};
@@ -392,12 +392,13 @@ int lb_set_mesh(lb_handle* h, int NE, int NN, const double* rg, const int* node,
     }
     int rc = dev_upload(h, &h->d_geom, geom.data(), geom.size(), "upload geometry");
     if (rc) return rc;
-    // distinct element shapes (bitwise-equal FP32 face vectors); a table of at most kMaxShapes
-    // shapes replaces the 48 bytes of face vectors per element by a 4-byte index
+    // distinct (element shape, material) types: bitwise-equal FP32 face vectors and equal material.
+    // With at most 256 types every element is described by its neighbour words alone, the 8-bit type
+    // index taking the place of the material bits.
     {
-        constexpr int kMaxShapes = 512;
+        constexpr int kMaxTypes = 256;
         struct Key {
-            uint32_t v[12];
+            uint32_t v[13];
             bool operator==(const Key& o) const { return std::memcmp(v, o.v, sizeof v) == 0; }
         };
         struct KeyHash {
@@ -407,34 +408,39 @@ int lb_set_mesh(lb_handle* h, int NE, int NN, const double* rg, const int* node,
                 return (size_t)x;
             }
         };
-        std::unordered_map<Key, int, KeyHash> shapes;
+        std::unordered_map<Key, int, KeyHash> types;
         std::vector<int> idx(NE);
         std::vector<float4> tab;
+        std::vector<int> tmat;
         bool ok = true;
         for (int e = 0; e < NE && ok; ++e) {
             Key k;
             std::memcpy(k.v, &geom[(size_t)e * 4], 48);
-            auto it = shapes.find(k);
-            if (it == shapes.end()) {
-                if ((int)shapes.size() >= kMaxShapes) { ok = false; break; }
-                it = shapes.emplace(k, (int)shapes.size()).first;
+            k.v[12] = (uint32_t)h->mat[e];
+            auto it = types.find(k);
+            if (it == types.end()) {
+                if ((int)types.size() >= kMaxTypes) { ok = false; break; }
+                it = types.emplace(k, (int)types.size()).first;
                 tab.push_back(geom[(size_t)e * 4 + 0]);
                 tab.push_back(geom[(size_t)e * 4 + 1]);
                 tab.push_back(geom[(size_t)e * 4 + 2]);
+                tmat.push_back(h->mat[e]);
             }
             idx[e] = it->second;
         }
         h->ngeom = 0;
         if (ok) {
-            std::vector<int4> rec((size_t)NE * 2);
+            std::vector<int4> rec(NE);
             for (int e = 0; e < NE; ++e) {
-                const int* w = reinterpret_cast<const int*>(&geom[(size_t)e * 4 + 3]);
-                rec[(size_t)e * 2 + 0] = make_int4(w[0], w[1], w[2], w[3]);
-                rec[(size_t)e * 2 + 1] = make_int4(idx[e], 0, 0, 0);
+                uint32_t w[4];
+                for (int f = 0; f < 4; ++f)
+                    w[f] = (h->nbrpack[(size_t)e * 4 + f] & 0x3FFFFFFFu) | ((uint32_t)((idx[e] >> (2 * f)) & 3) << 30);
+                rec[e] = make_int4((int)w[0], (int)w[1], (int)w[2], (int)w[3]);
             }
             if ((rc = dev_upload(h, &h->d_rec, rec.data(), rec.size(), "upload element records"))) return rc;
-            if ((rc = dev_upload(h, &h->d_gtab, tab.data(), tab.size(), "upload shape table"))) return rc;
-            h->ngeom = (int)shapes.size();
+            if ((rc = dev_upload(h, &h->d_gtab, tab.data(), tab.size(), "upload type table"))) return rc;
+            if ((rc = dev_upload(h, &h->d_tmat, tmat.data(), tmat.size(), "upload type materials"))) return rc;
+            h->ngeom = (int)types.size();
         }
     }
     rc = dev_upload(h, &h->d_mat, h->mat.data(), h->mat.size(), "upload materials");

@@ -85,11 +85,13 @@ struct Handle {
 
     // ---- device buffers ----
     float4* d_geom = nullptr;      // [NE][4] (snx, sny, snz, nbrpack)
-    // meshes with few distinct element shapes (voxel-based meshes): the face vectors of the distinct
-    // shapes in a table, and per element a 32-byte record {nbrpack[4], shape index, 0, 0, 0}
-    int4* d_rec = nullptr;         // [NE][2]
+    // meshes with few distinct (element shape, material) types (voxel-based meshes): the face vectors
+    // and material of every type in a table, and per element a 16-byte record: the four neighbour
+    // words with the 8-bit type index in the bits that otherwise carry the material
+    int4* d_rec = nullptr;         // [NE]
     float4* d_gtab = nullptr;      // [ngeom][3] (snx, sny, snz)
-    int ngeom = 0;                 // 0: no table (use d_geom)
+    int* d_tmat = nullptr;         // [ngeom] material of each type
+    int ngeom = 0;                 // number of types; 0: no table (use d_geom)
     int* d_mat = nullptr;          // [NE]
     int* d_items = nullptr;        // [NI][NE]
     int4* d_chunks = nullptr;      // [nchunks]

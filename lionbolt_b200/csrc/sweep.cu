@@ -59,8 +59,9 @@ struct SweepArgs {
     int Nm;
     SweepStatus* status;
     long long spin_limit;
-    const int4* __restrict__ rec;     // 32-byte element records (when ngeom > 0)
-    const float4* __restrict__ gtab;  // [ngeom][3] face vectors of the distinct element shapes
+    const int4* __restrict__ rec;     // 16-byte element records with type indices (when ngeom > 0)
+    const float4* __restrict__ gtab;  // [ngeom][3] face vectors of the element types
+    const int* __restrict__ tmat;     // [ngeom] material of the element types
     int ngeom;
 };
 
@@ -128,24 +129,31 @@ template <bool kCG, bool kHaveQ = false>
 __device__ __forceinline__ void assemble_g(const float* base, float4 dir, int item, const Geom& G, const float* s_sigt,
                                            Update& u, float4 qpre);
 
-// Element record from the 32-byte record and the shape table in shared memory (one 256-bit load).
+// Element from its 16-byte record (one 128-bit load) and the type table in shared memory.  The type
+// index sits in the bits that otherwise carry the material, so the element update reads it as the
+// material id and the CTA's cross-section table is indexed by type (load_gtab).
 __device__ __forceinline__ Geom load_geom_tab(const int4* __restrict__ rec, const float4* s_gtab, int e) {
-    float r[8];
-    ld_nc_v8(reinterpret_cast<const float*>(rec + (size_t)e * 2), r);
     Geom g;
-    g.gn = make_int4(__float_as_int(r[0]), __float_as_int(r[1]), __float_as_int(r[2]), __float_as_int(r[3]));
-    const int s = __float_as_int(r[4]);
-    g.gx = s_gtab[3 * s + 0];
-    g.gy = s_gtab[3 * s + 1];
-    g.gz = s_gtab[3 * s + 2];
+    g.gn = __ldg(&rec[e]);
+    const int t = (int)(((unsigned)g.gn.x >> 30) | (((unsigned)g.gn.y >> 30) << 2) | (((unsigned)g.gn.z >> 30) << 4) |
+                        (((unsigned)g.gn.w >> 30) << 6));
+    g.gx = s_gtab[3 * t + 0];
+    g.gy = s_gtab[3 * t + 1];
+    g.gz = s_gtab[3 * t + 2];
     return g;
 }
 
-// Copies the shape table into shared memory (kernels launched with 48 * ngeom bytes of dynamic
-// shared memory); returns the table, or nullptr when the mesh has none.
-__device__ __forceinline__ const float4* load_gtab(const SweepArgs& a, float4* s_gtab) {
+// Copies the type table into shared memory (kernels launched with 48 * ngeom bytes of dynamic shared
+// memory) and re-indexes the cross sections by type; returns the table, or nullptr when the mesh has
+// none (then s_sigt stays indexed by material).
+__device__ __forceinline__ const float4* load_gtab(const SweepArgs& a, float4* s_gtab, float* s_sigt) {
     if (a.ngeom <= 0) return nullptr;
+    __syncthreads();   // s_sigt was filled by material
+    float st = 0.f;
+    if (threadIdx.x < a.ngeom) st = a.sigt[__ldg(&a.tmat[threadIdx.x])];
     for (int k = threadIdx.x; k < 3 * a.ngeom; k += blockDim.x) s_gtab[k] = __ldg(&a.gtab[k]);
+    __syncthreads();
+    if (threadIdx.x < 256) s_sigt[threadIdx.x] = threadIdx.x < a.ngeom ? st : 0.f;
     __syncthreads();
     return s_gtab;
 }
@@ -249,7 +257,7 @@ __global__ void __launch_bounds__(1024) sweep_levels_kernel(SweepArgs a) {
     __shared__ float s_sigt[256];
     extern __shared__ float4 s_gtab_dyn[];
     load_sigt(a, s_sigt);
-    const float4* s_gtab = load_gtab(a, s_gtab_dyn);
+    const float4* s_gtab = load_gtab(a, s_gtab_dyn, s_sigt);
     const int nt = blockDim.x;
     for (int d0 = blockIdx.x * DPC; d0 < a.NI; d0 += gridDim.x * DPC) {
         int nl[DPC], lb[DPC];
@@ -303,7 +311,7 @@ __global__ void __launch_bounds__(1024, MINB) sweep_levels_pf_kernel(SweepArgs a
     __shared__ float s_sigt[256];
     extern __shared__ float4 s_gtab_dyn[];
     load_sigt(a, s_sigt);
-    const float4* s_gtab = load_gtab(a, s_gtab_dyn);
+    const float4* s_gtab = load_gtab(a, s_gtab_dyn, s_sigt);
     const int nt = blockDim.x;
     for (int i = blockIdx.x; i < a.NI; i += gridDim.x) {
         const int nl = __ldg(&a.nlev[i]);
@@ -787,6 +795,7 @@ int launch_sweep(Handle* h, float* psi) {
     a.spin_limit = 1LL << 24;
     a.rec = h->d_rec;
     a.gtab = h->d_gtab;
+    a.tmat = h->d_tmat;
     a.ngeom = h->ngeom;
 
     if (h->sweep_cfg_forced < 0) {
