@@ -104,7 +104,8 @@ int lb_get_schedule(lb_handle* h, int* sl, unsigned char* upmask, int* nlevels, 
 int lb_transport_inv(lb_handle* h, double* s);
 
 /* T^{-1} in place on a caller-owned device vector, without allocating: psi is the FP32 angular
- * vector [NI][NENK] in device memory of the handle's GPU (same layout as lb_transport_inv).  No
+ * vector [NI][NENK] in device memory of the handle's GPU (same layout as lb_transport_inv), 16-byte
+ * aligned (LB_ERR_ARG otherwise, before anything is launched).  No
  * counterpart in the reference: it exists for callers that cannot allocate device memory at solve
  * time (a host framework that owns the allocator, a Fortran runtime that only passes pre-allocated
  * device arrays, a loop that must not hit cudaMalloc's implicit synchronisation).  Its dependency
@@ -171,6 +172,11 @@ int lb_synchronize(lb_handle* h);
  * directions per CTA, cfg[3] updates in flight per thread.  Returns
  * LB_ERR_STATE while candidates are still being timed (the first sweeps of a handle). */
 int lb_get_sweep_config(lb_handle* h, int* cfg);
+
+/* Number of distinct (element shape, material) types of the mesh when it has at most 256 of them
+ * (the sweep then reads 16-byte element records and a per-type table); 0 otherwise (64-byte
+ * records).  No counterpart in the reference. */
+int lb_mesh_types(lb_handle* h, int* ntypes);
 
 
 /* ---- Learned right preconditioner (no counterpart in the reference) ------------------------------

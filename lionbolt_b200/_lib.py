@@ -63,6 +63,7 @@ SIGNATURES = {
     "lb_sweep_stats": (ctypes.c_int, [_vp, _c_double_p, _c_double_p, _c_ll_p]),
     "lb_synchronize": (ctypes.c_int, [_vp]),
     "lb_get_sweep_config": (ctypes.c_int, [_vp, _c_int_p]),
+    "lb_mesh_types": (ctypes.c_int, [_vp, _c_int_p]),
     "lb_mg_update_inputs": (ctypes.c_int, [_vp, _c_double_p, _c_double_p, _c_double_p, _c_double_p, _c_double_p]),
     "lb_mark": (ctypes.c_int, [_vp, ctypes.c_int]),
     "lb_transport_inv_noalloc": (ctypes.c_int, [_vp, ctypes.c_void_p]),
@@ -195,6 +196,11 @@ class Handle:
         kind = int(cfg[0])
         return dict(schedule=names[kind] if 0 <= kind < len(names) else str(kind), threads=int(cfg[1]),
                     dirs_per_cta=int(cfg[2]), ilp=int(cfg[3]))
+
+    def mesh_types(self):
+        n = np.zeros(1, dtype=np.int32)
+        self.call("lb_mesh_types", iptr(n))
+        return int(n[0])
 
     def mark(self, slot):
         self.call("lb_mark", int(slot))

@@ -719,8 +719,9 @@ int lb_sweep_stats(lb_handle* h, double* bytes, double* updates, long long* upfa
     if (!h || !h->angle_ready) return LB_ERR_STATE;
     double upd = (double)h->NE * h->NI;
     // algorithmic bytes: q read (16 B) + psi write (16 B) + 3 FP32 face values per upstream face
-    // (12 B) per update, plus the packed schedule item (4 B) and one 64-B element record per pass
-    double b = upd * (16.0 + 16.0 + 4.0) + 12.0 * (double)h->nz_upstream + 64.0 * h->NE;
+    // (12 B) per update, plus the packed schedule item (4 B) and one element record per pass (16 B with
+    // the type table, 64 B without)
+    double b = upd * (16.0 + 16.0 + 4.0) + 12.0 * (double)h->nz_upstream + (h->ngeom ? 16.0 : 64.0) * h->NE;
     if (bytes) *bytes = b;
     if (updates) *updates = upd;
     if (upfaces) *upfaces = h->nz_upstream;
@@ -750,6 +751,13 @@ int lb_elapsed_ms(lb_handle* h, int a, int b, double* ms) {
 int lb_get_sweep_config(lb_handle* h, int* cfg) {
     if (!h || !cfg) return LB_ERR_ARG;
     if (sweep_config(h, &cfg[0], &cfg[1], &cfg[2], &cfg[3]) < 0) return LB_ERR_STATE;
+    return LB_OK;
+}
+
+int lb_mesh_types(lb_handle* h, int* ntypes) {
+    if (!h || !ntypes) return LB_ERR_ARG;
+    if (!h->mesh_ready) return fail(h, LB_ERR_STATE, "lb_mesh_types: mesh not set");
+    *ntypes = h->ngeom;
     return LB_OK;
 }
 

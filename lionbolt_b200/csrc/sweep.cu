@@ -132,15 +132,19 @@ __device__ __forceinline__ void assemble_g(const float* base, float4 dir, int it
 // Element from its 16-byte record (one 128-bit load) and the type table in shared memory.  The type
 // index sits in the bits that otherwise carry the material, so the element update reads it as the
 // material id and the CTA's cross-section table is indexed by type (load_gtab).
-__device__ __forceinline__ Geom load_geom_tab(const int4* __restrict__ rec, const float4* s_gtab, int e) {
+__device__ __forceinline__ Geom geom_from_rec(int4 rec, const float4* s_gtab) {
     Geom g;
-    g.gn = __ldg(&rec[e]);
+    g.gn = rec;
     const int t = (int)(((unsigned)g.gn.x >> 30) | (((unsigned)g.gn.y >> 30) << 2) | (((unsigned)g.gn.z >> 30) << 4) |
                         (((unsigned)g.gn.w >> 30) << 6));
     g.gx = s_gtab[3 * t + 0];
     g.gy = s_gtab[3 * t + 1];
     g.gz = s_gtab[3 * t + 2];
     return g;
+}
+
+__device__ __forceinline__ Geom load_geom_tab(const int4* __restrict__ rec, const float4* s_gtab, int e) {
+    return geom_from_rec(__ldg(&rec[e]), s_gtab);
 }
 
 // Copies the type table into shared memory (kernels launched with 48 * ngeom bytes of dynamic shared
@@ -961,6 +965,9 @@ extern "C" int lb_transport_inv_noalloc(lb_handle* hh, float* psi) {
     if (h->device < 0) return fail(h, LB_ERR_STATE, "host-only handle: no device attached");
     if (!h->mesh_ready || !h->angle_ready || h->sigt.empty())
         return fail(h, LB_ERR_STATE, "TransportOp%MatInv was called, but the operator was not ready.");
+    // the sweep reads and writes the four nodes of an element as one 16-byte vector
+    if (reinterpret_cast<uintptr_t>(psi) % 16 != 0)
+        return fail(h, LB_ERR_ARG, "lb_transport_inv_noalloc: psi must be 16-byte aligned");
     if (h->total_levels > kNoAllocMaxLevels) {
         char buf[200];
         std::snprintf(buf, sizeof buf,

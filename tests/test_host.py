@@ -187,3 +187,20 @@ def test_nan_cross_section_rejected():
     st = np.array([np.nan])
     ss = np.zeros((1, 2))
     assert hh.lib.lb_set_xs(hh.h, 1, _lib.dptr(st), _lib.dptr(ss)) == _lib.LB_ERR_NAN
+
+
+def test_element_type_table():
+    """Box meshes have 6 element shapes (the Kuhn split) per material, so the sweep reads 16-byte
+    records and a per-type table; a jittered mesh has a shape per element and keeps 64-byte records."""
+    n = np.zeros(1, np.int32)
+    hh = HostHandle()
+    assert hh.lib.lb_mesh_types(hh.h, _lib.iptr(n)) == _lib.LB_ERR_STATE
+    assert hh.mesh(M.box_mesh(4, 4, 4)) == 0
+    assert hh.lib.lb_mesh_types(hh.h, _lib.iptr(n)) == 0 and n[0] == 6
+    two = M.box_mesh(4, 4, 8, (0, 0, 0), (2, 2, 4), material=lambda c: (c[:, 2] > 2.0).astype(np.int32), Nm=2)
+    assert hh.mesh(two) == 0
+    assert hh.lib.lb_mesh_types(hh.h, _lib.iptr(n)) == 0 and n[0] == 12
+    jit = jittered(M.box_mesh(6, 5, 4, (0, 0, 0), (3.0, 2.5, 2.0)), 0.07)
+    assert jit.NE > 256
+    assert hh.mesh(jit) == 0
+    assert hh.lib.lb_mesh_types(hh.h, _lib.iptr(n)) == 0 and n[0] == 0

@@ -14,6 +14,7 @@ import pytest
 
 from helpers import rel_l2
 from lionbolt_b200 import AngularClass, TransportOp, XSType
+from lionbolt_b200 import _lib
 from lionbolt_b200 import problems as P
 
 pytestmark = pytest.mark.gpu
@@ -38,3 +39,8 @@ def test_noalloc_sweep_matches_regular_entry_point_twice():
         assert st == 0, f"call {call}: status {st}"
         out = dev.cpu().numpy().astype(np.float64)
         assert rel_l2(out, ref) < TOL, f"call {call}"
+    # a vector that is not 16-byte aligned is refused before anything is launched
+    assert lib.lb_transport_inv_noalloc(h, ctypes.c_void_p(dev.data_ptr() + 4)) == _lib.LB_ERR_ARG
+    buf = ctypes.create_string_buffer(256)
+    lib.lb_last_error(h, buf, 256)
+    assert b"aligned" in buf.value
