@@ -192,10 +192,13 @@ class Handle:
         st = self.lib.lb_get_sweep_config(self.h, iptr(cfg))
         if st != LB_OK:
             return None
-        names = ("levels", "dataflow", "levels+prefetch", "element flags", "grouped directions")
+        names = ("levels", "dataflow", "levels+prefetch", "element flags", "grouped directions", "cluster levels")
         kind = int(cfg[0])
-        return dict(schedule=names[kind] if 0 <= kind < len(names) else str(kind), threads=int(cfg[1]),
-                    dirs_per_cta=int(cfg[2]), ilp=int(cfg[3]))
+        d = dict(schedule=names[kind] if 0 <= kind < len(names) else str(kind), threads=int(cfg[1]),
+                 dirs_per_cta=int(cfg[2]), ilp=int(cfg[3]))
+        if kind == 5:
+            d.pop("dirs_per_cta")
+        return d
 
     def mesh_types(self):
         n = np.zeros(1, dtype=np.int32)

@@ -122,7 +122,7 @@ static int dev_upload(Handle* h, T** p, const T* src, size_t count, const char* 
 }
 
 static void free_all(Handle* h) {
-    void* ptrs[] = {h->d_geom, h->d_rec, h->d_gtab, h->d_tmat, h->d_mat, h->d_items, h->d_groups, h->d_pitems, h->d_pbase, h->d_chunks, h->d_lvl_start, h->d_lvl_base, h->d_nlev, h->d_done, h->d_status, h->d_dirs, h->d_sigt,
+    void* ptrs[] = {h->d_geom, h->d_rec, h->d_crec, h->d_cl_start, h->d_cl_base, h->d_ncl, h->d_gtab, h->d_tmat, h->d_mat, h->d_items, h->d_groups, h->d_pitems, h->d_pbase, h->d_chunks, h->d_lvl_start, h->d_lvl_base, h->d_nlev, h->d_done, h->d_status, h->d_dirs, h->d_sigt,
                     h->d_psi, h->d_qext, h->d_Ym2d, h->d_Yd2m, h->d_sigl, h->d_lofj, h->d_V, h->d_Z, h->d_x,
                     h->d_b, h->d_t, h->d_red, h->d_unc, h->d_phi_all, h->d_src, h->d_dose, h->d_flux,
                     h->d_sigl_mg, h->d_yb, h->d_dd};
@@ -452,6 +452,133 @@ int lb_set_mesh(lb_handle* h, int NE, int NN, const double* rg, const int* node,
     return LB_OK;
 }
 
+// Cluster schedule (sweep_cluster_kernel): blocks of kClusterSize consecutive elements (a hex of a
+// box mesh split into 6 tets is one block) are swept as units, one thread per block taking its
+// elements in level order, so a block's sources and solutions (96 contiguous bytes) are read and
+// written together.  Per direction the block graph (block B depends on block A when an element of B
+// has an upstream neighbour in A) must be acyclic; its longest-path levels order the blocks, and
+// blocks with the same element order and face masks are adjacent inside a level.  Record of a block:
+//   x: block index;  y, z, w: two 16-bit slots each, in execution order: element offset in the
+//   block (3 b, 7 = empty) | upstream-face mask << 3 | outflow-face mask << 7.
+// Built on device handles; when some direction's block graph has a cycle no cluster schedule is
+// kept and the sweep uses the element schedules.
+static int build_cluster_schedule(Handle* h) {
+    constexpr int K = kClusterSize;
+    h->nclusters = 0;
+    h->max_cluster_levels = 0;
+    for (void** p : {(void**)&h->d_crec, (void**)&h->d_cl_start, (void**)&h->d_cl_base, (void**)&h->d_ncl})
+        if (*p) {
+            cudaFree(*p);
+            *p = nullptr;
+        }
+    const int NE = h->NE, NI = h->NI;
+    if (h->device < 0 || NE < K) return LB_OK;
+    const int NC = (NE + K - 1) / K;
+    std::vector<int4> crec((size_t)NI * NC);
+    std::vector<std::vector<int>> cstart(NI);
+    bool cyclic = false;
+#pragma omp parallel reduction(|| : cyclic)
+    {
+        std::vector<int> lev(NE), indeg(NC), ostart(NC + 1), odst, fill(NC), cur, nxt, members, ord;
+        std::vector<uint16_t> fld(NE);
+        std::vector<unsigned long long> key;
+        std::vector<int4> tmp;
+#pragma omp for schedule(dynamic, 1)
+        for (int i = 0; i < NI; ++i) {
+            if (cyclic) continue;
+            const int* it = &h->items[(size_t)i * NE];
+            const int* st = &h->lvl_start[h->lvl_base[i]];
+            for (int L = 0; L < h->nlev[i]; ++L)
+                for (int es = st[L]; es < st[L + 1]; ++es) lev[it[es] & 0xFFFFFF] = L;
+            for (int es = 0; es < NE; ++es) {
+                const int e = it[es] & 0xFFFFFF;
+                fld[e] = (uint16_t)((e % K) | (((it[es] >> 24) & 0xF) << 3) | (((it[es] >> 28) & 0xF) << 7));
+            }
+            // block edges A -> B, one per cross-block upstream face (duplicates are harmless)
+            std::fill(ostart.begin(), ostart.end(), 0);
+            std::fill(indeg.begin(), indeg.end(), 0);
+            for (int e = 0; e < NE; ++e) {
+                const int upm = (fld[e] >> 3) & 0xF;
+                for (int f = 0; f < 4; ++f)
+                    if ((upm >> f) & 1) {
+                        const int a = h->nbr[(size_t)e * 4 + f] / K, b = e / K;
+                        if (a != b) {
+                            ++ostart[a + 1];
+                            ++indeg[b];
+                        }
+                    }
+            }
+            for (int c = 0; c < NC; ++c) ostart[c + 1] += ostart[c];
+            odst.resize(ostart[NC]);
+            for (int c = 0; c < NC; ++c) fill[c] = ostart[c];
+            for (int e = 0; e < NE; ++e) {
+                const int upm = (fld[e] >> 3) & 0xF;
+                for (int f = 0; f < 4; ++f)
+                    if ((upm >> f) & 1) {
+                        const int a = h->nbr[(size_t)e * 4 + f] / K, b = e / K;
+                        if (a != b) odst[fill[a]++] = b;
+                    }
+            }
+            // longest-path levels (Kahn, level by level)
+            cur.clear();
+            for (int c = 0; c < NC; ++c)
+                if (indeg[c] == 0) cur.push_back(c);
+            int4* out = crec.data() + (size_t)i * NC;
+            int pos = 0;
+            cstart[i].clear();
+            while (!cur.empty()) {
+                cstart[i].push_back(pos);
+                const int n = (int)cur.size();
+                tmp.resize(n);
+                key.resize(n);
+                for (int q = 0; q < n; ++q) {
+                    const int c = cur[q];
+                    members.clear();
+                    for (int e = c * K; e < std::min(NE, c * K + K); ++e) members.push_back(e);
+                    std::sort(members.begin(), members.end(),
+                              [&](int x, int y) { return lev[x] != lev[y] ? lev[x] < lev[y] : x < y; });
+                    uint32_t sl[6];
+                    for (int k = 0; k < 6; ++k) sl[k] = k < (int)members.size() ? fld[members[k]] : 7u;
+                    tmp[q] = make_int4(c, (int)(sl[0] | (sl[1] << 16)), (int)(sl[2] | (sl[3] << 16)),
+                                       (int)(sl[4] | (sl[5] << 16)));
+                    key[q] = ((unsigned long long)(uint32_t)tmp[q].y * 0x9E3779B97F4A7C15ull) ^
+                             ((unsigned long long)(uint32_t)tmp[q].z << 21) ^ (uint32_t)tmp[q].w;
+                }
+                // blocks with equal patterns next to each other (a warp then runs one element sequence)
+                ord.resize(n);
+                for (int q = 0; q < n; ++q) ord[q] = q;
+                std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return key[x] < key[y]; });
+                for (int q = 0; q < n; ++q) out[pos + q] = tmp[ord[q]];
+                pos += n;
+                nxt.clear();
+                for (int c : cur)
+                    for (int j = ostart[c]; j < ostart[c + 1]; ++j)
+                        if (--indeg[odst[j]] == 0) nxt.push_back(odst[j]);
+                cur.swap(nxt);
+            }
+            cstart[i].push_back(pos);
+            if (pos != NC) cyclic = true;
+        }
+    }
+    if (cyclic) return LB_OK;
+    std::vector<int> cl_start, cl_base(NI), ncl(NI);
+    int maxl = 0;
+    for (int i = 0; i < NI; ++i) {
+        cl_base[i] = (int)cl_start.size();
+        ncl[i] = (int)cstart[i].size() - 1;
+        maxl = std::max(maxl, ncl[i]);
+        cl_start.insert(cl_start.end(), cstart[i].begin(), cstart[i].end());
+    }
+    int rc = dev_upload(h, &h->d_crec, crec.data(), crec.size(), "upload cluster records");
+    if (!rc) rc = dev_upload(h, &h->d_cl_start, cl_start.data(), cl_start.size(), "upload cluster levels");
+    if (!rc) rc = dev_upload(h, &h->d_cl_base, cl_base.data(), cl_base.size(), "upload cluster level offsets");
+    if (!rc) rc = dev_upload(h, &h->d_ncl, ncl.data(), ncl.size(), "upload cluster level counts");
+    if (rc) return rc;
+    h->nclusters = NC;
+    h->max_cluster_levels = maxl;
+    return LB_OK;
+}
+
 int lb_set_quadrature(lb_handle* h, int NI, const double* k, const double* w) {
     if (!h) return LB_ERR_ARG;
     if (!h->mesh_ready) return fail(h, LB_ERR_STATE, "lb_set_quadrature: mesh not set");
@@ -527,6 +654,8 @@ int lb_set_quadrature(lb_handle* h, int NI, const double* k, const double* w) {
         }
     }
     int rc = dev_upload(h, &h->d_items, exec_items.data(), exec_items.size(), "upload sweep items");
+    if (rc) return rc;
+    rc = build_cluster_schedule(h);
     if (rc) return rc;
     rc = dev_upload(h, &h->d_chunks, chunks.data(), chunks.size(), "upload sweep chunks");
     if (rc) return rc;

@@ -9,6 +9,9 @@
 
 namespace lb {
 
+// elements per block of the cluster sweep schedule (a hex of a box mesh split into 6 tets)
+constexpr int kClusterSize = 6;
+
 // Packed schedule item (one per element-direction, in sweep order):
 //   bits 0-23 element id, bits 24-27 upstream-face mask, bits 28-31 outflow-face mask.
 constexpr int kElemBits = 24;
@@ -92,6 +95,13 @@ struct Handle {
     float4* d_gtab = nullptr;      // [ngeom][3] (snx, sny, snz)
     int* d_tmat = nullptr;         // [ngeom] material of each type
     int ngeom = 0;                 // number of types; 0: no table (use d_geom)
+    // cluster schedule: blocks of kClusterSize consecutive elements swept as units (0 blocks: none)
+    int4* d_crec = nullptr;        // [NI][nclusters] block records in block-level order
+    int* d_cl_start = nullptr;     // block-level starts, per direction (ncl[i] + 1 entries)
+    int* d_cl_base = nullptr;      // [NI] offset of direction i's starts in d_cl_start
+    int* d_ncl = nullptr;          // [NI] block levels per direction
+    int nclusters = 0;
+    int max_cluster_levels = 0;
     int* d_mat = nullptr;          // [NE]
     int* d_items = nullptr;        // [NI][NE]
     int4* d_chunks = nullptr;      // [nchunks]

@@ -58,10 +58,10 @@ def test_transport_inverse_matches_oracle(case):
     assert T.timers()["sweep"][1] >= 1
 
 
-@pytest.mark.parametrize("cfg", range(14))
+@pytest.mark.parametrize("cfg", range(16))
 def test_every_sweep_schedule_matches_oracle(cfg, monkeypatch):
     """Each launch candidate of the sweep autotuner (levels, prefetching levels, element flags,
-    grouped directions, dataflow) reproduces the oracle's T^{-1} on a two-material mesh."""
+    grouped directions, dataflow, cluster levels) reproduces the oracle's T^{-1} on a two-material mesh."""
     monkeypatch.setenv("LB_SWEEP_CONFIG", str(cfg))
     m, (k, w), sigt, sigs = SWEEP_CASES["two_material"]()
     o, ang, xs = _pair(m, k, w, sigt, sigs)
@@ -71,6 +71,36 @@ def test_every_sweep_schedule_matches_oracle(cfg, monkeypatch):
     out = q.copy()
     T.MatInv(out)
     assert rel_l2(out, ref) < TOL
+
+
+CLUSTER_CONFIGS = range(14, 16)   # launch candidates of the cluster schedule
+
+
+def _sweep_case(m, k, w, sigt, seed):
+    o, ang, xs = _pair(m, k, w, sigt, np.zeros((sigt.size, 1)))
+    T = TransportOp().Build(m, ang, xs)
+    q = np.random.default_rng(seed).uniform(0.0, 1.0, size=m.NENK * k.shape[0])
+    out = q.copy()
+    T.MatInv(out)
+    assert rel_l2(out, o.transport_inv(q)) < TOL
+    return T
+
+
+@pytest.mark.parametrize("cfg", CLUSTER_CONFIGS)
+def test_cluster_schedule_wide_levels_and_cyclic_blocks(cfg, monkeypatch):
+    """The cluster schedule (6-tet blocks swept as units) against the oracle on a two-material
+    32^3-hex box whose block levels (over a thousand blocks) take several passes of a CTA, and on a
+    jittered mesh whose block graphs have cycles in some directions, where the launcher runs the
+    plain level kernel instead."""
+    monkeypatch.setenv("LB_SWEEP_CONFIG", str(cfg))
+    k, w = P.quadrature(2, 4)
+    two = M.box_mesh(32, 32, 32, (0, 0, 0), (4, 4, 4), material=lambda c: (c[:, 0] > 2.5).astype(np.int32), Nm=2)
+    T = _sweep_case(two, k, w, np.array([0.3, 1.1]), cfg)
+    assert T._h.mesh_types() == 12
+    assert T._h.sweep_config()["schedule"] == "cluster levels"
+    m, (k, w), sigt, sigs = SWEEP_CASES["jittered"]()
+    T = _sweep_case(m, k, w, sigt, cfg + 20)
+    assert T._h.sweep_config()["schedule"] == "levels"
 
 
 def test_transport_mms_matches_oracle():
