@@ -159,14 +159,18 @@ __device__ __forceinline__ void bar_arrive(uint64_t* bar) {
 // One CTA per SM, warp-specialised, directions [half*NH, half*NH + NH) of every tile it takes:
 //   warps 0-7   producers: threads t and t + 128 read node tile*128 + (t & 127), half of its moments
 //               each, split them into BF16 planes and write the A buffer (two buffers);
-//   warps 8-15  epilogue: warps 8+e and 12+e read TMEM lanes 32e.. (the tile's nodes), half of the
-//               direction columns each, and write q rows (two accumulators);
-//   warp 16     lane 0 issues the MMAs; the warp owns the TMEM allocation.
+//   warps 8-19  epilogue: warps 8+e, 12+e and 16+e read TMEM lanes 32e.. (the tile's nodes), a third
+//               of the direction columns each, and write q rows (two accumulators);
+//   warp 20     lane 0 issues the MMAs; the warp owns the TMEM allocation.
 // Barriers per buffer b: full[b] (producers -> MMA), done[b] (MMA commit -> producers, epilogue),
 // empty[b] (epilogue -> MMA).  The k-th use of a buffer waits on phase parity k & 1.
 // ---------------------------------------------------------------------------------------------
+constexpr int kM2dEpi = 12;                          // epilogue warps (three per TMEM lane quarter)
+constexpr int kM2dMma = 8 + kM2dEpi;                 // the MMA warp
+constexpr int kM2dThreads = 32 * (kM2dMma + 1);
+
 template <int KT>
-__global__ void __launch_bounds__(544, 1) m2d_tc_kernel(const int* __restrict__ active, const double* __restrict__ x,
+__global__ void __launch_bounds__(kM2dThreads, 1) m2d_tc_kernel(const int* __restrict__ active, const double* __restrict__ x,
                                                       const float* __restrict__ sigl, const double* __restrict__ add,
                                                       const float* __restrict__ qadd, const int* __restrict__ mat,
                                                       const __nv_bfloat16* __restrict__ Y, float* __restrict__ q,
@@ -191,9 +195,9 @@ __global__ void __launch_bounds__(544, 1) m2d_tc_kernel(const int* __restrict__ 
         for (int k = 0; k < 2; ++k) {
             bar_init(&full[k], 256);
             bar_init(&done[k], 1);
-            bar_init(&empty[k], 256);
+            bar_init(&empty[k], 32 * kM2dEpi);
         }
-    if (warp == 16) tmem_alloc(tslot, 512);
+    if (warp == kM2dMma) tmem_alloc(tslot, 512);
     fence_async_smem();
     tc_before_sync();
     __syncthreads();
@@ -247,11 +251,11 @@ __global__ void __launch_bounds__(544, 1) m2d_tc_kernel(const int* __restrict__ 
             fence_async_smem();
             bar_arrive(&full[b]);
         }
-    } else if (warp < 16) {
-        // ---- epilogue: warps w and w + 4 share TMEM lanes 32(w%4).. and split the columns ----
+    } else if (warp < kM2dMma) {
+        // ---- epilogue: warps w, w + 4 and w + 8 share TMEM lanes 32(w%4).. and split the columns ----
         const int e = warp - 8;
         const int r = (e & 3) * 32 + (tid & 31);
-        const int ngr = NH / 16, per = (ngr + 1) / 2;
+        const int ngr = NH / 16, per = (ngr + kM2dEpi / 4 - 1) / (kM2dEpi / 4);
         const int g0 = (e >> 2) * per, g1 = min(ngr, g0 + per);
         const uint32_t lane_base = tmem + ((uint32_t)((e & 3) * 32) << 16);
         int it = 0;
@@ -304,7 +308,7 @@ __global__ void __launch_bounds__(544, 1) m2d_tc_kernel(const int* __restrict__ 
     }
     tc_before_sync();
     __syncthreads();
-    if (warp == 16) tmem_free(tmem, 512);
+    if (warp == kM2dMma) tmem_free(tmem, 512);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -526,7 +530,7 @@ int launch_m2d_tc(Handle* h, const double* x, const float* sigl, const double* a
     long long grid = std::min<long long>(ntiles * nhalves, (long long)h->sm_count);
     grid = std::max<long long>(nhalves, grid / nhalves * nhalves);
 #define LB_M2DTC(K)                                                                                                \
-    m2d_tc_kernel<K><<<(int)grid, 544, smem, h->stream>>>(h->d_active, x, sigl, a, qadd, h->d_mat, h->d_Ym2d, q,   \
+    m2d_tc_kernel<K><<<(int)grid, kM2dThreads, smem, h->stream>>>(h->d_active, x, sigl, a, qadd, h->d_mat, h->d_Ym2d, q,   \
                                                            h->NENK, h->NI, h->NIpad, h->nm, h->nmpad, NH, nhalves, \
                                                            ntiles, err)
     switch (h->nmpad / 16) {
