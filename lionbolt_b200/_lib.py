@@ -197,7 +197,7 @@ class Handle:
         d = dict(schedule=names[kind] if 0 <= kind < len(names) else str(kind), threads=int(cfg[1]),
                  dirs_per_cta=int(cfg[2]), ilp=int(cfg[3]))
         if kind == 5:
-            d.pop("dirs_per_cta")
+            d["min_ctas_per_sm"] = d.pop("dirs_per_cta")
         return d
 
     def mesh_types(self):

@@ -315,16 +315,21 @@ __global__ void __launch_bounds__(kM2dThreads, 1) m2d_tc_kernel(const int* __res
 // D2M: z[j][n] = sum_i Dw[j][i] psi[i][n];  out = alpha * xin + beta * z.  KT = nmpad / 16.
 // One CTA per SM, warp-specialised; psi streams in K chunks of 48 directions through a ring of
 // kStages A buffers:
-//   warps 0-7   producers: threads t and t + 128 share node tile*128 + (t & 127), each loads and
-//               splits 24 directions of the chunk;
-//   warps 8-11  epilogue (TMEM lanes 32(w%4)..): out rows of the tile (two accumulators);
-//   warp 12     lane 0 issues the MMAs; the warp owns the TMEM allocation.
+//   warps 0..8S-1  producers, S = kD2mSets sets of 8 warps taking alternate chunks (S chunks of loads
+//               in flight): threads t and t + 128 of a set share node tile*128 + (t & 127), each loads
+//               and splits 24 directions of the chunk;
+//   next 4 warps  epilogue (TMEM lanes 32(w%4)..): out rows of the tile (two accumulators);
+//   last warp   lane 0 issues the MMAs; the warp owns the TMEM allocation.
 // ---------------------------------------------------------------------------------------------
 constexpr int kKC = 48;       // directions per K chunk (3 MMA K-steps)
 constexpr int kStages = 3;    // A ring depth
+constexpr int kD2mSets = 2;                     // producer sets of 8 warps, taking alternate chunks
+constexpr int kD2mEpi = 8 * kD2mSets;           // first of the 4 epilogue warps
+constexpr int kD2mMma = kD2mEpi + 4;            // the MMA warp
+constexpr int kD2mThreads = 32 * (kD2mMma + 1);
 
 template <int KT>
-__global__ void __launch_bounds__(416, 1) d2m_tc_kernel(const int* __restrict__ active, const float* __restrict__ psi,
+__global__ void __launch_bounds__(kD2mThreads, 1) d2m_tc_kernel(const int* __restrict__ active, const float* __restrict__ psi,
                                                       const __nv_bfloat16* __restrict__ Dw, const double* xin,
                                                       double alpha, double beta, double* out, long long NENK, int NI,
                                                       int NIpad, int nm, int nmpad, long long ntiles, int* err) {
@@ -364,65 +369,61 @@ __global__ void __launch_bounds__(416, 1) d2m_tc_kernel(const int* __restrict__ 
             bar_init(&dempty[k], 128);
         }
     }
-    if (warp == 12) tmem_alloc(tslot, 128);
+    if (warp == kD2mMma) tmem_alloc(tslot, 128);
     fence_async_smem();
     tc_before_sync();
     __syncthreads();
     tc_after_sync();
     const uint32_t tmem = *tslot;
     const int nchunks = NKpad / kKC;
-    if (warp < 8) {
-        // ---- producers ----
-        const int row = tid & 127, side = tid >> 7;
-        long long c = 0;   // chunk sequence number of this CTA
-        bool ok = true;
-        for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    if (warp < kD2mEpi) {
+        // ---- producers: set `set` takes the CTA's chunks c with c % kD2mSets == set ----
+        const int set = warp >> 3;
+        const int row = tid & 127, side = (tid >> 7) & 1;
+        const long long my_tiles = (ntiles - 1 - (long long)blockIdx.x) / gridDim.x + 1;
+        for (long long c = set; c < my_tiles * nchunks; c += kD2mSets) {
+            const long long tile = blockIdx.x + (c / nchunks) * gridDim.x;
+            const int ch = (int)(c % nchunks);
             const long long n = tile * kTM + row;
             const bool valid = n < NENK;
-            for (int ch = 0; ch < nchunks; ++ch, ++c) {
-                const int s = (int)(c % kStages);
-                const uint32_t u = (uint32_t)(c / kStages);
-                float v[24];
+            const int s = (int)(c % kStages);
+            const uint32_t u = (uint32_t)(c / kStages);
+            float v[24];
 #pragma unroll
-                for (int k = 0; k < 24; ++k) {
-                    const int i = ch * kKC + side * 24 + k;
-                    v[k] = (valid && i < NI) ? __ldcs(&psi[(size_t)i * NENK + n]) : 0.f;
-                }
-                if (u > 0 && !bar_wait(&done[s], (u - 1) & 1u, err)) {
-                    ok = false;
-                    break;
-                }
-                unsigned char* A = sA + s * abuf;
-#pragma unroll
-                for (int cl = 0; cl < 3; ++cl) {
-                    float w[8];
-#pragma unroll
-                    for (int k = 0; k < 8; ++k) w[k] = v[cl * 8 + k];
-                    uint4 hi, mid, lo;
-                    split8(w, hi, mid, lo);
-                    unsigned char* rp = A + (size_t)(side * 3 + cl) * kTM * 16 + (size_t)row * 16;
-                    *reinterpret_cast<uint4*>(rp) = hi;
-                    *reinterpret_cast<uint4*>(rp + aplane) = mid;
-                    *reinterpret_cast<uint4*>(rp + 2 * aplane) = lo;
-                }
-                fence_async_smem();
-                bar_arrive(&full[s]);
+            for (int k = 0; k < 24; ++k) {
+                const int i = ch * kKC + side * 24 + k;
+                v[k] = (valid && i < NI) ? __ldcs(&psi[(size_t)i * NENK + n]) : 0.f;
             }
+            if (u > 0 && !bar_wait(&done[s], (u - 1) & 1u, err)) break;
+            unsigned char* A = sA + s * abuf;
+#pragma unroll
+            for (int cl = 0; cl < 3; ++cl) {
+                float w[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) w[k] = v[cl * 8 + k];
+                uint4 hi, mid, lo;
+                split8(w, hi, mid, lo);
+                unsigned char* rp = A + (size_t)(side * 3 + cl) * kTM * 16 + (size_t)row * 16;
+                *reinterpret_cast<uint4*>(rp) = hi;
+                *reinterpret_cast<uint4*>(rp + aplane) = mid;
+                *reinterpret_cast<uint4*>(rp + 2 * aplane) = lo;
+            }
+            fence_async_smem();
+            bar_arrive(&full[s]);
         }
-    } else if (warp < 12) {
-        // ---- epilogue ----
-        const int r = tid - 256;
+    } else if (warp < kD2mMma) {
+        // ---- epilogue (TMEM lanes 32(w%4)..): out rows of the tile, 16 moments at a time ----
+        const int r = tid - 32 * kD2mEpi;
         const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-        constexpr int NMP = KT * 16;
         int it = 0;
         for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
             const int b = it & 1;
             const uint32_t u = (uint32_t)(it >> 1);
             const long long n = tile * kTM + r;
             const bool valid = n < NENK;
-            double xv[NMP];
+            double xv[16];
 #pragma unroll
-            for (int j = 0; j < NMP; ++j) xv[j] = (xin && valid && j < nm) ? xin[(size_t)j * NENK + n] : 0.0;
+            for (int k = 0; k < 16; ++k) xv[k] = (xin && valid && k < nm) ? xin[(size_t)k * NENK + n] : 0.0;
             if (!bar_wait(&dfull[b], u & 1u, err)) break;
             tc_after_sync();
 #pragma unroll
@@ -433,7 +434,15 @@ __global__ void __launch_bounds__(416, 1) d2m_tc_kernel(const int* __restrict__ 
 #pragma unroll
                     for (int k = 0; k < 16; ++k) {
                         const int j = g * 16 + k;
-                        if (j < nm) out[(size_t)j * NENK + n] = beta * (double)v[k] + alpha * xv[j];
+                        if (j < nm) out[(size_t)j * NENK + n] = beta * (double)v[k] + alpha * xv[k];
+                    }
+                }
+                // the next group's inputs
+                if (g + 1 < KT) {
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) {
+                        const int j = (g + 1) * 16 + k;
+                        xv[k] = (xin && valid && j < nm) ? xin[(size_t)j * NENK + n] : 0.0;
                     }
                 }
             }
@@ -475,7 +484,7 @@ __global__ void __launch_bounds__(416, 1) d2m_tc_kernel(const int* __restrict__ 
     }
     tc_before_sync();
     __syncthreads();
-    if (warp == 12) tmem_free(tmem, 128);
+    if (warp == kD2mMma) tmem_free(tmem, 128);
 }
 
 size_t m2d_tc_smem(int NH, int nmpad) {
@@ -562,7 +571,7 @@ int launch_d2m_tc(Handle* h, const float* psi, const double* xin, double alpha, 
     const long long ntiles = (h->NENK + kTM - 1) / kTM;
     const long long grid = std::min<long long>(ntiles, (long long)h->sm_count);
 #define LB_D2MTC(K)                                                                                         \
-    d2m_tc_kernel<K><<<(int)grid, 416, smem, h->stream>>>(h->d_active, psi, h->d_Yd2m, xin, alpha, beta, out, \
+    d2m_tc_kernel<K><<<(int)grid, kD2mThreads, smem, h->stream>>>(h->d_active, psi, h->d_Yd2m, xin, alpha, beta, out, \
                                                            h->NENK, h->NI, h->NIpad, h->nm, h->nmpad, ntiles, err)
     switch (h->nmpad / 16) {
         case 1: LB_D2MTC(1); break;

@@ -373,7 +373,8 @@ __global__ void __launch_bounds__(1024, MINB) sweep_levels_pf_kernel(SweepArgs a
 // has about a third as many block levels as element levels.  The element update is the level
 // kernel's, so the results are bit-identical.
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024, 1) sweep_cluster_kernel(SweepArgs a) {
+template <int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) sweep_cluster_kernel(SweepArgs a) {
     __shared__ float s_sigt[256];
     extern __shared__ float4 s_gtab_dyn[];
     load_sigt(a, s_sigt);
@@ -715,14 +716,14 @@ struct Config {
     int kind;      // 0 levels, 1 dataflow, 2 levels with next-level prefetch, 3 element flags, 4 grouped levels,
                    // 5 blocks of elements (cluster records)
     int threads;
-    int dpc;       // directions per CTA (kind 0); minimum CTAs per SM (kind 2)
+    int dpc;       // directions per CTA (kind 0); minimum CTAs per SM (kinds 2, 5)
     int ilp;
 };
 
 const Config kConfigs[] = {
     {4, 1024, 2, 1}, {4, 512, 2, 1}, {4, 512, 3, 1}, {4, 1024, 3, 1}, {4, 512, 6, 1},
     {0, 1024, 1, 1}, {0, 512, 1, 1}, {2, 1024, 1, 1}, {3, 512, 0, 1}, {1, 256, 0, 0},
-    {4, 768, 2, 1}, {0, 1024, 1, 2}, {0, 1024, 1, 3}, {0, 768, 1, 3}, {5, 1024, 0, 1}, {5, 512, 0, 1},
+    {4, 768, 2, 1}, {0, 1024, 1, 2}, {0, 1024, 1, 3}, {0, 768, 1, 3}, {5, 1024, 1, 1}, {5, 512, 2, 1}, {5, 768, 2, 1}, {5, 1024, 2, 1},
 };
 constexpr int kNumConfigs = sizeof(kConfigs) / sizeof(kConfigs[0]);
 
@@ -795,13 +796,14 @@ cudaError_t launch_flags(const SweepArgs& a, int sm_count, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_cluster(const SweepArgs& a, int threads, int sm_count, cudaStream_t s) {
+template <int NT, int MINB>
+cudaError_t launch_cluster(const SweepArgs& a, int sm_count, cudaStream_t s) {
     const size_t smem = sizeof(float4) * 3 * (size_t)a.ngeom;
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_cluster_kernel, threads, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_cluster_kernel<NT, MINB>, NT, smem);
     if (per_sm < 1) per_sm = 1;
     int grid = std::min(a.NI, sm_count * per_sm);
-    sweep_cluster_kernel<<<grid, threads, smem, s>>>(a);
+    sweep_cluster_kernel<NT, MINB><<<grid, NT, smem, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -902,7 +904,10 @@ int launch_sweep(Handle* h, float* psi) {
         cudaFuncGetAttributes(&fa, sweep_levels_kernel<2, 2>);
         cudaFuncGetAttributes(&fa, sweep_dataflow_kernel);
         cudaFuncGetAttributes(&fa, sweep_group_kernel<2, 768>);
-        cudaFuncGetAttributes(&fa, sweep_cluster_kernel);
+        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<1024, 1>);
+        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<1024, 2>);
+        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<768, 2>);
+        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2>);
     }
     Config cfg = kConfigs[cfg_idx];
     // the element-flag schedule keeps one bit per element in shared memory
@@ -937,7 +942,10 @@ int launch_sweep(Handle* h, float* psi) {
           : (cfg.threads == 1024) ? launch_flags<1024>(a, h->sm_count, h->stream)
                                   : launch_flags<512>(a, h->sm_count, h->stream);
     } else if (cfg.kind == 5) {
-        e = launch_cluster(a, cfg.threads, h->sm_count, h->stream);
+        if (cfg.threads == 1024) e = cfg.dpc == 2 ? launch_cluster<1024, 2>(a, h->sm_count, h->stream)
+                                                  : launch_cluster<1024, 1>(a, h->sm_count, h->stream);
+        else if (cfg.threads == 768) e = launch_cluster<768, 2>(a, h->sm_count, h->stream);
+        else e = launch_cluster<512, 2>(a, h->sm_count, h->stream);
     } else if (cfg.kind == 2) {
         e = (cfg.dpc == 2) ? launch_levels_pf<2>(a, cfg.threads, h->sm_count, h->stream)
                            : launch_levels_pf<1>(a, cfg.threads, h->sm_count, h->stream);

@@ -58,7 +58,7 @@ def test_transport_inverse_matches_oracle(case):
     assert T.timers()["sweep"][1] >= 1
 
 
-@pytest.mark.parametrize("cfg", range(16))
+@pytest.mark.parametrize("cfg", range(18))
 def test_every_sweep_schedule_matches_oracle(cfg, monkeypatch):
     """Each launch candidate of the sweep autotuner (levels, prefetching levels, element flags,
     grouped directions, dataflow, cluster levels) reproduces the oracle's T^{-1} on a two-material mesh."""
@@ -73,7 +73,7 @@ def test_every_sweep_schedule_matches_oracle(cfg, monkeypatch):
     assert rel_l2(out, ref) < TOL
 
 
-CLUSTER_CONFIGS = range(14, 16)   # launch candidates of the cluster schedule
+CLUSTER_CONFIGS = range(14, 18)   # launch candidates of the cluster schedule
 
 
 def _sweep_case(m, k, w, sigt, seed):
