@@ -287,6 +287,12 @@ def real_sh(Ls, dirs):
     return Y
 
 
+# kernel of each sweep schedule the autotuner can pick
+SWEEP_KERNELS = {"cluster levels": "sweep_cluster_kernel", "levels": "sweep_levels_kernel",
+                 "levels+prefetch": "sweep_levels_pf_kernel", "element flags": "sweep_flags_kernel",
+                 "grouped directions": "sweep_group_kernel", "dataflow": "sweep_dataflow_kernel"}
+
+
 def run_gemm(args):
     """Standalone scattering contractions (config2 shapes): M2D psi[288][3,072,000] = Y[288][36]
     phi[36][3,072,000] and D2M phi = (wY)^T psi, on the device.  Split-BF16 tensor-core kernels vs
@@ -515,13 +521,16 @@ def run_ours(args):
     per_sweep_ms = sw_ms / max(sw_n, 1)
     achieved = by[0] / (per_sweep_ms / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
+    launch = h.sweep_config() or {}
+    kernel = SWEEP_KERNELS.get(launch.get("schedule"), "sweep")
     traffic = None
     tp = os.path.join(ROOT, "profiles", "sweep_dram_traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
             d = json.load(f)
-        # dram bytes of one captured sweep, scaled by the update count of this workload
-        traffic = d["dram_bytes"] * (up[0] / d["updates"])
+        # dram bytes of one captured sweep of the same kernel, scaled by the update count of this workload
+        if d.get("kernel") == kernel:
+            traffic = d["dram_bytes"] * (up[0] / d["updates"])
 
     # ---- end-to-end through the C ABI with pinned host buffers ----
     NENK, G = prob.mesh.NENK, prob.G
@@ -571,9 +580,9 @@ def run_ours(args):
                 "updates_per_s": float(up[0]) * (sum(int(x) for x in iters) + 2 * G) / (ms_per_step / 1e3),
                 "phase_ms_per_step": {k: v[0] / args.steps for k, v in tm.items()},
                 "sweep": {"ms": per_sweep_ms, "gbs": achieved, "updates_per_s": up[0] / (per_sweep_ms / 1e3),
-                          "launch": h.sweep_config()},
+                          "launch": launch},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak, "traffic": traffic, "kernel": "sweep_levels_kernel",
+                             "frac": achieved / peak, "traffic": traffic, "kernel": kernel,
                              "peak_source": peak_kind},
                 "gpu_launches": launches,
                 "clocks": clocks.summary(),
