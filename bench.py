@@ -288,7 +288,8 @@ def real_sh(Ls, dirs):
 
 
 # kernel of each sweep schedule the autotuner can pick
-SWEEP_KERNELS = {"cluster levels": "sweep_cluster_kernel", "levels": "sweep_levels_kernel",
+SWEEP_KERNELS = {"cluster levels": "sweep_cluster_kernel", "cluster levels+type tables": "sweep_cluster_kernel",
+                 "levels": "sweep_levels_kernel",
                  "levels+prefetch": "sweep_levels_pf_kernel", "element flags": "sweep_flags_kernel",
                  "grouped directions": "sweep_group_kernel", "dataflow": "sweep_dataflow_kernel"}
 

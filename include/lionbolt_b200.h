@@ -169,7 +169,8 @@ int lb_sweep_stats(lb_handle* h, double* bytes_per_sweep, double* updates_per_sw
 int lb_synchronize(lb_handle* h);
 /* Sweep launch shape picked by the autotuner: cfg[0] schedule (0 levels, 1 dataflow, 2 levels with
  * next-level prefetch, 3 element flags, 4 grouped directions, 5 blocks of 6 elements swept as
- * units), cfg[1] threads per CTA, cfg[2] directions per CTA, cfg[3] updates in flight per thread.  Returns
+ * units, 6 the same with per-type element tables), cfg[1] threads per CTA, cfg[2] directions per CTA
+ * (minimum CTAs per SM for 5 and 6), cfg[3] updates in flight per thread.  Returns
  * LB_ERR_STATE while candidates are still being timed (the first sweeps of a handle). */
 int lb_get_sweep_config(lb_handle* h, int* cfg);
 

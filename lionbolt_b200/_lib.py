@@ -192,11 +192,12 @@ class Handle:
         st = self.lib.lb_get_sweep_config(self.h, iptr(cfg))
         if st != LB_OK:
             return None
-        names = ("levels", "dataflow", "levels+prefetch", "element flags", "grouped directions", "cluster levels")
+        names = ("levels", "dataflow", "levels+prefetch", "element flags", "grouped directions", "cluster levels",
+                 "cluster levels+type tables")
         kind = int(cfg[0])
         d = dict(schedule=names[kind] if 0 <= kind < len(names) else str(kind), threads=int(cfg[1]),
                  dirs_per_cta=int(cfg[2]), ilp=int(cfg[3]))
-        if kind == 5:
+        if kind in (5, 6):
             d["min_ctas_per_sm"] = d.pop("dirs_per_cta")
         return d
 

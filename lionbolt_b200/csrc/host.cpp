@@ -729,6 +729,7 @@ int lb_set_quadrature(lb_handle* h, int NI, const double* k, const double* w) {
     h->sweep_cfg = -1;
     h->sweep_trial = 0;
     h->sweep_trial_ms.clear();
+    h->sweep_finalists.clear();
     std::vector<float4> dirs(NI);
     for (int i = 0; i < NI; ++i)
         dirs[i] = make_float4((float)k[i * 3], (float)k[i * 3 + 1], (float)k[i * 3 + 2], (float)w[i]);

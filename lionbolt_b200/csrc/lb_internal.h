@@ -167,6 +167,7 @@ struct Handle {
     int sweep_cfg = -1;            // index into the candidate table, -1 = still tuning
     int sweep_trial = 0;
     std::vector<float> sweep_trial_ms;
+    std::vector<int> sweep_finalists;   // candidates of the second timing round
     int sweep_cfg_forced = -1;     // set through LB_SWEEP_CONFIG for experiments
 
     cudaEvent_t marks[16] = {};

@@ -58,7 +58,7 @@ def test_transport_inverse_matches_oracle(case):
     assert T.timers()["sweep"][1] >= 1
 
 
-@pytest.mark.parametrize("cfg", range(18))
+@pytest.mark.parametrize("cfg", range(20))
 def test_every_sweep_schedule_matches_oracle(cfg, monkeypatch):
     """Each launch candidate of the sweep autotuner (levels, prefetching levels, element flags,
     grouped directions, dataflow, cluster levels) reproduces the oracle's T^{-1} on a two-material mesh."""
@@ -73,7 +73,7 @@ def test_every_sweep_schedule_matches_oracle(cfg, monkeypatch):
     assert rel_l2(out, ref) < TOL
 
 
-CLUSTER_CONFIGS = range(14, 18)   # launch candidates of the cluster schedule
+CLUSTER_CONFIGS = range(14, 20)   # launch candidates of the cluster schedule (plain, type tables)
 
 
 def _sweep_case(m, k, w, sigt, seed):
@@ -97,7 +97,7 @@ def test_cluster_schedule_wide_levels_and_cyclic_blocks(cfg, monkeypatch):
     two = M.box_mesh(32, 32, 32, (0, 0, 0), (4, 4, 4), material=lambda c: (c[:, 0] > 2.5).astype(np.int32), Nm=2)
     T = _sweep_case(two, k, w, np.array([0.3, 1.1]), cfg)
     assert T._h.mesh_types() == 12
-    assert T._h.sweep_config()["schedule"] == "cluster levels"
+    assert T._h.sweep_config()["schedule"].startswith("cluster levels")
     m, (k, w), sigt, sigs = SWEEP_CASES["jittered"]()
     T = _sweep_case(m, k, w, sigt, cfg + 20)
     assert T._h.sweep_config()["schedule"] == "levels"
