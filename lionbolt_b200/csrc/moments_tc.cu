@@ -276,7 +276,9 @@ __global__ void __launch_bounds__(kM2dThreads, 1) m2d_tc_kernel(const int* __res
                         if (i < NI) {
                             float o = v[k];
                             if (qadd) o += qadd[(size_t)i * NENK + n];
-                            __stcs(&q[(size_t)i * NENK + n], o);
+                            // plain (write-back) stores: the tile's 512-byte row pieces stay in L2 until
+                            // the neighbouring tiles' pieces join them (evict-first stores: 5 % slower)
+                            q[(size_t)i * NENK + n] = o;
                         }
                     }
                 }
