@@ -94,9 +94,24 @@ int build_work(lb_batch* b, const std::vector<int>& ids, int threads) {
             x.Nm = h->Nm;
             x.problem = p;
             double c = 0.0;
-            for (int L = 0; L < h->nlev[i]; ++L) {
-                const int sz = h->lvl_start[h->lvl_base[i] + L + 1] - h->lvl_start[h->lvl_base[i] + L];
-                c += 1.0 + std::ceil((double)sz / threads);
+            if (h->nclusters > 0) {
+                // block schedule: block levels, one thread per block of kClusterSize elements
+                x.crec = h->d_crec + (size_t)i * h->nclusters;
+                x.cl_start = h->d_cl_start + h->cl_base_h[i];
+                x.ncl = h->ncl_h[i];
+                if (h->ngeom > 0) {
+                    x.ngeom = h->ngeom;
+                    x.rec = h->d_rec;
+                    x.gtab = h->d_gtab;
+                    x.tmat = h->d_tmat;
+                }
+                const int* st = &h->cl_start_h[h->cl_base_h[i]];
+                for (int L = 0; L < x.ncl; ++L) c += 1.0 + kClusterSize * std::ceil((double)(st[L + 1] - st[L]) / threads);
+            } else {
+                for (int L = 0; L < h->nlev[i]; ++L) {
+                    const int sz = h->lvl_start[h->lvl_base[i] + L + 1] - h->lvl_start[h->lvl_base[i] + L];
+                    c += 1.0 + std::ceil((double)sz / threads);
+                }
             }
             w.push_back(x);
             cost.push_back(c);

@@ -466,6 +466,9 @@ static int build_cluster_schedule(Handle* h) {
     constexpr int K = kClusterSize;
     h->nclusters = 0;
     h->max_cluster_levels = 0;
+    h->cl_start_h.clear();
+    h->cl_base_h.clear();
+    h->ncl_h.clear();
     for (void** p : {(void**)&h->d_crec, (void**)&h->d_cl_start, (void**)&h->d_cl_base, (void**)&h->d_ncl})
         if (*p) {
             cudaFree(*p);
@@ -576,6 +579,9 @@ static int build_cluster_schedule(Handle* h) {
     if (rc) return rc;
     h->nclusters = NC;
     h->max_cluster_levels = maxl;
+    h->cl_start_h = cl_start;
+    h->cl_base_h = cl_base;
+    h->ncl_h = ncl;
     return LB_OK;
 }
 

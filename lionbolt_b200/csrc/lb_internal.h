@@ -102,6 +102,7 @@ struct Handle {
     int* d_ncl = nullptr;          // [NI] block levels per direction
     int nclusters = 0;
     int max_cluster_levels = 0;
+    std::vector<int> cl_start_h, cl_base_h, ncl_h;   // host copies of d_cl_start, d_cl_base, d_ncl
     int* d_mat = nullptr;          // [NE]
     int* d_items = nullptr;        // [NI][NE]
     int4* d_chunks = nullptr;      // [nchunks]
@@ -235,7 +236,14 @@ struct BatchWork {
     int nlev;
     int Nm;
     int problem;
-    int pad;
+    int ngeom;              // element types of the problem (0: no type table)
+    const int4* crec;       // the direction's block records (nullptr: element schedule)
+    const int* cl_start;    // [ncl + 1] block-level starts of the direction
+    const int4* rec;        // the problem's 16-byte element records (type table)
+    const float4* gtab;     // [ngeom][3] face vectors of the types
+    const int* tmat;        // [ngeom] material of the types
+    int ncl;
+    int pad[3];
 };
 // Sweeps every work item whose problem has active[problem] != 0, CTAs claiming items in order from
 // *counter (reset before the launch).  threads: 1024 or 512.

@@ -531,7 +531,9 @@ __global__ void __launch_bounds__(NT, MINB) sweep_cluster_kernel(SweepArgs a) {
 
 // ---------------------------------------------------------------------------------------------
 // Batched level schedule: one persistent launch over the directions of many independent problems
-// (meshes, quadratures and cross sections differ).  CTAs claim work items in order from a global
+// (meshes, quadratures and cross sections differ).  A direction whose problem has a block schedule is
+// walked block level by block level, as the cluster kernel does, with the problem's element types
+// staged in shared memory.  CTAs claim work items in order from a global
 // counter, so items sorted by decreasing cost give a longest-first list schedule; each item is a
 // whole direction walked level by level with a CTA barrier between levels, exactly like the
 // single-problem level kernel (same element update, bit-identical results).
@@ -540,6 +542,7 @@ template <int NT>
 __global__ void __launch_bounds__(NT) sweep_batch_kernel(const BatchWork* __restrict__ work, int nwork, int* counter,
                                                         const int* __restrict__ active) {
     __shared__ float s_sigt[256];
+    __shared__ float4 s_gt[3 * 256];   // the item's element types (face vectors), when it has a type table
     __shared__ int s_w;
     for (;;) {
         if (threadIdx.x == 0) s_w = atomicAdd(counter, 1);
@@ -554,7 +557,16 @@ __global__ void __launch_bounds__(NT) sweep_batch_kernel(const BatchWork* __rest
         }
         const int Nm = __ldg(&W->Nm);
         const float* sg = W->sigt;
-        for (int m = threadIdx.x; m < 256; m += NT) s_sigt[m] = (m < Nm) ? __ldg(&sg[m]) : 0.f;
+        const int ngeom = __ldg(&W->ngeom);
+        const int4* crec = W->crec;
+        // cross sections by material, or by element type when the problem has a type table
+        for (int m = threadIdx.x; m < 256; m += NT) {
+            float v = 0.f;
+            if (ngeom > 0) v = (m < ngeom) ? __ldg(&sg[__ldg(&W->tmat[m])]) : 0.f;
+            else v = (m < Nm) ? __ldg(&sg[m]) : 0.f;
+            s_sigt[m] = v;
+        }
+        for (int k = threadIdx.x; k < 3 * ngeom; k += NT) s_gt[k] = __ldg(&W->gtab[k]);
         const int nl = __ldg(&W->nlev);
         const int* ls = W->lvl_start;
         const int* it = W->items;
@@ -562,6 +574,36 @@ __global__ void __launch_bounds__(NT) sweep_batch_kernel(const BatchWork* __rest
         float* base = W->psi;
         const float4 dir = __ldg(&W->dir);
         __syncthreads();
+        if (crec) {
+            // block schedule, as sweep_cluster_kernel
+            const int ncl = __ldg(&W->ncl);
+            const int* cls = W->cl_start;
+            const int4* rec = W->rec;
+            for (int L = 0; L < ncl; ++L) {
+                const int s0 = __ldg(&cls[L]), s1 = __ldg(&cls[L + 1]);
+                for (int cs = s0 + threadIdx.x; cs < s1; cs += NT) {
+                    const int4 r = __ldcs(crec + cs);
+                    const int e0 = r.x * kClusterSize;
+                    unsigned long long pk = (unsigned long long)(unsigned)r.y | ((unsigned long long)(unsigned)r.z << 32);
+                    unsigned pw = (unsigned)r.w;
+#pragma unroll 1
+                    for (int k = 0; k < kClusterSize; ++k) {
+                        const unsigned f = (unsigned)(pk & 0xFFFFu);
+                        pk = (pk >> 16) | ((unsigned long long)(pw & 0xFFFFu) << 48);
+                        pw >>= 16;
+                        if ((f & 7u) == 7u) break;
+                        const int e = e0 + (int)(f & 7u);
+                        const int item = e | (int)(((f >> 3) & 0xFu) << 24) | (int)(((f >> 7) & 0xFu) << 28);
+                        const Geom g = ngeom > 0 ? load_geom_tab(rec, s_gt, e) : load_geom(geom, e);
+                        Update up;
+                        assemble_g<false>(base, dir, item, g, s_sigt, up, make_float4(0.f, 0.f, 0.f, 0.f));
+                        finish<false>(base, item, up);
+                    }
+                }
+                __syncthreads();
+            }
+            continue;
+        }
         for (int L = 0; L < nl; ++L) {
             const int s0 = __ldg(&ls[L]), s1 = __ldg(&ls[L + 1]);
             for (int es = s0 + threadIdx.x; es < s1; es += NT) {
