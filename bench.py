@@ -404,9 +404,13 @@ def run_batch(args):
     torch.cuda.synchronize()
     ms, it = [], None
     with ClockSampler(local) as clocks:
+        if args.profile_range:
+            torch.cuda.profiler.start()
         for _ in range(args.steps):
             it = bs.solve(m=args.m, rtol=args.rtol)
             ms.append(bs.info()["last_ms"])
+        if args.profile_range:
+            torch.cuda.profiler.stop()
     info = bs.info()
     t = float(np.sum(ms))
     NE = np.array([p.mesh.NE for p in probs])

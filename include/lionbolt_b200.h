@@ -179,6 +179,17 @@ int lb_get_sweep_config(lb_handle* h, int* cfg);
  * records).  No counterpart in the reference. */
 int lb_mesh_types(lb_handle* h, int* ntypes);
 
+/* Block schedule of the sweep (schedule 5): the mesh's elements in blocks of 6 consecutive ids (a hex of
+ * a box mesh split into 6 tets), swept as units over each direction's block-level graph.  Built by
+ * lb_set_quadrature when every direction's block graph is acyclic.  lb_cluster_info: *nblocks = number
+ * of blocks (0: no block schedule), *max_levels = largest block-level count of a direction.
+ * lb_get_cluster_schedule: rec[NI][nblocks][4] block records in execution order (x = block index;
+ * y, z, w = two 16-bit slots each in execution order: element offset in the block (3 b, 7 = empty),
+ * upstream-face mask << 3, outflow-face mask << 7), starts[NI][nblocks + 1] block-level starts,
+ * nlevels[NI].  Diagnostics for tests; no counterpart in the reference. */
+int lb_cluster_info(lb_handle* h, int* nblocks, int* max_levels);
+int lb_get_cluster_schedule(lb_handle* h, int* rec, int* starts, int* nlevels);
+
 
 /* ---- Learned right preconditioner (no counterpart in the reference) ------------------------------
  * A per-cell MLP (19 -> 64 -> 64 -> 16, ReLU, 6,480 parameters, BF16 weights and activations with

@@ -64,6 +64,8 @@ SIGNATURES = {
     "lb_synchronize": (ctypes.c_int, [_vp]),
     "lb_get_sweep_config": (ctypes.c_int, [_vp, _c_int_p]),
     "lb_mesh_types": (ctypes.c_int, [_vp, _c_int_p]),
+    "lb_cluster_info": (ctypes.c_int, [_vp, _c_int_p, _c_int_p]),
+    "lb_get_cluster_schedule": (ctypes.c_int, [_vp, _c_int_p, _c_int_p, _c_int_p]),
     "lb_mg_update_inputs": (ctypes.c_int, [_vp, _c_double_p, _c_double_p, _c_double_p, _c_double_p, _c_double_p]),
     "lb_mark": (ctypes.c_int, [_vp, ctypes.c_int]),
     "lb_transport_inv_noalloc": (ctypes.c_int, [_vp, ctypes.c_void_p]),

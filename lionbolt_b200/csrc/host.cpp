@@ -467,6 +467,7 @@ static int build_cluster_schedule(Handle* h) {
     h->nclusters = 0;
     h->max_cluster_levels = 0;
     h->cl_start_h.clear();
+    h->crec_h.clear();
     h->cl_base_h.clear();
     h->ncl_h.clear();
     for (void** p : {(void**)&h->d_crec, (void**)&h->d_cl_start, (void**)&h->d_cl_base, (void**)&h->d_ncl})
@@ -475,7 +476,7 @@ static int build_cluster_schedule(Handle* h) {
             *p = nullptr;
         }
     const int NE = h->NE, NI = h->NI;
-    if (h->device < 0 || NE < K) return LB_OK;
+    if (NE < K) return LB_OK;
     const int NC = (NE + K - 1) / K;
     std::vector<int4> crec((size_t)NI * NC);
     std::vector<std::vector<int>> cstart(NI);
@@ -581,6 +582,7 @@ static int build_cluster_schedule(Handle* h) {
     h->max_cluster_levels = maxl;
     h->cl_start_h = cl_start;
     h->cl_base_h = cl_base;
+    if (h->device < 0) h->crec_h = std::move(crec);   // host-only handles keep the records for queries
     h->ncl_h = ncl;
     return LB_OK;
 }
@@ -887,6 +889,33 @@ int lb_elapsed_ms(lb_handle* h, int a, int b, double* ms) {
 int lb_get_sweep_config(lb_handle* h, int* cfg) {
     if (!h || !cfg) return LB_ERR_ARG;
     if (sweep_config(h, &cfg[0], &cfg[1], &cfg[2], &cfg[3]) < 0) return LB_ERR_STATE;
+    return LB_OK;
+}
+
+int lb_cluster_info(lb_handle* h, int* nblocks, int* max_levels) {
+    if (!h || !nblocks || !max_levels) return LB_ERR_ARG;
+    if (!h->angle_ready) return fail(h, LB_ERR_STATE, "lb_cluster_info: quadrature not set");
+    *nblocks = h->nclusters;
+    *max_levels = h->max_cluster_levels;
+    return LB_OK;
+}
+
+int lb_get_cluster_schedule(lb_handle* h, int* rec, int* starts, int* nlevels) {
+    if (!h || !rec || !starts || !nlevels) return LB_ERR_ARG;
+    if (!h->angle_ready) return fail(h, LB_ERR_STATE, "lb_get_cluster_schedule: quadrature not set");
+    if (h->nclusters <= 0) return fail(h, LB_ERR_STATE, "lb_get_cluster_schedule: the mesh has no block schedule");
+    const size_t n = (size_t)h->NI * h->nclusters;
+    if (h->device < 0) {
+        std::memcpy(rec, h->crec_h.data(), sizeof(int4) * n);
+    } else {
+        cudaSetDevice(h->device);
+        cudaError_t e = cudaMemcpy(rec, h->d_crec, sizeof(int4) * n, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return cuda_fail(h, e, "lb_get_cluster_schedule");
+    }
+    for (int i = 0; i < h->NI; ++i) {
+        nlevels[i] = h->ncl_h[i];
+        for (int L = 0; L <= h->ncl_h[i]; ++L) starts[(size_t)i * (h->nclusters + 1) + L] = h->cl_start_h[h->cl_base_h[i] + L];
+    }
     return LB_OK;
 }
 

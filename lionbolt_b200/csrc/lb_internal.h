@@ -103,6 +103,7 @@ struct Handle {
     int nclusters = 0;
     int max_cluster_levels = 0;
     std::vector<int> cl_start_h, cl_base_h, ncl_h;   // host copies of d_cl_start, d_cl_base, d_ncl
+    std::vector<int4> crec_h;                        // the block records (host-only handles)
     int* d_mat = nullptr;          // [NE]
     int* d_items = nullptr;        // [NI][NE]
     int4* d_chunks = nullptr;      // [nchunks]

@@ -204,3 +204,64 @@ def test_element_type_table():
     assert jit.NE > 256
     assert hh.mesh(jit) == 0
     assert hh.lib.lb_mesh_types(hh.h, _lib.iptr(n)) == 0 and n[0] == 0
+
+
+def _cluster_schedule(hh, NE, NI):
+    nb, ml = np.zeros(1, np.int32), np.zeros(1, np.int32)
+    assert hh.lib.lb_cluster_info(hh.h, _lib.iptr(nb), _lib.iptr(ml)) == 0
+    if nb[0] == 0:
+        return 0, 0, None, None, None
+    rec = np.zeros((NI, nb[0], 4), np.int32)
+    st = np.zeros((NI, nb[0] + 1), np.int32)
+    nl = np.zeros(NI, np.int32)
+    assert hh.lib.lb_get_cluster_schedule(hh.h, _lib.iptr(rec), _lib.iptr(st), _lib.iptr(nl)) == 0
+    return int(nb[0]), int(ml[0]), rec, st, nl
+
+
+def test_cluster_schedule_respects_every_dependency():
+    """The block schedule (blocks of 6 consecutive tets swept as units) against the reference schedule:
+    every block once per direction, every element once with the reference's upstream mask, every
+    upstream neighbour in another block on an earlier block level and every upstream neighbour in the
+    same block in an earlier slot.  A box mesh has nx + ny + nz - 2 block levels in an oblique
+    direction; a jittered mesh has cyclic block graphs and no block schedule."""
+    m = P.config1_small(n=(6, 6, 12)).mesh
+    k, w = P.quadrature(6, 12)
+    hh = HostHandle()
+    assert hh.mesh(m) == 0 and hh.quad(k, w) == 0
+    NE, NI = m.NE, k.shape[0]
+    sl, up, nlev, ls = hh.schedule(NE, NI)
+    nb, ml, rec, st, nl = _cluster_schedule(hh, NE, NI)
+    assert nb == NE // 6 and ml == 6 + 6 + 12 - 2
+    nbr = m.neighbors
+    for i in range(NI):
+        upm = np.zeros(NE, np.int64)
+        upm[sl[i]] = up[i]
+        blk_level = np.empty(nb, np.int64)
+        for L in range(nl[i]):
+            blk_level[rec[i, st[i, L]:st[i, L + 1], 0]] = L
+        assert st[i, nl[i]] == nb and sorted(rec[i, :, 0]) == list(range(nb))
+        words = rec[i, :, 1:].astype(np.uint32)
+        slots = np.stack([words & 0xFFFF, words >> 16], axis=2).reshape(nb, 6)
+        off = slots & 7
+        seen = np.zeros(NE, np.int64)
+        slot_of = np.full(NE, -1, np.int64)
+        for b in range(nb):
+            e0 = rec[i, b, 0] * 6
+            for kk in range(6):
+                if off[b, kk] == 7:
+                    continue
+                e = e0 + int(off[b, kk])
+                seen[e] += 1
+                slot_of[e] = kk
+                assert ((slots[b, kk] >> 3) & 15) == upm[e]
+        assert np.all(seen == 1)
+        for f in range(4):
+            e = np.nonzero((upm >> f) & 1)[0]
+            ne = nbr[e, f]
+            other = ne // 6 != e // 6
+            assert np.all(blk_level[ne[other] // 6] < blk_level[e[other] // 6])
+            assert np.all(slot_of[ne[~other]] < slot_of[e[~other]])
+    jit = jittered(M.box_mesh(6, 5, 4, (0, 0, 0), (3.0, 2.5, 2.0)), 0.07)
+    hj = HostHandle()
+    assert hj.mesh(jit) == 0 and hj.quad(*P.quadrature(4, 8)) == 0
+    assert _cluster_schedule(hj, jit.NE, 32)[0] == 0
