@@ -15,14 +15,19 @@
 // per element.  T is a rank-2 update of a multiple of the identity, so the reference's pivoted LU
 // (LocalLU) becomes a 2x2 capacitance solve with the same FP32 accuracy.
 //
-// Two schedules share that element update:
-//  * levels (default): one CTA owns whole directions and walks their wavefront levels in order
-//    with a CTA barrier between levels.  No global synchronisation; upstream values written by the
-//    same SM are re-read through its L1.
-//  * dataflow: warps claim 32-element chunks of (direction, level) in level-major order from a
-//    global counter and wait, with a bounded spin, on the completion counter of the previous level.
-// Launch shape (schedule, threads per CTA, directions per CTA, updates in flight per thread) is
-// picked by timing the first sweeps of a handle; every candidate computes bit-identical results.
+// The schedules share that element update:
+//  * cluster levels: blocks of 6 consecutive elements (a hex of a box mesh split into 6 tets) are
+//    swept as units over each direction's block-level graph, one thread per block, a CTA barrier
+//    between block levels; optionally with the element matrices of every element type computed once
+//    per direction.  The fastest at the 768k-tet configuration.
+//  * levels: one CTA owns whole directions and walks their element wavefront levels in order with a
+//    CTA barrier between levels; upstream values written by the same SM are re-read through its L1.
+//  * levels with next-level prefetch, element flags in shared memory, grouped same-schedule
+//    directions, and dataflow (warps claim 32-element chunks from a global counter and wait, with a
+//    bounded spin, on the completion counter of the previous level): candidates for other meshes.
+// Launch shape (schedule, threads per CTA, directions or CTAs per SM, updates in flight per thread)
+// is picked by timing the first sweeps of a handle (the three fastest twice); every candidate
+// computes bit-identical results.
 #include "lb_internal.h"
 #include <algorithm>
 #include <cstdio>
