@@ -111,6 +111,37 @@ double cgs2_norm(double nrm0, double nrm1, const double* h2, int k, bool* reorth
     return hk2;
 }
 
+// Solves G c = hh for the k x k Gram matrix G of the Arnoldi basis (row stride ld) by Cholesky; G is
+// the identity up to the basis' loss of orthogonality.  Returns false (c untouched) if G is not
+// numerically positive definite.
+static bool gram_solve(const std::vector<double>& G, int ld, int k, const double* hh, double* c) {
+    std::vector<double> L((size_t)k * k, 0.0);
+    for (int j = 0; j < k; ++j) {
+        double d = G[(size_t)j * ld + j];
+        for (int p = 0; p < j; ++p) d -= L[(size_t)j * k + p] * L[(size_t)j * k + p];
+        if (!(d > 0.5)) return false;   // G = I + E with |E| << 1 for any usable basis
+        const double ljj = std::sqrt(d);
+        L[(size_t)j * k + j] = ljj;
+        for (int i = j + 1; i < k; ++i) {
+            double t = G[(size_t)i * ld + j];
+            for (int p = 0; p < j; ++p) t -= L[(size_t)i * k + p] * L[(size_t)j * k + p];
+            L[(size_t)i * k + j] = t / ljj;
+        }
+    }
+    std::vector<double> y(k);
+    for (int i = 0; i < k; ++i) {
+        double t = hh[i];
+        for (int p = 0; p < i; ++p) t -= L[(size_t)i * k + p] * y[p];
+        y[i] = t / L[(size_t)i * k + i];
+    }
+    for (int i = k - 1; i >= 0; --i) {
+        double t = y[i];
+        for (int p = i + 1; p < k; ++p) t -= L[(size_t)p * k + i] * c[p];
+        c[i] = t / L[(size_t)i * k + i];
+    }
+    return true;
+}
+
 // Restarted GMRES(m) / FGMRES(m) (right preconditioner `prec`), SPARSKIT semantics.
 static KrylovResult gmres_device(Handle* h, size_t n, const double* rhs, double* sol, int m, double rtol, double atol,
                                  int maxit, const DevOp& matvec, const DevOp* prec) {
@@ -119,7 +150,9 @@ static KrylovResult gmres_device(Handle* h, size_t n, const double* rhs, double*
     double* V = h->d_V;
     double* Z = h->d_Z;
     GmresHost gh(m);
-    std::vector<double> hh(m + 2), h2(m + 2), coef;
+    std::vector<double> hh(m + 2), h2(m + 2), cc(m + 2), coef;
+    const int ldg = m + 2;
+    std::vector<double> G((size_t)ldg * ldg, 0.0);   // Gram matrix V^T V of the current cycle's basis
     double rn = vnorm(h, rhs, n, &rc);
     if (rc) { res.status = rc; return res; }
     const double fpar4 = rtol * rn + atol;
@@ -137,6 +170,7 @@ static KrylovResult gmres_device(Handle* h, size_t n, const double* rhs, double*
         gh.start(alpha);
         if (alpha <= fpar4) { res.status = LB_OK; res.nmv = nmv; res.resid = alpha; return res; }
         k_scale(h, V, 1.0 / alpha, n);
+        G[0] = 1.0;
         int k = 0;
         bool breakdown = false;
         while (true) {
@@ -149,23 +183,20 @@ static KrylovResult gmres_device(Handle* h, size_t n, const double* rhs, double*
             double* vk = V + (size_t)k * n;
             if ((rc = matvec(vin, vk))) { res.status = rc; return res; }
             ++nmv;
-            // Classical Gram-Schmidt with one selective re-orthogonalisation, in three passes over
-            // V[0..k-1]:  (1) hh = V^T vk and |vk|^2;  (2) vk -= V hh, with h2 = V^T vk and |vk|^2 of
-            // the result in the same pass;  (3) either vk = (vk - V h2) / hk when |vk| dropped below
-            // |vk_0| / sqrt(2) (|vk - V h2|^2 = |vk|^2 - |h2|^2 for orthonormal V), or vk /= hk.
+            // Gram-corrected classical Gram-Schmidt in two passes over V[0..k-1]: (1) hh = V^T vk and
+            // |vk|^2;  (2) vk -= V c with G c = hh (G = V^T V, kept up to date from the dots of pass 2),
+            // with h2 = V^T vk and |vk|^2 of the result in the same pass;  then vk /= hk.  Then
+            // A v_{k-1} = V c + hk v_k holds exactly, hk is a measured norm, and the residual
+            // non-orthogonality h2 / hk enters G for the next steps (this replaces the second projection
+            // pass of classical Gram-Schmidt with re-orthogonalisation: 2k + 5 vector passes per step
+            // instead of 3k + 5).
             double nrm0 = 0.0, nrm1 = 0.0;
             if ((rc = k_dots_norm(h, V, n, k, vk, n, hh.data(), &nrm0))) { res.status = rc; return res; }
-            if ((rc = k_axpy_dots(h, vk, V, n, k, hh.data(), n, h2.data(), &nrm1))) { res.status = rc; return res; }
-            bool reorth = false;
-            double hk2 = cgs2_norm(nrm0, nrm1, h2.data(), k, &reorth);
-            if (reorth) {
-                for (int i = 0; i < k; ++i) hh[i] += h2[i];
-            } else if (hk2 < 0.0) {
-                // near breakdown: apply the correction and measure the norm exactly
-                if ((rc = k_axpy_dots(h, vk, V, n, k, h2.data(), n, nullptr, &hk2))) { res.status = rc; return res; }
-                for (int i = 0; i < k; ++i) hh[i] += h2[i];
-            }
-            const double hk = std::sqrt(std::max(0.0, hk2));
+            if (!gram_solve(G, ldg, k, hh.data(), cc.data()))
+                for (int i = 0; i < k; ++i) cc[i] = hh[i];
+            if ((rc = k_axpy_dots(h, vk, V, n, k, cc.data(), n, h2.data(), &nrm1))) { res.status = rc; return res; }
+            for (int i = 0; i < k; ++i) hh[i] = cc[i];
+            const double hk = std::sqrt(std::max(0.0, nrm1));
             if (std::isnan(hk)) { res.status = fail(h, LB_ERR_NAN, "RESIDUAL NORM is NaN."); return res; }
             if (!(hk > 0.0)) {
                 for (int i = 0; i < k; ++i) gh.H[k][i + 1] = hh[i];
@@ -174,7 +205,9 @@ static KrylovResult gmres_device(Handle* h, size_t n, const double* rhs, double*
                 --k;
                 break;
             }
-            if ((rc = k_axpy_scale(h, vk, V, n, reorth ? k : 0, h2.data(), 1.0 / hk, n))) { res.status = rc; return res; }
+            if ((rc = k_axpy_scale(h, vk, V, n, 0, h2.data(), 1.0 / hk, n))) { res.status = rc; return res; }
+            for (int i = 0; i < k; ++i) G[(size_t)i * ldg + k] = G[(size_t)k * ldg + i] = h2[i] / hk;
+            G[(size_t)k * ldg + k] = 1.0;
             alpha = gh.add_column(k, hh.data(), hk);
             fpar5 = alpha;
             if (k < m && !(alpha <= fpar4) && (maxit <= 0 || nmv < maxit)) continue;
