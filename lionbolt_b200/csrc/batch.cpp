@@ -229,7 +229,7 @@ struct PState {
     size_t n = 0;
     double* x = nullptr;   // solution (group flux moments)
     GmresHost gh;
-    std::vector<double> hh, h2, coef;
+    std::vector<double> hh, h2, coef, G;   // G: Gram matrix V^T V of the cycle's basis, (m + 2)^2
     double fpar4 = 0.0, fpar5 = 0.0, hk = 0.0, hk2 = 0.0;
     int nmv = 0, status = LB_OK, kk = 0;
     bool done = false, brk = false, reorth = false, cont = false;
@@ -261,6 +261,7 @@ int batch_gmres(lb_batch* b, const std::vector<int>& ids, int g, int m, double r
         st[q].gh.resize(m);
         st[q].hh.assign(m + 2, 0.0);
         st[q].h2.assign(m + 2, 0.0);
+        st[q].G.assign((size_t)(m + 2) * (m + 2), 0.0);
     }
     // graphs of this group step: residual (x -> V0), a -> b, b -> a
     free_graphs(b);
@@ -328,6 +329,7 @@ int batch_gmres(lb_batch* b, const std::vector<int>& ids, int g, int m, double r
             }
             s.fpar5 = alpha;
             s.gh.start(alpha);
+            s.G[0] = 1.0;
             if (alpha <= s.fpar4) {
                 s.status = LB_OK;
                 s.done = true;
@@ -361,44 +363,25 @@ int batch_gmres(lb_batch* b, const std::vector<int>& ids, int g, int m, double r
                 sg.push_back(seg(o, st[q].h->d_V, st[q].n, st[q].n));
             }
             seg_assign_blocks(sg, seg_grid(b));
-            // (1) projections and |w|^2
+            // Gram-corrected classical Gram-Schmidt, as gmres_device: (1) projections and |w|^2;
+            // G c = hh per problem; (2) w -= V c with h2 = V^T w and the exact |w|^2 in the same pass
             if ((rc = seg_dots_norm(ax, sg, k, out))) return bfail(b, rc, ax->err);
-            std::vector<double> nrm0(A.size()), coef;
+            const int ldg = m + 2;
+            std::vector<double> coef;
             for (size_t a = 0; a < A.size(); ++a) {
                 PState& s = st[A[a]];
-                for (int i = 0; i < k; ++i) s.hh[i] = out[a * (k + 1) + i];
-                nrm0[a] = out[a * (k + 1) + k];
+                std::vector<double> hraw(out.begin() + a * (k + 1), out.begin() + a * (k + 1) + k);
+                if (!gram_solve(s.G, ldg, k, hraw.data(), s.hh.data()))
+                    for (int i = 0; i < k; ++i) s.hh[i] = hraw[i];
                 coef.insert(coef.end(), s.hh.begin(), s.hh.begin() + k);
             }
             for (size_t a = 0; a < A.size(); ++a) sg[a].coef = (int)(a * k);
-            // (2) w -= V hh, second projections and |w|^2
             if ((rc = seg_axpy_dots(ax, sg, k, coef, true, out))) return bfail(b, rc, ax->err);
-            std::vector<size_t> exact;
             for (size_t a = 0; a < A.size(); ++a) {
                 PState& s = st[A[a]];
                 for (int i = 0; i < k; ++i) s.h2[i] = out[a * (k + 1) + i];
-                s.hk2 = cgs2_norm(nrm0[a], out[a * (k + 1) + k], s.h2.data(), k, &s.reorth);
-                if (s.reorth)
-                    for (int i = 0; i < k; ++i) s.hh[i] += s.h2[i];
-                else if (s.hk2 < 0.0)
-                    exact.push_back(a);
-            }
-            if (!exact.empty()) {   // near breakdown: apply the second projection, exact norm
-                std::vector<SegVec> se;
-                std::vector<double> ce;
-                for (size_t a : exact) {
-                    SegVec s = sg[a];
-                    s.coef = (int)ce.size();
-                    se.push_back(s);
-                    ce.insert(ce.end(), st[A[a]].h2.begin(), st[A[a]].h2.begin() + k);
-                }
-                seg_assign_blocks(se, seg_grid(b));
-                if ((rc = seg_axpy_dots(ax, se, k, ce, false, out))) return bfail(b, rc, ax->err);
-                for (size_t j = 0; j < exact.size(); ++j) {
-                    PState& s = st[A[exact[j]]];
-                    s.hk2 = out[j * (k + 1) + k];
-                    for (int i = 0; i < k; ++i) s.hh[i] += s.h2[i];
-                }
+                s.hk2 = out[a * (k + 1) + k];
+                s.reorth = false;
             }
             // (3) Hessenberg column, Givens rotation and the continue/leave decision
             std::vector<size_t> norm_re, norm_plain;
@@ -422,10 +405,15 @@ int batch_gmres(lb_batch* b, const std::vector<int>& ids, int g, int m, double r
                 s.fpar5 = alpha;
                 s.kk = k;
                 s.cont = k < m && !(alpha <= s.fpar4) && (maxit <= 0 || s.nmv < maxit);
-                if (s.cont) (s.reorth ? norm_re : norm_plain).push_back(a);
+                if (s.cont) {
+                    norm_plain.push_back(a);
+                    for (int i = 0; i < k; ++i)
+                        s.G[(size_t)i * ldg + k] = s.G[(size_t)k * ldg + i] = s.h2[i] / s.hk;
+                    s.G[(size_t)k * ldg + k] = 1.0;
+                }
             }
-            // normalise the continuing problems' new basis vector: v_k = (w - [V h2]) / hk, kept in
-            // the product buffer (next input) and stored in V
+            // normalise the continuing problems' new basis vector: v_k = w / hk, kept in the product
+            // buffer (next input) and stored in V
             for (int pass = 0; pass < 2; ++pass) {
                 const std::vector<size_t>& lst = pass == 0 ? norm_re : norm_plain;
                 if (lst.empty()) continue;

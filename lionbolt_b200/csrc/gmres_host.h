@@ -79,4 +79,35 @@ struct GmresHost {
     }
 };
 
+// Solves G c = hh for the k x k Gram matrix G of the Arnoldi basis (row stride ld) by Cholesky; G is
+// the identity up to the basis' loss of orthogonality.  Returns false (c untouched) if G is not
+// numerically positive definite.
+inline bool gram_solve(const std::vector<double>& G, int ld, int k, const double* hh, double* c) {
+    std::vector<double> L((size_t)k * k, 0.0);
+    for (int j = 0; j < k; ++j) {
+        double d = G[(size_t)j * ld + j];
+        for (int p = 0; p < j; ++p) d -= L[(size_t)j * k + p] * L[(size_t)j * k + p];
+        if (!(d > 0.5)) return false;   // G = I + E with |E| << 1 for any usable basis
+        const double ljj = std::sqrt(d);
+        L[(size_t)j * k + j] = ljj;
+        for (int i = j + 1; i < k; ++i) {
+            double t = G[(size_t)i * ld + j];
+            for (int p = 0; p < j; ++p) t -= L[(size_t)i * k + p] * L[(size_t)j * k + p];
+            L[(size_t)i * k + j] = t / ljj;
+        }
+    }
+    std::vector<double> y(k);
+    for (int i = 0; i < k; ++i) {
+        double t = hh[i];
+        for (int p = 0; p < i; ++p) t -= L[(size_t)i * k + p] * y[p];
+        y[i] = t / L[(size_t)i * k + i];
+    }
+    for (int i = k - 1; i >= 0; --i) {
+        double t = y[i];
+        for (int p = i + 1; p < k; ++p) t -= L[(size_t)p * k + i] * c[p];
+        c[i] = t / L[(size_t)i * k + i];
+    }
+    return true;
+}
+
 }  // namespace lb

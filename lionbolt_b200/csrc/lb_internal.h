@@ -213,10 +213,6 @@ inline void allow_max_dynamic_smem(K kernel) {
     cudaGetLastError();
 }
 
-// Squared norm of an Arnoldi vector after classical Gram-Schmidt with selective re-orthogonalisation
-// (solve.cpp); a negative value asks for an exact norm.
-double cgs2_norm(double nrm0, double nrm1, const double* h2, int k, bool* reorth);
-
 // Krylov workspace of a handle for restart length m (solve.cpp)
 int ensure_krylov(Handle* h, int m, bool flexible);
 // multigroup helpers (solve.cpp): transfer table sigma_l(j) of g' -> g, beam harmonics, and the

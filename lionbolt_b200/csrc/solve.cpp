@@ -96,52 +96,6 @@ struct KrylovResult {
 
 using DevOp = std::function<int(const double* in, double* out)>;
 
-// Squared norm of the Arnoldi vector after the second Gram-Schmidt pass.  nrm0 = |w|^2 before the
-// first projection, nrm1 = |w - V hh|^2, h2 = V^T (w - V hh).  When the first pass cancelled more
-// than half of |w|^2, the second pass is applied (*reorth = true) and |w - V hh - V h2|^2 =
-// nrm1 - |h2|^2 for orthonormal V; a negative return asks for an exact norm (near breakdown).
-double cgs2_norm(double nrm0, double nrm1, const double* h2, int k, bool* reorth) {
-    *reorth = false;
-    if (!(nrm1 < 0.5 * nrm0)) return nrm1;
-    double s2 = 0.0;
-    for (int i = 0; i < k; ++i) s2 += h2[i] * h2[i];
-    const double hk2 = nrm1 - s2;
-    if (!(hk2 > 1e-4 * nrm1)) return -1.0;
-    *reorth = true;
-    return hk2;
-}
-
-// Solves G c = hh for the k x k Gram matrix G of the Arnoldi basis (row stride ld) by Cholesky; G is
-// the identity up to the basis' loss of orthogonality.  Returns false (c untouched) if G is not
-// numerically positive definite.
-static bool gram_solve(const std::vector<double>& G, int ld, int k, const double* hh, double* c) {
-    std::vector<double> L((size_t)k * k, 0.0);
-    for (int j = 0; j < k; ++j) {
-        double d = G[(size_t)j * ld + j];
-        for (int p = 0; p < j; ++p) d -= L[(size_t)j * k + p] * L[(size_t)j * k + p];
-        if (!(d > 0.5)) return false;   // G = I + E with |E| << 1 for any usable basis
-        const double ljj = std::sqrt(d);
-        L[(size_t)j * k + j] = ljj;
-        for (int i = j + 1; i < k; ++i) {
-            double t = G[(size_t)i * ld + j];
-            for (int p = 0; p < j; ++p) t -= L[(size_t)i * k + p] * L[(size_t)j * k + p];
-            L[(size_t)i * k + j] = t / ljj;
-        }
-    }
-    std::vector<double> y(k);
-    for (int i = 0; i < k; ++i) {
-        double t = hh[i];
-        for (int p = 0; p < i; ++p) t -= L[(size_t)i * k + p] * y[p];
-        y[i] = t / L[(size_t)i * k + i];
-    }
-    for (int i = k - 1; i >= 0; --i) {
-        double t = y[i];
-        for (int p = i + 1; p < k; ++p) t -= L[(size_t)p * k + i] * c[p];
-        c[i] = t / L[(size_t)i * k + i];
-    }
-    return true;
-}
-
 // Restarted GMRES(m) / FGMRES(m) (right preconditioner `prec`), SPARSKIT semantics.
 static KrylovResult gmres_device(Handle* h, size_t n, const double* rhs, double* sol, int m, double rtol, double atol,
                                  int maxit, const DevOp& matvec, const DevOp* prec) {
