@@ -227,6 +227,8 @@ def test_cluster_schedule_respects_every_dependency():
     m = P.config1_small(n=(6, 6, 12)).mesh
     k, w = P.quadrature(6, 12)
     hh = HostHandle()
+    nb0, ml0 = np.zeros(1, np.int32), np.zeros(1, np.int32)
+    assert hh.lib.lb_cluster_info(hh.h, _lib.iptr(nb0), _lib.iptr(ml0)) == _lib.LB_ERR_STATE   # no quadrature yet
     assert hh.mesh(m) == 0 and hh.quad(k, w) == 0
     NE, NI = m.NE, k.shape[0]
     sl, up, nlev, ls = hh.schedule(NE, NI)
@@ -265,3 +267,5 @@ def test_cluster_schedule_respects_every_dependency():
     hj = HostHandle()
     assert hj.mesh(jit) == 0 and hj.quad(*P.quadrature(4, 8)) == 0
     assert _cluster_schedule(hj, jit.NE, 32)[0] == 0
+    one = np.zeros(4, np.int32)
+    assert hj.lib.lb_get_cluster_schedule(hj.h, _lib.iptr(one), _lib.iptr(one), _lib.iptr(one)) == _lib.LB_ERR_STATE
