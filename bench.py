@@ -221,7 +221,7 @@ def training_problem(args, k):
 
 def learned_comparison(args, mg, device, barrier, gmres_ms, gmres_dose):
     """Train the per-cell network on plain-solver data (untimed), then time FGMRES with it on the
-    benchmarked problem; the plain-GMRES dose judges its answer."""
+    benchmarked problem; the plain-GMRES dose checks its answer."""
     from lionbolt_b200 import MultigroupSolver
     t0 = time.perf_counter()
     tr = MultigroupSolver(device=device)

@@ -198,7 +198,7 @@ int lb_get_cluster_schedule(lb_handle* h, int* rec, int* starts, int* nlevels);
  * sigma_t*ell, sigma_s0*ell and sigma_s0/sigma_t (ell = 4V/S, the mean chord) and returns
  * z = v + s * net(x) on the cell's nodes for j < 16 (z = v for j >= 16).  Parameter layout (FP32):
  * W1[64][19], b1[64], W2[64][64], b2[64], W3[16][64], b3[16].  Without weights, or when disabled,
- * LB_SOLVER_FGMRES_ML runs plain GMRES; with weights the learned iterate is judged by its true
+ * LB_SOLVER_FGMRES_ML runs plain GMRES; with weights the learned iterate is checked by its true
  * residual and finished with plain GMRES when it misses the tolerance. */
 int lb_lp_nparams(void);
 /* He-uniform initialisation from `seed` (output layer scaled by 0.1); enables the network. */

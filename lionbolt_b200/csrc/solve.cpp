@@ -239,7 +239,7 @@ static KrylovResult moment_solve(Handle* h, const double* b, double* phi, int so
         if (kr.status == LB_ERR_NAN) {
             k_copy(h, phi, b, n);   // the learned iterate is unusable: restart from the first-flight moments
         } else {
-            // Plain-operator judge: the true residual ||b - A phi|| of the learned iterate.
+            // Plain-operator check: the true residual ||b - A phi|| of the learned iterate.
             if ((rc = apply_A(h, phi, h->d_t, sigl))) { kr.status = rc; return kr; }
             ++nmv;
             double rn = 0.0;

@@ -1049,7 +1049,7 @@ int launch_sweep(Handle* h, float* psi) {
     if (h->sweep_cfg_forced < kNumConfigs) cfg_idx = h->sweep_cfg_forced;
     else if (h->sweep_cfg >= 0) cfg_idx = h->sweep_cfg;
     else {
-        // round 1 times every candidate once; round 2 times the kFinalists fastest once more
+        // a first pass times every candidate once; a second pass times the kFinalists fastest once more
         cfg_idx = h->sweep_trial < kNumConfigs ? h->sweep_trial : h->sweep_finalists[h->sweep_trial - kNumConfigs];
         tuning = true;
     }

@@ -1,6 +1,6 @@
 """GPU tests of the learned right preconditioner: inference, preconditioner and training kernels
 against the NumPy reference (tests/mlp_ref.py), and FGMRES with the trained network against
-plain GMRES, which judges its answer.
+plain GMRES, which checks its answer.
 
 Tolerances: the network runs in BF16 with FP32 accumulation, so kernel-vs-reference comparisons
 allow for accumulation order (relative L2 2e-3 on outputs and gradients).  The solver with the
