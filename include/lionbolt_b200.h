@@ -3,8 +3,8 @@
  *
  * Drop-in boundary for Lionbolt's within-group transport solve.  The reference exposes this path
  * as Fortran type-bound procedures re-exported by src/LionboltAPI.f90:1-12; every entry point
- * below names the reference procedure it replaces.  A Fortran iso_c_binding interface for these
- * functions is given in INTEGRATION.md.
+ * below names the reference procedure it replaces.  A Fortran caller binds them with iso_c_binding
+ * interfaces (bind(C, name="lb_...")) whose arguments follow the C types below one for one.
  *
  * Conventions
  *   - Plain pointers and sizes only; all host arrays are C-contiguous, 0-based.
