@@ -102,11 +102,16 @@ CASES = {
     "two_material": lambda: (P.config1_small(n=(4, 4, 8)).mesh, P.quadrature(6, 12)),
     "jittered": lambda: (jittered(M.box_mesh(5, 4, 3, (0, 0, 0), (2.5, 2.0, 1.5)), 0.06), P.quadrature(4, 8)),
     "L11_288": lambda: (M.box_mesh(3, 3, 6, (0, 0, 0), (1.5, 1.5, 3.0)), P.quadrature(12, 24)),
+    # an unstructured gmsh mesh of the reference (read where the reference tree is present)
+    "gmsh_simple_cube": lambda: (M.read_gmsh(REF_CUBE), P.quadrature(4, 8)),
 }
+REF_CUBE = os.path.join(os.environ.get("LIONBOLT_REFERENCE", "/root/reference"), "validation/operators/simple_cube.msh")
 
 
 @pytest.mark.parametrize("case", sorted(CASES))
 def test_schedule_bitexact_vs_literal_sweep_order(case):
+    if case.startswith("gmsh") and not os.path.exists(REF_CUBE):
+        pytest.skip("the reference's mesh files are not present")
     m, (k, w) = CASES[case]()
     o = O.Oracle(m)
     assert o.set_angular(k, w, 0, literal=True) == 0
