@@ -36,10 +36,10 @@ enum lb_status {
     LB_ERR_OOM = 3,      /* device allocation failed                                          */
     LB_ERR_CYCLE = 4,    /* sweep ordering stagnated: cyclic dependency (SweepOrder.f90:178)  */
     LB_ERR_TIMEOUT = 5,  /* a bounded device-side dependency wait gave up                     */
-    LB_ERR_NOCONV = 6,   /* Krylov iteration limit reached (SPARSKIT.f90:241-244, ipar(1)=-1) */
-    LB_ERR_NAN = 7,      /* residual norm is NaN (SPARSKIT.f90:205-207)                       */
+    LB_ERR_NOCONV = 6,   /* Krylov iteration limit reached (SPARSKIT.f90:159-162, ipar(1)=-1) */
+    LB_ERR_NAN = 7,      /* residual norm is NaN (SPARSKIT.f90:123-124)                       */
     LB_ERR_STATE = 8,    /* operator not ready (TransportOperator.f90:87-88)                  */
-    LB_ERR_BREAKDOWN = 9 /* Krylov breakdown (SPARSKIT.f90:248-251, ipar(1)=-3)               */
+    LB_ERR_BREAKDOWN = 9 /* Krylov breakdown (SPARSKIT.f90:166-169, ipar(1)=-3)               */
 };
 
 enum lb_solver {
@@ -111,8 +111,11 @@ int lb_transport_inv(lb_handle* h, double* s);
  * device arrays, a loop that must not hit cudaMalloc's implicit synchronisation).  Its dependency
  * counters live in a fixed 1 MiB file-scope device array (at most 262,144 direction-level pairs;
  * larger schedules return LB_ERR_ARG) that every GPU loading the library keeps until exit.  The
- * first call on a device looks up the array's device address; make that first call before any
- * stream capture.  All calls on a device share the array: calls that overlap on the GPU race. */
+ * first call on a device looks up the array's device address.  The call runs the dataflow sweep
+ * schedule (not the autotuned one of lb_transport_inv) on the handle's stream and waits for it, so
+ * it cannot be stream-captured; writes to psi queued on other streams must be finished first (an
+ * event wait or a host synchronisation).  All calls on a device share the array: calls that
+ * overlap on the GPU race. */
 int lb_transport_inv_noalloc(lb_handle* h, float* psi);
 
 /* The two halves of K on caller-owned device arrays of the handle's GPU, asynchronous on the
@@ -164,7 +167,9 @@ int lb_elapsed_ms(lb_handle* h, int slot_a, int slot_b, double* ms);
 /* Device-time phase timers (ms) accumulated since the last reset, and kernel launch counts. */
 int lb_get_timers(lb_handle* h, double* ms, long long* launches);
 int lb_reset_timers(lb_handle* h);
-/* Algorithmic traffic of one full sweep (bytes) and its update count (NE*NI). */
+/* Algorithmic traffic of one full sweep and its update count (NE*NI): 16 B source read + 16 B
+ * solution write per update, 12 B per upstream face, and the element record (16 B with the type
+ * table, 64 B without) once per sweep; schedule records are not counted. */
 int lb_sweep_stats(lb_handle* h, double* bytes_per_sweep, double* updates_per_sweep, long long* upstream_faces);
 int lb_synchronize(lb_handle* h);
 /* Sweep launch shape picked by the autotuner: cfg[0] schedule (0 levels, 1 dataflow, 2 levels with
@@ -178,6 +183,10 @@ int lb_get_sweep_config(lb_handle* h, int* cfg);
  * (the sweep then reads 16-byte element records and a per-type table); 0 otherwise (64-byte
  * records).  No counterpart in the reference. */
 int lb_mesh_types(lb_handle* h, int* ntypes);
+
+/* SPARSKIT givens (third_party/SPARSKIT/iters.f:3225-3262) as the Krylov drivers apply it: the
+ * rotation (c, s) taking (x, y) to (r, 0); x or y NaN gives c = 1, s = 0, r = 0.  Diagnostic. */
+int lb_givens(double x, double y, double* c, double* s, double* r);
 
 /* Block schedule of the sweep (schedule 5): the mesh's elements in blocks of 6 consecutive ids (a hex of
  * a box mesh split into 6 tets), swept as units over each direction's block-level graph.  Built by

@@ -64,6 +64,7 @@ SIGNATURES = {
     "lb_synchronize": (ctypes.c_int, [_vp]),
     "lb_get_sweep_config": (ctypes.c_int, [_vp, _c_int_p]),
     "lb_mesh_types": (ctypes.c_int, [_vp, _c_int_p]),
+    "lb_givens": (ctypes.c_int, [ctypes.c_double, ctypes.c_double, _c_double_p, _c_double_p, _c_double_p]),
     "lb_cluster_info": (ctypes.c_int, [_vp, _c_int_p, _c_int_p]),
     "lb_get_cluster_schedule": (ctypes.c_int, [_vp, _c_int_p, _c_int_p, _c_int_p]),
     "lb_mg_update_inputs": (ctypes.c_int, [_vp, _c_double_p, _c_double_p, _c_double_p, _c_double_p, _c_double_p]),

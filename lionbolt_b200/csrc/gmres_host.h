@@ -7,6 +7,32 @@
 
 namespace lb {
 
+// Givens rotation of SPARSKIT givens (iters.f:3225-3262): c, s with (x, y) -> (r, 0); on return
+// x = r = |x_in * y'|.  When neither |y| > |x| nor |y| <= |x| holds (x or y is NaN) the rotation is
+// the identity and r = 0, as in the reference.
+inline void givens_rotation(double& x, double& y, double& c, double& s) {
+    if (x == 0.0 && y == 0.0) {
+        c = 1.0;
+        s = 0.0;
+    } else if (std::fabs(y) > std::fabs(x)) {
+        const double t = x / y;
+        x = std::sqrt(1.0 + t * t);
+        s = std::copysign(1.0 / x, y);
+        c = t * s;
+    } else if (std::fabs(y) <= std::fabs(x)) {
+        const double t = y / x;
+        y = std::sqrt(1.0 + t * t);
+        c = std::copysign(1.0 / y, x);
+        s = t * c;
+    } else {
+        x = 0.0;
+        y = 0.0;
+        c = 1.0;
+        s = 0.0;
+    }
+    x = std::fabs(x * y);
+}
+
 struct GmresHost {
     int m = 0;
     std::vector<std::vector<double>> H;   // H[col][row], 1-based rows as in SPARSKIT
@@ -37,21 +63,8 @@ struct GmresHost {
             H[k][i + 1] = c[i] * H[k][i + 1] - s[i] * a;
         }
         double x = H[k][k], y = H[k][k + 1], cc, ss;
-        if (x == 0.0 && y == 0.0) {
-            cc = 1.0;
-            ss = 0.0;
-        } else if (std::fabs(y) > std::fabs(x)) {
-            const double t = x / y;
-            x = std::sqrt(1.0 + t * t);
-            ss = std::copysign(1.0 / x, y);
-            cc = t * ss;
-        } else {
-            const double t = y / x;
-            y = std::sqrt(1.0 + t * t);
-            cc = std::copysign(1.0 / y, x);
-            ss = t * cc;
-        }
-        H[k][k] = std::fabs(x * y);
+        givens_rotation(x, y, cc, ss);
+        H[k][k] = x;
         H[k][k + 1] = 0.0;
         c[k] = cc;
         s[k] = ss;

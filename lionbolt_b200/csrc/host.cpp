@@ -3,6 +3,7 @@
 // C-ABI entry points.  Compiled with -ffp-contract=off: the FP64 face-orientation tests must
 // round exactly like the reference's DOT_PRODUCT so that the sweep levels are bit-identical.
 #include "lb_internal.h"
+#include "gmres_host.h"
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -856,10 +857,10 @@ int lb_reset_timers(lb_handle* h) {
 int lb_sweep_stats(lb_handle* h, double* bytes, double* updates, long long* upfaces) {
     if (!h || !h->angle_ready) return LB_ERR_STATE;
     double upd = (double)h->NE * h->NI;
-    // algorithmic bytes: q read (16 B) + psi write (16 B) + 3 FP32 face values per upstream face
-    // (12 B) per update, plus the packed schedule item (4 B) and one element record per pass (16 B with
-    // the type table, 64 B without)
-    double b = upd * (16.0 + 16.0 + 4.0) + 12.0 * (double)h->nz_upstream + (h->ngeom ? 16.0 : 64.0) * h->NE;
+    // algorithmic bytes of one sweep: per update the FP32 source read (16 B) and solution write
+    // (16 B), 3 FP32 face-node values per upstream face (12 B), and the compact element record once
+    // per sweep (16 B with the type table, 64 B without).  Schedule records are not counted.
+    double b = upd * (16.0 + 16.0) + 12.0 * (double)h->nz_upstream + (h->ngeom ? 16.0 : 64.0) * h->NE;
     if (bytes) *bytes = b;
     if (updates) *updates = upd;
     if (upfaces) *upfaces = h->nz_upstream;
@@ -916,6 +917,13 @@ int lb_get_cluster_schedule(lb_handle* h, int* rec, int* starts, int* nlevels) {
         nlevels[i] = h->ncl_h[i];
         for (int L = 0; L <= h->ncl_h[i]; ++L) starts[(size_t)i * (h->nclusters + 1) + L] = h->cl_start_h[h->cl_base_h[i] + L];
     }
+    return LB_OK;
+}
+
+int lb_givens(double x, double y, double* c, double* s, double* r) {
+    if (!c || !s || !r) return LB_ERR_ARG;
+    givens_rotation(x, y, *c, *s);
+    *r = x;
     return LB_OK;
 }
 

@@ -1222,6 +1222,11 @@ int sweep_config(Handle* h, int* kind, int* threads, int* dpc, int* ilp) {
 //  dataflow schedule's per-level completion counters and status word live in the file-scope array
 //  below instead of handle memory, so a call makes no cudaMalloc / cudaFree.
 //
+//  It always runs the dataflow schedule (sweep_dataflow_kernel), whose only scratch is these
+//  counters, not the schedule the autotuner picks for lb_transport_inv, so its timing differs.
+//  The call is synchronous on the handle's stream (it reads the status block back), so it cannot
+//  be stream-captured, and writes to psi issued on other streams must be complete before it.
+//
 //  Limits and sharing: the array holds kNoAllocMaxLevels (direction, level) counters (1 MiB); a
 //  problem with more levels is rejected.  Every GPU that loads this library keeps the array until
 //  the process exits.  All calls on a device share it and it keeps the last call's contents: the
@@ -1232,11 +1237,13 @@ namespace lb {
 namespace {
 
 constexpr int kNoAllocMaxLevels = 1 << 18;
-constexpr int kNoAllocStatusInts = 8;   // SweepStatus, padded
+constexpr int kNoAllocStatusInts = 16;  // the SweepStatus block, padded; the level counters follow it
+static_assert(sizeof(SweepStatus) <= kNoAllocStatusInts * sizeof(int), "status block overlaps the level counters");
 static __device__ __align__(256) int g_noalloc_scratch[kNoAllocStatusInts + kNoAllocMaxLevels];
 
 constexpr int kMaxDevices = 64;
 void* g_noalloc_ptr[kMaxDevices] = {};
+int g_noalloc_per_sm[kMaxDevices] = {};   // resident dataflow CTAs per SM, per device
 
 }  // namespace
 }  // namespace lb
@@ -1292,10 +1299,11 @@ extern "C" int lb_transport_inv_noalloc(lb_handle* hh, float* psi) {
     a.spin_limit = 1LL << 24;
     e = cudaMemsetAsync(base, 0, sizeof(int) * ((size_t)kNoAllocStatusInts + h->total_levels), h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "lb_transport_inv_noalloc: clear scratch");
-    static int per_sm = -1;
-    if (per_sm < 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_dataflow_kernel, 256, 0);
-        if (per_sm < 1) per_sm = 1;
+    int& per_sm = g_noalloc_per_sm[h->device];
+    if (per_sm < 1) {
+        int n = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_dataflow_kernel, 256, 0);
+        per_sm = n < 1 ? 1 : n;
     }
     sweep_dataflow_kernel<<<h->sm_count * per_sm, 256, 0, h->stream>>>(a);
     e = cudaGetLastError();

@@ -97,8 +97,9 @@ def read_gmsh(path):
     """Tetrahedral mesh from a gmsh MSH 4.1 ASCII file, as the reference reads it (ReadGMSH.f90:3-236
     with gmshprocessing.py): the nodes of $Nodes (indexed by tag); the 3-D elements of $Elements in
     block order (4-node tetrahedra only); the material of an element = the physical tag of its volume
-    entity in $Entities (no physical tag on every volume: one material; a volume with more than one
-    tag, or tags on only some volumes, is an error); neighbours by face matching.  Physical tags are
+    entity in $Entities (a volume without a physical tag is material 1, ReadGMSH.f90:119-139; a
+    volume with more than one tag, or untagged volumes next to a tag other than 1, is an error);
+    neighbours by face matching.  Physical tags are
     1-based in the file and 0-based in the returned mesh, and must not skip numbers."""
     sec = _sections(path)
     fmt = sec.get("MeshFormat", [""])[0].split()
@@ -109,15 +110,17 @@ def read_gmsh(path):
     if not ent:
         raise ValueError(f"{path}: no $Entities section")
     npts, ncur, nsur, nvol = (int(v) for v in ent[0].split()[:4])
-    vol_mat = {}
+    vol_mat, untagged = {}, False
     for line in ent[1 + npts + ncur + nsur:1 + npts + ncur + nsur + nvol]:
         tok = line.split()
         ntags = int(tok[7])
         if ntags > 1:
             raise ValueError(f"{path}: volume {tok[0]} has {ntags} physical tags; a volume takes one material")
-        vol_mat[int(tok[0])] = int(tok[8]) if ntags == 1 else 0
-    tagged = [t for t in vol_mat.values() if t > 0]
-    if tagged and len(tagged) != len(vol_mat):
+        # a volume without a physical tag is material 1 (homogeneous transport)
+        vol_mat[int(tok[0])] = int(tok[8]) if ntags == 1 else 1
+        untagged = untagged or ntags == 0
+    # untagged volumes are accepted next to volumes tagged 1, not next to other materials
+    if untagged and any(t != 1 for t in vol_mat.values()):
         raise ValueError(f"{path}: materials are given for some volumes but not for all")
     # nodes: blocks of (entityDim entityTag parametric n), n tags, n coordinate lines
     nd = sec["Nodes"]
@@ -149,7 +152,7 @@ def read_gmsh(path):
             raise ValueError(f"{path}: element type {etype} in volume {etag}; only 4-node tetrahedra are supported")
         blk = np.array([[int(v) for v in r.split()[1:5]] for r in rows], dtype=np.int64)
         nodes.append(tag_to_idx[blk])
-        mats.append(np.full(n, max(vol_mat.get(etag, 0), 1) - 1, dtype=np.int32))
+        mats.append(np.full(n, vol_mat.get(etag, 1) - 1, dtype=np.int32))
     if not nodes:
         raise ValueError(f"{path}: no tetrahedra")
     node = np.concatenate(nodes).astype(np.int32)

@@ -733,7 +733,7 @@ int mgsro(std::vector<std::vector<double>>& V, int ind, size_t n, double* hh) {
 // ------------------------------------------------------------------------------------------
 //  Restarted GMRES(m) / FGMRES(m) with SPARSKIT semantics: gmres iters.f:1901-2206, fgmres
 //  iters.f:2511-2795, stopping test ipar(3)=2 (||r|| <= rtol*||rhs|| + atol), as configured by
-//  GMRESWrapper (SPARSKIT.f90:151-192).  Written as a direct loop instead of reverse
+//  GMRESWrapper (SPARSKIT.f90:20-181).  Written as a direct loop instead of reverse
 //  communication; the arithmetic sequence per iteration is the reference's.
 //  precond == nullptr -> GMRES; otherwise FGMRES with right preconditioner z = precond(v).
 //  Returns 0 converged, -1 iteration limit, -3 breakdown.  iters = ipar(7) (matvec count).

@@ -8,13 +8,14 @@ plain text next to itself:
   ordinates_L7.txt   128 x 3  examples/three_beam_water_tank/lb.out                (PNSCATTERING 7)
   mu_slab_L15.txt     16      validation/electrons_incident/Al_521keV_0deg/lb.out  (slab, 16-point GL)
 
-Run from anywhere:  python tests/golden/make_golden.py [reference_root]
+Run from anywhere:  python tests/golden/make_golden.py <Lionbolt source root>
 """
 import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("LIONBOLT_REFERENCE") or sys.exit(
+    "usage: make_golden.py <Lionbolt source root> (or set LIONBOLT_REFERENCE)")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 

@@ -69,3 +69,13 @@ def jittered(mesh, amount, seed=1):
     from lionbolt_b200.mesh import Mesh
     return Mesh(rg=rg, node=mesh.node.copy(), neighbors=mesh.neighbors.copy(), mat=mesh.mat.copy(), Nm=mesh.Nm,
                 shape=mesh.shape)
+
+
+def golden_mesh(name):
+    """A mesh of the reference's tree stored as a tests/golden fixture (make_mesh_fixtures.py):
+    nodes, connectivity and materials as read by read_gmsh, neighbours rebuilt by face matching."""
+    from lionbolt_b200.mesh import Mesh, neighbours
+    d = np.load(os.path.join(GOLDEN, f"mesh_{name}.npz"))
+    node = d["node"].astype(np.int32)
+    mat = d["mat"].astype(np.int32)
+    return Mesh(rg=d["rg"].astype(np.float64), node=node, neighbors=neighbours(node), mat=mat, Nm=int(mat.max()) + 1)

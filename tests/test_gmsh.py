@@ -11,7 +11,8 @@ from lionbolt_b200 import mesh as M
 from lionbolt_b200 import problems as P
 from test_host import HostHandle
 
-REF = os.environ.get("LIONBOLT_REFERENCE", "/root/reference")
+# root of a Lionbolt source tree (its shipped meshes are read where it is given)
+REF = os.environ.get("LIONBOLT_REFERENCE")
 
 
 def _grouped(m):
@@ -43,9 +44,9 @@ def test_round_trip(tmp_path, which):
     ("examples/water_tank_with_aluminum/het_cube_spherical_beam.msh", 78771, 13707, [63313, 15458]),
 ])
 def test_reference_meshes(rel, ne, nn, counts):
+    if not REF or not os.path.exists(os.path.join(REF, rel)):
+        pytest.skip("LIONBOLT_REFERENCE does not name a Lionbolt tree with its mesh files")
     path = os.path.join(REF, rel)
-    if not os.path.exists(path):
-        pytest.skip("the reference's mesh files are not present")
     m = M.read_gmsh(path)
     assert (m.NE, m.NN) == (ne, nn)
     assert np.bincount(m.mat).tolist() == counts
@@ -104,3 +105,45 @@ def test_errors(tmp_path):
         M.read_gmsh(_write(tmp_path, ONE_TET.format(tags="1 2", etype=4, extra="")))
     with pytest.raises(ValueError, match="MSH 4.1 ASCII"):
         M.read_gmsh(_write(tmp_path, ONE_TET.replace("4.1 0 8", "2.2 0 8").format(tags="1 1", etype=4, extra="")))
+
+
+TWO_VOLUMES = """$MeshFormat
+4.1 0 8
+$EndMeshFormat
+$Entities
+0 0 0 2
+1 0 0 0 1 1 1 0 0
+2 0 0 0 1 1 1 {tags2} 0
+$EndEntities
+$Nodes
+1 5 1 5
+3 1 0 5
+1
+2
+3
+4
+5
+0 0 0
+1 0 0
+0 1 0
+0 0 1
+1 1 1
+$EndNodes
+$Elements
+2 2 1 2
+3 1 4 1
+1 1 2 3 4
+3 2 4 1
+2 2 3 4 5
+$EndElements
+"""
+
+
+def test_untagged_volume_is_material_one(tmp_path):
+    """ReadGMSH.f90:119-139: a volume without a physical tag is material 1; it may sit next to
+    volumes tagged 1, but not next to volumes of another material."""
+    m = M.read_gmsh(_write(tmp_path, TWO_VOLUMES.format(tags2="1 1")))
+    assert m.NE == 2 and m.Nm == 1 and np.all(m.mat == 0)
+    assert m.neighbors[0].tolist().count(1) == 1 and m.neighbors[1].tolist().count(0) == 1
+    with pytest.raises(ValueError, match="not for all"):
+        M.read_gmsh(_write(tmp_path, TWO_VOLUMES.format(tags2="1 2")))

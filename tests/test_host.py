@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from helpers import golden, jittered
+from helpers import golden, golden_mesh, jittered
 from lionbolt_b200 import _lib
 from lionbolt_b200 import mesh as M
 from lionbolt_b200 import problems as P
@@ -29,6 +29,24 @@ def test_library_exports_every_header_symbol():
     for s in syms:
         assert hasattr(lib, s), s
         assert s in _lib.SIGNATURES, f"{s} missing from the ctypes signature table"
+
+
+def _givens(x, y):
+    lib = _lib.load()
+    c, s, r = np.zeros(1), np.zeros(1), np.zeros(1)
+    assert lib.lb_givens(x, y, _lib.dptr(c), _lib.dptr(s), _lib.dptr(r)) == 0
+    return c[0], s[0], r[0]
+
+
+def test_givens_rotation_follows_sparskit():
+    """iters.f:3225-3262: (x, y) -> (r, 0), including its branch for NaN input (identity, r = 0)."""
+    for x, y in [(3.0, 4.0), (-4.0, 3.0), (1e-300, -2.0), (5.0, 0.0)]:
+        c, s, r = _givens(x, y)
+        assert abs(c * x + s * y - r) <= 1e-15 * max(1.0, r) and abs(-s * x + c * y) <= 1e-15 * max(1.0, r)
+        assert abs(r - np.hypot(x, y)) <= 1e-15 * r and abs(c * c + s * s - 1.0) < 1e-15
+    assert _givens(0.0, 0.0) == (1.0, 0.0, 0.0)
+    for x, y in [(np.nan, 1.0), (1.0, np.nan), (np.nan, np.nan)]:
+        assert _givens(x, y) == (1.0, 0.0, 0.0)
 
 
 def test_status_strings():
@@ -102,16 +120,14 @@ CASES = {
     "two_material": lambda: (P.config1_small(n=(4, 4, 8)).mesh, P.quadrature(6, 12)),
     "jittered": lambda: (jittered(M.box_mesh(5, 4, 3, (0, 0, 0), (2.5, 2.0, 1.5)), 0.06), P.quadrature(4, 8)),
     "L11_288": lambda: (M.box_mesh(3, 3, 6, (0, 0, 0), (1.5, 1.5, 3.0)), P.quadrature(12, 24)),
-    # an unstructured gmsh mesh of the reference (read where the reference tree is present)
-    "gmsh_simple_cube": lambda: (M.read_gmsh(REF_CUBE), P.quadrature(4, 8)),
+    # unstructured gmsh meshes of the reference (tests/golden fixtures of its shipped .msh files)
+    "gmsh_simple_cube": lambda: (golden_mesh("simple_cube"), P.quadrature(4, 8)),
+    "gmsh_het_cube": lambda: (golden_mesh("het_cube_spherical_beam"), P.quadrature(2, 4)),
 }
-REF_CUBE = os.path.join(os.environ.get("LIONBOLT_REFERENCE", "/root/reference"), "validation/operators/simple_cube.msh")
 
 
 @pytest.mark.parametrize("case", sorted(CASES))
 def test_schedule_bitexact_vs_literal_sweep_order(case):
-    if case.startswith("gmsh") and not os.path.exists(REF_CUBE):
-        pytest.skip("the reference's mesh files are not present")
     m, (k, w) = CASES[case]()
     o = O.Oracle(m)
     assert o.set_angular(k, w, 0, literal=True) == 0
