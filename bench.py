@@ -27,7 +27,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "B200 time-to-dose @1e-6 resid: learned-precond FGMRES vs plain GMRES; sweep GB/s"
-UNIT = "dose solves/s"
+UNIT = "cell-direction-group updates/s"
+NE_NI_NOTE = "an update = one element x one direction x one group of a transport sweep"
 
 
 def parse():
@@ -44,11 +45,15 @@ def parse():
     p.add_argument("--mesh", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
                    help="hexes per axis of a reduced box with the same physics (profiling cases)")
     p.add_argument("--groups", type=int, default=None, help="energy groups of the reduced box")
-    p.add_argument("--workload", default="dose", choices=["dose", "gemm", "batch"],
+    p.add_argument("--workload", default="dose", choices=["dose", "gemm", "batch", "mesh"],
                    help="dose: multigroup dose solve (default); gemm: standalone moment-to-discrete and "
                         "discrete-to-moment contractions at the 768k-tet size, split-BF16 vs cuBLAS FP32 vs FP64; "
                         "batch: 64 independent problems (8^3..32^3 hexes, S8/S12/S16, 1-10 groups, P3) solved "
-                        "together")
+                        "together; mesh: sweep throughput of a within-group solve on --mesh-file")
+    p.add_argument("--mesh-file", default=os.path.join(ROOT, "tests", "golden", "mesh_het_cube_spherical_beam.npz"),
+                   help="mesh of --workload mesh: .npz fixture, gmsh .msh, or 'jittered' (768k-tet box, moved nodes)")
+    p.add_argument("--no-subbench", action="store_true",
+                   help="skip the standalone-contraction and batched sub-records of the default line")
     p.add_argument("--no-learned", action="store_true",
                    help="skip the learned-preconditioner FGMRES comparison (training + timed solves)")
     p.add_argument("--lp-problems", type=int, default=3, help="training problems (seeded cross sections / slab)")
@@ -62,13 +67,29 @@ def parse():
 def workload(args):
     """The benchmarked problem: config1 (768,000 tets, 288 directions, 20 groups) unless reduced."""
     from lionbolt_b200 import problems as P
-    if args.mesh is None and args.groups is None:
-        return P.config1(), "config1 multigroup dose solve: 768000 tets x 288 dirs x 20 groups, P5"
+    full, wl = workload_name(args)
+    if full:
+        return P.config1(), wl
     n = tuple(args.mesh) if args.mesh else (40, 40, 80)
     G = args.groups or 20
     prob = P.multigroup_box(n=n, size=(0.5 * n[0], 0.5 * n[1], 0.5 * n[2]), G=G,
                             slab=(5.0 * n[2] / 80, 7.0 * n[2] / 80), name=f"box{n}")
-    return prob, (f"reduced config1 physics (profiling case): {prob.mesh.NE} tets x 288 dirs x {G} groups, P5")
+    return prob, wl
+
+
+def bench_config(args, world):
+    """The workload description both arms print (the reference arm times a slice of the same problem)."""
+    _, wl = workload_name(args)
+    return {"workload": f"{wl}, {args.solver}({args.m}) to {args.rtol:g}", "parallelism": f"replicas x{world}",
+            "l2": "inputs > L2 (3.5 GB angular vector)"}
+
+
+def workload_name(args):
+    if args.mesh is None and args.groups is None:
+        return True, "config1 multigroup dose solve: 768000 tets x 288 dirs x 20 groups, P5"
+    n = tuple(args.mesh) if args.mesh else (40, 40, 80)
+    NE = 6 * n[0] * n[1] * n[2]
+    return False, f"reduced config1 physics (profiling case): {NE} tets x 288 dirs x {args.groups or 20} groups, P5"
 
 
 def dist_env():
@@ -139,73 +160,103 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------------------------
-#  CPU baseline: the FP64 oracle (a restatement of the reference's OpenMP CPU path) on a bounded
-#  sample of the same workload.
+#  CPU side: the FP64 oracle, a restatement of the reference's OpenMP CPU path (literal
+#  encode / Sweep / decode for T^-1, the per-node dgemv loop of ScatteringAlgebra.f90:39-48 through
+#  the OpenBLAS bundled with scipy for K), timed on the host cores.
 # ---------------------------------------------------------------------------------------------
-_CPU_CACHE = {}
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            return next(l.split(":", 1)[1].strip() for l in f if l.startswith("model name"))
+    except (OSError, StopIteration):
+        return "unknown"
 
 
-def cpu_setup(prob, threads):
-    """Oracle on the full mesh (sweep sample) and on a sub-box (scattering sample)."""
-    if "o_full" in _CPU_CACHE:
-        return _CPU_CACHE
+def _oracle():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    from lionbolt_b200 import problems as P
+    return O
+
+
+def cpu_operator_oracles(prob, threads, nd):
+    """Oracles on the full mesh: one with nd evenly spaced directions and their sweep schedule (T^-1
+    on complete directions), one with the full quadrature and no schedule (K)."""
+    O = _oracle()
     O.set_threads(threads)
-    o_full = O.Oracle(prob.mesh)
-    sel = np.linspace(0, prob.NI - 1, threads).astype(int)         # one direction per thread
-    o_full.set_angular(prob.k[sel], prob.w[sel], prob.Ls, literal=False)
+    O.set_blas()
     sigt, sigs = prob.within_group(0)
-    o_full.set_xs(sigt, sigs)
-    sub = P.multigroup_box(n=(6, 6, 12), size=(3.0, 3.0, 6.0), G=1, Ng=prob.Ng, Nc=prob.Nc, slab=(1.0, 2.0))
-    o_sub = O.Oracle(sub.mesh)
-    o_sub.set_angular(sub.k, sub.w, prob.Ng - 1, literal=False)
-    s = np.zeros((2, prob.Ng))
-    s[:, :sigs.shape[1]] = sigs
-    o_sub.set_xs(sigt, s)
-    # matvec count of the FP64 reference method (angular GMRES(m)) per group, from the same physics
-    # on a coarsened mesh (iteration counts of the within-group solve depend on the scattering
-    # ratios and the optical size, not on the mesh resolution to first order)
-    coarse = P.multigroup_box(n=(4, 4, 8), G=prob.G, Ng=prob.Ng, Nc=prob.Nc)
-    o_c = O.Oracle(coarse.mesh)
-    o_c.set_angular(coarse.k, coarse.w, prob.Ls, literal=False)
+    sel = np.round(np.linspace(0, prob.NI - 1, nd)).astype(int)
+    o_t = O.Oracle(prob.mesh)
+    assert o_t.set_angular(prob.k[sel], prob.w[sel], prob.Ls, literal=False) == 0
+    o_t.set_xs(sigt, sigs)
+    o_k = O.Oracle(prob.mesh)
+    assert o_k.set_angular_no_schedule(prob.k, prob.w, prob.Ls) == 0
+    o_k.set_xs(sigt, sigs)
+    return o_t, o_k, sel
+
+
+def cpu_operator_time(o_t, o_k, q, x, sd1):
+    """Wall seconds of T^-1 on q (o_t's directions) and of K on the nodes [0, sd1) of x."""
     t0 = time.perf_counter()
-    _, _, iters = o_c.multigroup(coarse, "GMRES", m=20, rtol=1e-6)
-    _CPU_CACHE.update(o_full=o_full, sel=sel, o_sub=o_sub, sub=sub, iters=iters,
-                      iter_seconds=time.perf_counter() - t0)
-    return _CPU_CACHE
+    o_t.transport_inv(q, inplace=True)
+    t1 = time.perf_counter()
+    o_k.scatter_apply_dgemv(x, 0, sd1, inplace=True)
+    return t1 - t0, time.perf_counter() - t1
 
 
-def cpu_sample(prob, threads, budget_s):
-    """One bounded sample -> (estimated seconds per dose, details)."""
-    c = cpu_setup(prob, threads)
-    o_full, sel, o_sub, sub = c["o_full"], c["sel"], c["o_sub"], c["sub"]
-    rng = np.random.default_rng(0)
-    q = rng.uniform(size=o_full.NENK * len(sel))
-    t_sw, n_sw = 0.0, 0
-    x = rng.normal(size=o_sub.NENK * sub.NI)
-    t_k, n_k = 0.0, 0
-    t_end = time.perf_counter() + budget_s
-    while True:
-        t0 = time.perf_counter()
-        o_full.transport_inv(q)
-        t_sw += time.perf_counter() - t0
-        n_sw += 1
-        t0 = time.perf_counter()
-        o_sub.scatter_apply(x)
-        t_k += time.perf_counter() - t0
-        n_k += 1
-        if time.perf_counter() > t_end:
-            break
-    NI = prob.NI
-    sweep_full = (t_sw / n_sw) * NI / len(sel)                    # all 288 directions
-    k_full = (t_k / n_k) * prob.mesh.NENK / o_sub.NENK              # all 3,072,000 nodes
-    matvec = sweep_full + k_full
-    nmv = int(np.sum(c["iters"])) + 2 * prob.G                     # + RHS sweep and final sweep per group
-    sec_per_dose = nmv * matvec
-    return sec_per_dose, dict(sweep_s=sweep_full, scatter_s=k_full, matvecs=nmv, iters=c["iters"].tolist(),
-                              sweep_dirs=len(sel), scatter_nodes=o_sub.NENK)
+def fixture_iterations():
+    """Operator applications per group of the FP64 moment-space oracle at 1e-6 on the benchmarked
+    problem (tests/golden/config1_oracle.npz), or None."""
+    path = os.path.join(ROOT, "tests", "golden", "config1_oracle.npz")
+    if not os.path.exists(path):
+        return None
+    return np.load(path)["iters_snap"].astype(int)
+
+
+def cpu_baseline(prob, threads):
+    """One complete operator application of the FP64 CPU path on the benchmarked problem (T^-1 over
+    all 288 directions, K on all 3,072,000 nodes), and a complete small-problem solve (6,000 tets, 80
+    directions, GMRES(20) to 1e-8 in the reference's angular space)."""
+    from lionbolt_b200 import problems as P
+    O = _oracle()
+    O.set_threads(threads)
+    O.set_blas()
+    t_setup = time.perf_counter()
+    o_t = O.Oracle(prob.mesh)
+    assert o_t.set_angular(prob.k, prob.w, prob.Ls, literal=False) == 0
+    o_t.set_xs(*prob.within_group(0))
+    n = prob.mesh.NENK * prob.NI
+    x = np.random.default_rng(0).uniform(size=n)
+    t_setup = time.perf_counter() - t_setup
+    t_t, t_k = cpu_operator_time(o_t, o_t, x, x, prob.mesh.NENK)
+    del x, o_t
+    updates = prob.mesh.NE * prob.NI
+    # complete small solve
+    c0 = P.config0()
+    o0 = O.Oracle(c0.mesh)
+    o0.set_angular(c0.k, c0.w, c0.Ls, literal=False)
+    o0.set_xs(c0.sigt[0], c0.sigs[0, 0])
+    q0 = np.random.default_rng(1).uniform(size=c0.mesh.NENK * c0.NI)
+    t0 = time.perf_counter()
+    _, info = o0.boltzmann_solve(q0, "GMRES", m=20, rtol=1e-8, atol=0.0)
+    t_c0 = time.perf_counter() - t0
+    nmv = info["iters"] + 1
+    its = fixture_iterations()
+    derived = None
+    if its is not None:
+        ops = int(its.sum()) + prob.G            # + the right-hand-side sweep of every group
+        derived = {"time_to_dose_s": ops * (t_t + t_k), "operator_applications": ops,
+                   "note": "measured operator time x the FP64 oracle's operator count at 1e-6 (moment space); "
+                           "the reference's angular GMRES cannot hold this problem (85 GB workspace)"}
+    return {"value": updates / (t_t + t_k), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": (f"one complete operator application of the FP64 oracle on the 768k-tet problem: T^-1 over all "
+                       f"{prob.NI} directions (literal encode/sweep/decode, {t_t:.2f} s) + K through the per-node "
+                       f"OpenBLAS dgemv path on all {prob.mesh.NENK} nodes ({t_k:.2f} s)"),
+            "cpu": cpu_model(), "nproc": os.cpu_count(), "transport_inv_s": t_t, "scatter_s": t_k,
+            "setup_s": t_setup, "derived_config1": derived,
+            "config0_solve": {"seconds": t_c0, "operator_applications": nmv, "status": info["status"],
+                              "updates_per_s": c0.mesh.NE * c0.NI * nmv / t_c0,
+                              "workload": "6000 tets x 80 dirs x 1 group, P3, angular GMRES(20) to 1e-8"}}
 
 
 def training_problem(args, k):
@@ -219,9 +270,10 @@ def training_problem(args, k):
                             slab=(z0, z0 + 0.05 * depth), name=f"train{k}")
 
 
-def learned_comparison(args, mg, device, barrier, gmres_ms, gmres_dose):
-    """Train the per-cell network on plain-solver data (untimed), then time FGMRES with it on the
-    benchmarked problem; the plain-GMRES dose checks its answer."""
+def learned_comparison(args, mg, device, barrier, gmres_ms, gmres_dose, gmres_iters, phase_ms):
+    """Train the per-cell network on plain-solver data (untimed), decide per group on a held-out
+    problem whether the learned FGMRES beats plain GMRES there (untimed), then time FGMRES with that
+    gating on the benchmarked problem; the plain-GMRES dose checks its answer."""
     from lionbolt_b200 import MultigroupSolver
     t0 = time.perf_counter()
     tr = MultigroupSolver(device=device)
@@ -233,9 +285,16 @@ def learned_comparison(args, mg, device, barrier, gmres_ms, gmres_dose):
     t_gen = time.perf_counter() - t0
     loss = tr.lp_train(steps=args.lp_steps, batch=2048, lr=3e-3, seed=11)
     w = tr.lp_get_weights()
-    tr.Destroy()
     t_train = time.perf_counter() - t0 - t_gen
+    # held-out calibration: another seed and slab position than every training problem
+    tr.set_problem(training_problem(args, args.lp_problems))
+    plain_v, learned_v = tr.lp_calibrate(m=args.m, rtol=args.rtol)
+    tr.Destroy()
+    t_cal = time.perf_counter() - t0 - t_gen - t_train
+    # a learned application costs one operator application plus the network (about a tenth of one)
+    enabled = (1.1 * learned_v < plain_v).astype(np.int32)
     mg.lp_set_weights(w)
+    mg.lp_set_groups(enabled, budget=plain_v)
     h = mg._h
     warm = min(args.warmup, 1)
     for _ in range(warm):
@@ -249,10 +308,27 @@ def learned_comparison(args, mg, device, barrier, gmres_ms, gmres_dose):
     ml_ms = h.elapsed_ms(2, 3) / args.steps
     _, dose = mg.results()
     mg.lp_enable(False)
+    mg.lp_set_groups(None)
     rel = float(np.linalg.norm(dose - gmres_dose) / max(np.linalg.norm(gmres_dose), 1e-300))
-    return {"solver": f"FGMRES({args.m}) + per-cell MLP right preconditioner", "time_to_dose_s": ml_ms / 1e3,
-            "speedup_vs_gmres": gmres_ms / ml_ms, "iterations_per_group": [int(x) for x in it],
+    # Upper bound of any right preconditioner: an exact, free A^-1 makes FGMRES converge after the
+    # initial-residual application and one more per group (plus the right-hand-side sweep); the time
+    # of everything else is unchanged.  Per-application time from the plain solve's phase timers.
+    G = len(gmres_iters)
+    nmv = int(np.sum(gmres_iters))
+    t_app = sum(phase_ms.get(k, 0.0) for k in ("sweep", "m2d", "d2m", "krylov")) / (nmv + G)
+    t_other = gmres_ms - t_app * (nmv + G)
+    bound = gmres_ms / (t_other + t_app * 3 * G)
+    bound_zero_guess = gmres_ms / (t_other + t_app * 2 * G)
+    return {"solver": f"FGMRES({args.m}) + per-cell MLP right preconditioner, gated per group",
+            "time_to_dose_s": ml_ms / 1e3, "speedup_vs_gmres": gmres_ms / ml_ms,
+            "iterations_per_group": [int(x) for x in it], "gmres_iterations_per_group": [int(x) for x in gmres_iters],
             "dose_rel_l2_vs_gmres": rel, "warmup": warm, "steps": args.steps,
+            "gating": {"heldout_plain": plain_v.tolist(), "heldout_learned": learned_v.tolist(),
+                       "enabled_groups": int(enabled.sum()), "rule": "learned x 1.1 < plain on a held-out problem",
+                       "calibrate_s": t_cal},
+            "bound_exact_inverse": {"speedup": bound, "speedup_zero_initial_guess": bound_zero_guess,
+                                    "ms_per_application": t_app,
+                                    "note": "free exact A^-1: 2 applications per group + the right-hand side"},
             "training": {"problems": args.lp_problems, "samples": int(total), "adam_steps": int(args.lp_steps),
                          "loss_first20": float(np.mean(loss[:20])), "loss_last50": float(np.mean(loss[-50:])),
                          "generate_s": t_gen, "train_s": t_train}}
@@ -289,17 +365,21 @@ def real_sh(Ls, dirs):
 
 # kernel of each sweep schedule the autotuner can pick
 SWEEP_KERNELS = {"cluster levels": "sweep_cluster_kernel", "cluster levels+type tables": "sweep_cluster_kernel",
+                 "cluster levels+element prefetch": "sweep_cluster_kernel",
+                 "cluster levels+type tables+element prefetch": "sweep_cluster_kernel",
                  "levels": "sweep_levels_kernel",
                  "levels+prefetch": "sweep_levels_pf_kernel", "element flags": "sweep_flags_kernel",
                  "grouped directions": "sweep_group_kernel", "dataflow": "sweep_dataflow_kernel"}
 
 
-def run_gemm(args):
+def run_gemm(args, steps=None, warmup=None, emit=True):
     """Standalone scattering contractions (config2 shapes): M2D psi[288][3,072,000] = Y[288][36]
     phi[36][3,072,000] and D2M phi = (wY)^T psi, on the device.  Split-BF16 tensor-core kernels vs
     cuBLAS FP32 (TF32 off) vs an FP64 reference on 65,536 sampled node columns."""
     import ctypes
     import torch
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
     from lionbolt_b200 import AngularClass, ScatteringOp, XSType
     from lionbolt_b200 import problems as P
     rank, world, local = dist_env()
@@ -322,14 +402,14 @@ def run_gemm(args):
     vp = ctypes.c_void_p
 
     def timed(fn, slot):
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             fn()
         h.call("lb_synchronize")
         h.mark(slot)
-        for _ in range(args.steps):
+        for _ in range(steps):
             fn()
         h.mark(slot + 1)
-        return h.elapsed_ms(slot, slot + 1) / args.steps
+        return h.elapsed_ms(slot, slot + 1) / steps
 
     t_m2d = timed(lambda: h.call("lb_m2d_device", vp(phi.data_ptr()), vp(psi.data_ptr())), 0)
     t_d2m = timed(lambda: h.call("lb_d2m_device", vp(psi.data_ptr()), vp(phi2.data_ptr())), 2)
@@ -341,16 +421,16 @@ def run_gemm(args):
     Y32, D32, phi32 = Y.float(), D.float(), phi.float()
 
     def tevent(fn):
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             fn()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         a.record()
-        for _ in range(args.steps):
+        for _ in range(steps):
             out = fn()
         b.record()
         torch.cuda.synchronize()
-        return a.elapsed_time(b) / args.steps, out
+        return a.elapsed_time(b) / steps, out
 
     t_m2d32, psi32 = tevent(lambda: Y32 @ phi32)
     t_d2m32, phi2_32 = tevent(lambda: D32 @ psi)
@@ -377,21 +457,25 @@ def run_gemm(args):
     line = {"metric": "config2 scattering contractions: split-BF16 (6 products, FP32 accumulate) vs FP32 vs FP64",
             "workload": f"M2D [{NI} x {nm}] x [{nm} x {NENK}] and D2M [{nm} x {NI}] x [{NI} x {NENK}], "
                         "phi ~ N(0,1) 0.8^l, seeded",
-            "steps": args.steps, "warmup": args.warmup, "peak_gbs": peak, "peak_source": kind,
+            "steps": steps, "warmup": warmup, "peak_gbs": peak, "peak_source": kind,
             "m2d": entry(t_m2d, by_m2d, e_m2d, t_m2d32, e_m2d32),
             "d2m": entry(t_d2m, by_d2m, e_d2m, t_d2m32, e_d2m32),
             "sample_columns": int(cols.numel()),
             "algorithmic_bytes": {"m2d": by_m2d, "d2m": by_d2m}}
-    if rank == 0:
+    if rank == 0 and emit:
         print(json.dumps(line), flush=True)
     op.Destroy()
-    return 0
+    del phi, psi, phi2, psi32, phi2_32, Y32, D32, phi32
+    torch.cuda.empty_cache()
+    return line
 
 
-def run_batch(args):
+def run_batch(args, steps=None, warmup=None, emit=True):
     """Batched workload: 64 seeded independent dose problems solved together (one step = all 64)."""
     import torch
     from lionbolt_b200 import BatchSolver
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
     from lionbolt_b200 import problems as P
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
@@ -399,14 +483,14 @@ def run_batch(args):
     bs = BatchSolver(device=local)
     for p in probs:
         bs.add_problem(p)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         bs.solve(m=args.m, rtol=args.rtol)
     torch.cuda.synchronize()
     ms, it = [], None
     with ClockSampler(local) as clocks:
         if args.profile_range:
             torch.cuda.profiler.start()
-        for _ in range(args.steps):
+        for _ in range(steps):
             it = bs.solve(m=args.m, rtol=args.rtol)
             ms.append(bs.info()["last_ms"])
         if args.profile_range:
@@ -416,54 +500,160 @@ def run_batch(args):
     NE = np.array([p.mesh.NE for p in probs])
     NI = np.array([p.NI for p in probs])
     upd = float(sum(int(NE[i]) * int(NI[i]) * int(it[i].sum()) for i in range(len(probs))))
-    line = {"metric": "batched dose solves (config3): 64 independent problems per step", "value": 64 * args.steps / (t / 1e3),
-            "unit": "dose solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": t / args.steps, "higher_is_better": True, "dtype": "f32 sweep / split-bf16 moments / f64 Krylov",
+    line = {"metric": "batched dose solves (config3): 64 independent problems per step", "value": 64 * steps / (t / 1e3),
+            "unit": "dose solves/s", "n_gpus": 1, "steps": steps, "warmup": warmup,
+            "ms_per_step": t / steps, "higher_is_better": True, "dtype": "f32 sweep / split-bf16 moments / f64 Krylov",
             "data": "synthetic",
             "config": {"workload": "64 problems: hexes per axis U{8..32} x 6 tets, S8/S12/S16, 1-10 groups, P3, "
                                    f"GMRES({args.m}) to {args.rtol:g}, seed 20261203",
                        "tets_total": int(NE.sum()), "groups_total": int(sum(p.G for p in probs))},
-            "updates_per_s": upd / (t / args.steps / 1e3) / args.steps * args.steps,
+            "updates_per_s": upd / (t / steps / 1e3),
             "operator_applications": int(it.sum()), "sweep_threads": info["sweep_threads"],
             "graph_launches": info["graph_launches"], "sweep_launches": info["sweep_launches"],
             "clocks": clocks.summary()}
-    if rank == 0:
+    if rank == 0 and emit:
         print(json.dumps(line), flush=True)
     bs.close()
-    return 0
+    return line
+
+
+def general_mesh(spec):
+    """A mesh for --workload mesh: a .npz fixture (rg, node, mat), a gmsh .msh file, or "jittered" (the
+    40 x 40 x 80-hex box of the dose workload with every interior node moved by up to 0.15 of a hex
+    edge, so that no two tets share a shape: 64-byte element records and the element-level sweep)."""
+    from lionbolt_b200 import mesh as M
+    if spec == "jittered":
+        m = M.box_mesh(40, 40, 80, (0, 0, 0), (20.0, 20.0, 40.0),
+                       material=lambda c: ((c[:, 2] >= 5.0) & (c[:, 2] <= 7.0)).astype(np.int32), Nm=2)
+        rg = m.rg.copy()
+        lo, hi = rg.min(axis=0), rg.max(axis=0)
+        inner = np.all((rg > lo + 1e-9) & (rg < hi - 1e-9), axis=1)
+        rg[inner] += 0.075 * np.random.default_rng(5).uniform(-1, 1, size=(int(inner.sum()), 3))
+        return M.Mesh(rg=rg, node=m.node, neighbors=m.neighbors, mat=m.mat, Nm=2), "768000-tet box, jittered nodes"
+    if spec.endswith(".npz"):
+        d = np.load(spec)
+        node = d["node"].astype(np.int32)
+        mat = d["mat"].astype(np.int32)
+        return (M.Mesh(rg=d["rg"], node=node, neighbors=M.neighbours(node), mat=mat, Nm=int(mat.max()) + 1),
+                os.path.basename(spec))
+    return M.read_gmsh(spec), os.path.basename(spec)
+
+
+def run_mesh(args):
+    """Sweep throughput of a within-group solve (288 directions, P5, c = 0.9, g = 0.95) on a general
+    mesh; the sweep's algorithmic bytes (lb_sweep_stats) over its device time give the roofline."""
+    import torch
+    from lionbolt_b200 import AngularClass, BoltzmannOp, XSType
+    from lionbolt_b200 import problems as P
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    m, name = general_mesh(args.mesh_file)
+    k, w = P.quadrature(12, 24)
+    sigt = np.array([0.2, 0.54])[:m.Nm]
+    sigs = np.array([[0.9 * s * 0.95 ** l for l in range(6)] for s in sigt])
+    L = BoltzmannOp(device=local, m=args.m, rtol=args.rtol, atol=0.0).Build(m, AngularClass(k=k, w=w),
+                                                                         XSType(sigt, sigs))
+    h = L._h
+    q = np.random.default_rng(0).uniform(size=m.NENK * k.shape[0])
+    for _ in range(max(args.warmup, 3)):      # the first sweeps of a handle time the schedule candidates
+        L.MatInv(q.copy())
+    h.reset_timers()
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            L.MatInv(q.copy())
+    tm = h.timers()
+    by, up, nz = np.zeros(1), np.zeros(1), np.zeros(1, dtype=np.int64)
+    h.call("lb_sweep_stats", _lib_mod().dptr(by), _lib_mod().dptr(up), nz.ctypes.data_as(_lib_mod()._c_ll_p))
+    sw_ms, sw_n = tm["sweep"]
+    per = sw_ms / max(sw_n, 1)
+    peak, kind = measured_peaks()
+    gbs = by[0] / (per / 1e3) / 1e9
+    launch = h.sweep_config() or {}
+    line = {"metric": "sweep throughput on a general mesh", "mesh": name, "tets": m.NE, "element_types": h.mesh_types(),
+            "directions": int(k.shape[0]), "sweep_ms": per, "sweeps": sw_n, "updates_per_s": up[0] / (per / 1e3),
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                         "peak_source": kind, "algorithmic_bytes": float(by[0]),
+                         "kernel": SWEEP_KERNELS.get(launch.get("schedule"), "sweep")},
+            "launch": launch, "operator_applications": L.iters, "clocks": clocks.summary()}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    L.Destroy()
+    return line
+
+
+def _lib_mod():
+    from lionbolt_b200 import _lib
+    return _lib
+
+
+REF_FRACTION = 4   # a reference step is 1/REF_FRACTION of one complete operator application
 
 
 def run_reference(args):
+    """The FP64 CPU path (the oracle, kind "port": the Fortran reference has no compiler here) on all host
+    cores.  A step is a complete 1/4 of one operator application of the benchmarked problem: T^-1 over 72
+    of the 288 directions on the full 768k-tet mesh and K through the per-node dgemv path on a quarter of
+    the 3,072,000 nodes.  value = cell-direction-group updates of the step / its wall time."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
     from lionbolt_b200 import problems as P
     prob = P.config1()
     threads = os.cpu_count() or 1
-    per_step = max(3.0, min(args.cpu_seconds, 12.0))
+    nd = prob.NI // REF_FRACTION
+    o_t, o_k, sel = cpu_operator_oracles(prob, threads, nd)
+    rng = np.random.default_rng(0)
+    q = rng.uniform(size=prob.mesh.NENK * nd)
+    x = rng.uniform(size=prob.mesh.NENK * prob.NI)
+    sd1 = prob.mesh.NENK // REF_FRACTION
     for _ in range(args.warmup):
-        cpu_sample(prob, threads, 1.0)
-    times, det = [], None
+        cpu_operator_time(o_t, o_k, q, x, sd1)
+    tt, tk = [], []
     for _ in range(args.steps):
-        s, det = cpu_sample(prob, threads, per_step)
-        times.append(s)
-    sec = float(np.mean(times))
-    value = 1.0 / sec
-    sample = (f"FP64 oracle (CPU restatement of the reference OpenMP path; the Fortran reference has no compiler "
-              f"here): T^-1 over {det['sweep_dirs']} of 288 directions on the full 768k-tet mesh + K (per-node "
-              f"dgemv path, 2 materials) on {det['scatter_nodes']} nodes, scaled to the full sizes; "
-              f"x {det['matvecs']} operator applications (angular GMRES(20) counts of the same physics on a "
-              f"coarsened mesh)")
+        a, b = cpu_operator_time(o_t, o_k, q, x, sd1)
+        tt.append(a)
+        tk.append(b)
+    sec = (sum(tt) + sum(tk)) / args.steps
+    updates = prob.mesh.NE * nd
+    value = updates / sec
+    its = fixture_iterations()
+    sample = (f"FP64 oracle (CPU restatement of the reference's OpenMP path): per step T^-1 over {nd} of {prob.NI} "
+              f"directions on the full 768000-tet mesh (literal encode/sweep/decode) + K through the per-node "
+              f"OpenBLAS dgemv path on {sd1} of {prob.mesh.NENK} nodes (1/{REF_FRACTION} of one operator "
+              f"application); {NE_NI_NOTE}")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "config1 multigroup dose solve: 768000 tets x 288 dirs x 20 groups, P5, GMRES to 1e-6",
-                       "timing": "CPU wall clock of a bounded sample, extrapolated"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "config": bench_config(args, world),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+                             "cpu": cpu_model(), "nproc": os.cpu_count()},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "details": det}
+            "transport_inv_s_per_step": sum(tt) / args.steps, "scatter_s_per_step": sum(tk) / args.steps,
+            "derived_time_to_dose_s": (None if its is None else
+                                       (int(its.sum()) + prob.G) * sec * REF_FRACTION)}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def fixture_errors(prob, flux, dose):
+    """Relative L2 errors of the dose and every group's fluence against the FP64 oracle's converged
+    solution of the benchmarked problem (tests/golden/config1_oracle.npz): on the fixture's 4096
+    sampled DG nodes, on the per-z-layer sums (every node), and of the full-vector norms."""
+    path = os.path.join(ROOT, "tests", "golden", "config1_oracle.npz")
+    if not os.path.exists(path):
+        return None
+    d = np.load(path)
+    nodes = d["nodes"]
+    nx, ny, nz = prob.mesh.shape
+    layers = lambda v: v.reshape(nz, -1).sum(axis=1)
+    rel = lambda a, b: float(np.linalg.norm(np.asarray(a) - b) / np.linalg.norm(b))
+    fl = [rel(flux[g, nodes], d["flux"][g]) for g in range(prob.G)]
+    return {"dose_rel_l2": rel(dose[nodes], d["dose"]), "flux_rel_l2_max": max(fl), "flux_rel_l2": fl,
+            "dose_layers_rel_l2": rel(layers(dose), d["dose_layers"]),
+            "flux_layers_rel_l2_max": max(rel(layers(flux[g]), d["flux_layers"][g]) for g in range(prob.G)),
+            "dose_norm_rel": abs(float(np.linalg.norm(dose)) / float(d["dose_norm"]) - 1.0),
+            "oracle": "FP64 moment-space GMRES(20) to 1e-10 (converged), tests/golden/config1_oracle.npz",
+            "oracle_1e-6_dose_rel_l2": float(d["snap_dose_rel_l2"])}
 
 
 def run_ours(args):
@@ -476,7 +666,6 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     from lionbolt_b200 import MultigroupSolver
     from lionbolt_b200 import _lib
-    from lionbolt_b200 import problems as P
 
     prob, wl = workload(args)
     mg = MultigroupSolver(device=local).set_problem(prob)
@@ -517,12 +706,14 @@ def run_ours(args):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         t_max = float(t.item())
     ms_per_step = t_max / args.steps
-    value = world * args.steps / (t_max / 1e3)
 
     # sweep roofline
     by, up, nz = np.zeros(1), np.zeros(1), np.zeros(1, dtype=np.int64)
     h.call("lb_sweep_stats", _lib.dptr(by), _lib.dptr(up), nz.ctypes.data_as(_lib._c_ll_p))
     sw_ms, sw_n = tm["sweep"]
+    sweeps_per_step = sw_n / args.steps
+    updates_per_step = float(up[0]) * sweeps_per_step        # NE * NI per sweep (one group)
+    value = world * updates_per_step / (ms_per_step / 1e3)
     per_sweep_ms = sw_ms / max(sw_n, 1)
     achieved = by[0] / (per_sweep_ms / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
@@ -557,45 +748,56 @@ def run_ours(args):
         t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e_value = world * args.steps / e2e_s
+    e2e_value = world * updates_per_step * args.steps / e2e_s
     gmres_dose = h_dose.numpy().copy()
+
+    # accuracy against the FP64 oracle's converged solution of the same problem
+    accuracy = None
+    if rank == 0 and workload_name(args)[0] and args.solver == "GMRES":
+        flux, dose = mg.results()
+        accuracy = fixture_errors(prob, flux, dose)
 
     learned = None
     if not args.no_learned and args.solver == "GMRES":
-        learned = learned_comparison(args, mg, local, barrier, ms_per_step, gmres_dose)
+        learned = learned_comparison(args, mg, local, barrier, ms_per_step, gmres_dose, iters,
+                                     {k: v[0] / args.steps for k, v in tm.items()})
+
+    sub = {}
+    if not args.no_subbench and world == 1:
+        mg.Destroy()
+        mg = None
+        sub["gemm"] = run_gemm(args, steps=10, warmup=3, emit=False)
+        sub["batch"] = run_batch(args, steps=2, warmup=1, emit=False)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        sec, det = cpu_sample(prob, threads, args.cpu_seconds)
-        cpu = {"value": 1.0 / sec, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": (f"FP64 oracle, T^-1 over {det['sweep_dirs']} directions of the full mesh + K on "
-                          f"{det['scatter_nodes']} nodes scaled to full size, x {det['matvecs']} operator "
-                          f"applications; {args.cpu_seconds:.0f} s budget")}
+        cpu = cpu_baseline(prob, os.cpu_count() or 1)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32 sweep / split-bf16 tensor-core moments / f64 Krylov",
-                "data": "synthetic",
-                "config": {"workload": f"{wl}, {args.solver}({args.m}) to {args.rtol:g}",
-                           "parallelism": f"replicas x{world}", "l2": "inputs > L2 (3.5 GB angular vector)"},
-                "time_to_dose_s": ms_per_step / 1e3,
+                "data": "synthetic", "config": bench_config(args, world),
+                "time_to_dose_s": ms_per_step / 1e3, "dose_solves_per_s": world / (ms_per_step / 1e3),
+                "updates_per_step": updates_per_step, "sweeps_per_step": sweeps_per_step,
                 "iterations_per_group": [int(x) for x in iters],
-                "updates_per_s": float(up[0]) * (sum(int(x) for x in iters) + 2 * G) / (ms_per_step / 1e3),
+                "accuracy_vs_fp64_oracle": accuracy,
                 "phase_ms_per_step": {k: v[0] / args.steps for k, v in tm.items()},
                 "sweep": {"ms": per_sweep_ms, "gbs": achieved, "updates_per_s": up[0] / (per_sweep_ms / 1e3),
-                          "launch": launch},
+                          "algorithmic_bytes": float(by[0]), "upstream_faces": int(nz[0]), "launch": launch},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "kernel": kernel,
                              "peak_source": peak_kind},
                 "gpu_launches": launches,
                 "clocks": clocks.summary(),
-                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "time_to_dose_s": e2e_s / args.steps},
                 "cpu_baseline": cpu,
                 "learned_preconditioner": learned}
+        line.update(sub)
         print(json.dumps(line), flush=True)
-    mg.Destroy()
+    if mg is not None:
+        mg.Destroy()
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
@@ -606,9 +808,14 @@ def main():
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "gemm":
-        return run_gemm(args)
+        run_gemm(args)
+        return 0
     if args.workload == "batch":
-        return run_batch(args)
+        run_batch(args)
+        return 0
+    if args.workload == "mesh":
+        run_mesh(args)
+        return 0
     return run_ours(args)
 
 

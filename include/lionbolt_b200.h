@@ -45,7 +45,9 @@ enum lb_status {
 enum lb_solver {
     LB_SOLVER_SI = 0,          /* source iteration, src/solvers/SourceIteration.f90           */
     LB_SOLVER_GMRES = 1,       /* restarted GMRES(m), third_party/SPARSKIT/iters.f:1901        */
-    LB_SOLVER_FGMRES_ML = 2    /* FGMRES(m) with the learned right preconditioner             */
+    LB_SOLVER_FGMRES_ML = 2,   /* FGMRES(m) with the learned right preconditioner             */
+    LB_SOLVER_FGMRES = 3       /* FGMRES(m), iters.f:2511-2795, with the diagonal right
+                                  preconditioner of lb_set_right_precond_diag (identity if unset) */
 };
 
 /* phase timers reported by lb_get_timers (milliseconds of device time, CUDA events) */
@@ -134,6 +136,12 @@ int lb_scatter_apply(lb_handle* h, double* x);
 
 /* x <- x - T^{-1} K x: replaces BoltzmannOp%MatVec with Tprecond (BoltzmannOperator.f90:59-104). */
 int lb_boltzmann_matvec(lb_handle* h, double* x);
+
+/* Right preconditioner of LB_SOLVER_FGMRES: z_j = d[j] v_j on moment row j (j = l*l + l + m),
+ * nm = (Ls+1)^2 of the current cross sections (<= 64); nm = 0 or d = NULL restores the identity.
+ * SPARSKIT fgmres takes any right preconditioner through reverse communication (ipar(1) = 5); this
+ * fixed one exists so that the flexible driver can be checked step for step. */
+int lb_set_right_precond_diag(lb_handle* h, int nm, const double* d);
 
 /* L^{-1} s in place: replaces BoltzmannOp%MatInv (BoltzmannOperator.f90:106-151).  The Krylov
  * iteration runs in flux-moment space (n = nm*NENK) with the SPARSKIT stopping test
@@ -234,6 +242,15 @@ int lb_lp_num_samples(lb_handle* h, long long* n);
  * over the 16 moments; its weight is s^2 over the mean square of the residual field's moments. */
 int lb_lp_get_samples(lb_handle* h, float* x, float* t, float* w);
 int lb_lp_clear_samples(lb_handle* h);
+/* Per-group use of the learned path in lb_mg_solve with LB_SOLVER_FGMRES_ML: enabled[g] = 0 runs
+ * plain GMRES on group g; budget[g] > 0 (budget may be NULL) caps group g's learned FGMRES at that
+ * many operator applications, after which plain GMRES finishes from the learned iterate (default
+ * cap 4m).  G = 0 clears both (every group learned, cap 4m). */
+int lb_lp_set_groups(lb_handle* h, int G, const int* enabled, const int* budget);
+/* Operator applications per group of the learned FGMRES(m) and of plain GMRES(m) to rtol on the
+ * handle's multigroup problem (each group from the first-flight moments, the plain answer feeding
+ * the groups below): the data for lb_lp_set_groups, taken on a problem other than the one solved. */
+int lb_lp_calibrate(lb_handle* h, int m, double rtol, int* plain_iters, int* learned_iters);
 /* `steps` Adam steps (cosine-decayed learning rate from lr to lr/20) on batches of `batch` samples
  * drawn from the training set; loss_hist[steps] (optional) receives the batch losses. */
 int lb_lp_train(lb_handle* h, int steps, int batch, double lr, unsigned long long seed, double* loss_hist);

@@ -25,6 +25,7 @@ LB_ERR_BREAKDOWN = 9
 SOLVER_SI = 0
 SOLVER_GMRES = 1
 SOLVER_FGMRES_ML = 2
+SOLVER_FGMRES = 3
 
 TIMER_NAMES = ("sweep", "m2d", "d2m", "krylov", "copy", "precond", "tally")
 
@@ -64,6 +65,9 @@ SIGNATURES = {
     "lb_synchronize": (ctypes.c_int, [_vp]),
     "lb_get_sweep_config": (ctypes.c_int, [_vp, _c_int_p]),
     "lb_mesh_types": (ctypes.c_int, [_vp, _c_int_p]),
+    "lb_set_right_precond_diag": (ctypes.c_int, [_vp, ctypes.c_int, _c_double_p]),
+    "lb_lp_set_groups": (ctypes.c_int, [_vp, ctypes.c_int, _c_int_p, _c_int_p]),
+    "lb_lp_calibrate": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, _c_int_p, _c_int_p]),
     "lb_givens": (ctypes.c_int, [ctypes.c_double, ctypes.c_double, _c_double_p, _c_double_p, _c_double_p]),
     "lb_cluster_info": (ctypes.c_int, [_vp, _c_int_p, _c_int_p]),
     "lb_get_cluster_schedule": (ctypes.c_int, [_vp, _c_int_p, _c_int_p, _c_int_p]),
@@ -202,6 +206,8 @@ class Handle:
                  dirs_per_cta=int(cfg[2]), ilp=int(cfg[3]))
         if kind in (5, 6):
             d["min_ctas_per_sm"] = d.pop("dirs_per_cta")
+            if d["ilp"] == 2:
+                d["schedule"] += "+element prefetch"
         return d
 
     def mesh_types(self):

@@ -201,6 +201,17 @@ __global__ void scale_kernel(double* y, double a, size_t n) {
     for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) y[q] *= a;
 }
 
+// z[j][n] = c[j] v[j][n] for the nm moment rows (blockIdx.y = j)
+struct RowCoefs {
+    double c[kMaxRowCoefs];
+};
+__global__ void scale_rows_kernel(double* __restrict__ z, const double* __restrict__ v, RowCoefs rc, size_t NENK) {
+    const double c = rc.c[blockIdx.y];
+    const size_t off = (size_t)blockIdx.y * NENK;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < NENK; q += (size_t)gridDim.x * blockDim.x)
+        z[off + q] = c * v[off + q];
+}
+
 __global__ void fill_kernel(double* y, double v, size_t n) {
     for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) y[q] = v;
 }
@@ -525,6 +536,19 @@ int k_scale(Handle* h, double* y, double a, size_t n) {
 int k_copy(Handle* h, double* y, const double* x, size_t n) {
     cudaError_t e = cudaMemcpyAsync(y, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream);
     return e == cudaSuccess ? LB_OK : cuda_fail(h, e, "copy");
+}
+
+int k_scale_rows(Handle* h, double* z, const double* v, const double* coef, int nm, size_t NENK) {
+    if (nm < 1 || nm > kMaxRowCoefs) return fail(h, LB_ERR_ARG, "k_scale_rows: too many moment rows");
+    RowCoefs rc{};
+    for (int j = 0; j < nm; ++j) rc.c[j] = coef[j];
+    Timer t;
+    timer_begin(h, LB_T_PRECOND, t);
+    int gx = grid_for(h, NENK * (size_t)nm) / nm;
+    dim3 grid(gx < 1 ? 1 : gx, nm);
+    scale_rows_kernel<<<grid, 256, 0, h->stream>>>(z, v, rc, NENK);
+    timer_end(h, t);
+    return LB_OK;
 }
 
 int k_fill(Handle* h, double* y, double v, size_t n) {

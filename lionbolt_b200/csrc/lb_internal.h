@@ -136,6 +136,7 @@ struct Handle {
     int kry_m = 0;
     double* d_V = nullptr;         // [(m+1)][N] basis
     double* d_Z = nullptr;         // [m][N] flexible basis (FGMRES)
+    std::vector<double> pdiag;     // per-moment right-preconditioner scaling of LB_SOLVER_FGMRES (empty: identity)
     double* d_x = nullptr;         // solution
     double* d_b = nullptr;         // rhs
     double* d_t = nullptr;         // scratch
@@ -176,6 +177,10 @@ struct Handle {
 
     // learned preconditioner state (mlp.cu)
     void* mlp = nullptr;
+    // per-group use of the learned path in multigroup solves (empty: every group) and the operator
+    // applications after which a group's learned FGMRES gives way to plain GMRES (0: 4m)
+    std::vector<char> lp_groups;
+    std::vector<int> lp_budget;
 
     // batched solves (batch.cpp): a problem of a batch records no CUDA events (its launches may be
     // captured into graphs) and its moment kernels skip their work while *d_active == 0
@@ -312,6 +317,8 @@ int k_axpby_norm(Handle* h, double* y, const double* x, double a, double b, size
 int k_multi_axpy(Handle* h, double* w, const double* V, size_t ldv, int nv, const double* coef_host, size_t n);
 int k_axpby(Handle* h, double* y, const double* x, double a, double b, size_t n);   // y = a*x + b*y
 int k_scale(Handle* h, double* y, double a, size_t n);
+constexpr int kMaxRowCoefs = 64;   // moment rows of k_scale_rows (P7)
+int k_scale_rows(Handle* h, double* z, const double* v, const double* coef, int nm, size_t NENK);   // z_j = c_j v_j
 int k_copy(Handle* h, double* y, const double* x, size_t n);
 int k_fill(Handle* h, double* y, double v, size_t n);
 int k_f64_to_f32(Handle* h, float* y, const double* x, size_t n);

@@ -8,8 +8,8 @@
 // and psi = T^{-1}(M Sigma phi + q).  The Krylov vectors shrink from NI*NENK to nm*NENK
 // (288 -> 36 per node at P5) and stay FP64; the sweep and the moment GEMMs run in FP32.
 // The Arnoldi/Givens/restart logic and the stopping test ||b - A phi|| <= rtol||b|| + atol follow
-// the reference's SPARSKIT gmres/fgmres; orthogonalisation is classical Gram-Schmidt with
-// selective re-orthogonalisation (one fused multi-dot and one fused multi-axpy per pass).
+// the reference's SPARSKIT gmres/fgmres; orthogonalisation is Gram-corrected classical
+// Gram-Schmidt (two fused passes over the basis per Arnoldi step, see gmres_device).
 #include "lb_internal.h"
 #include "gmres_host.h"
 #include <cmath>
@@ -215,21 +215,38 @@ static KrylovResult si_device(Handle* h, size_t n, const double* b, double* phi,
     }
 }
 
-// Solve A phi = b in moment space with the selected solver; phi holds the initial guess.
+// Solve A phi = b in moment space with the selected solver; phi holds the initial guess.  budget > 0
+// caps the learned path's FGMRES at that many operator applications before plain GMRES takes over.
 static KrylovResult moment_solve(Handle* h, const double* b, double* phi, int solver, int m, double rtol, double atol,
-                                 int maxit, const float* sigl) {
+                                 int maxit, const float* sigl, int budget = 0) {
     const size_t n = (size_t)h->nm * (size_t)h->NENK;
     if (solver == LB_SOLVER_SI) return si_device(h, n, b, phi, rtol, atol, maxit, sigl);
     DevOp mv = [h, sigl](const double* in, double* out) { return apply_A(h, in, out, sigl); };
+    if (solver == LB_SOLVER_FGMRES) {
+        // FGMRES(m) (iters.f:2511-2795) with the caller's per-moment diagonal as right preconditioner
+        if (!h->pdiag.empty() && (int)h->pdiag.size() != h->nm) {
+            KrylovResult bad;
+            bad.status = fail(h, LB_ERR_ARG, "FGMRES: the diagonal preconditioner has another moment count");
+            return bad;
+        }
+        const size_t NENK = (size_t)h->NENK;
+        DevOp pc = [h, NENK, n](const double* in, double* out) {
+            if (h->pdiag.empty()) return k_copy(h, out, in, n);
+            return k_scale_rows(h, out, in, h->pdiag.data(), h->nm, NENK);
+        };
+        return gmres_device(h, n, b, phi, m, rtol, atol, maxit, mv, &pc);
+    }
     if (solver == LB_SOLVER_FGMRES_ML) {
         if (!mlp_ready(h)) {
             // plain GMRES is the fallback when no trained network is loaded
             return gmres_device(h, n, b, phi, m, rtol, atol, maxit, mv, nullptr);
         }
-        // Learned path: FGMRES(m) with the network as right preconditioner, capped at 4m operator
-        // applications when the caller gives no limit.
+        // Learned path: FGMRES(m) with the network as right preconditioner, capped at `budget` operator
+        // applications (plain GMRES's count on this group in calibration), else 4m, and never beyond
+        // the caller's limit.
         DevOp pc = [h](const double* in, double* out) { return mlp_apply_precond(h, in, out); };
-        const int cap = maxit > 0 ? maxit : 4 * m;
+        int cap = budget > 0 ? budget : 4 * m;
+        if (maxit > 0) cap = std::min(cap, maxit);
         KrylovResult kr = gmres_device(h, n, b, phi, m, rtol, atol, cap, mv, &pc);
         if (kr.status != LB_OK && kr.status != LB_ERR_NOCONV && kr.status != LB_ERR_BREAKDOWN &&
             kr.status != LB_ERR_NAN)
@@ -415,11 +432,11 @@ int lb_boltzmann_solve(lb_handle* h, double* s, int solver, int m, double rtol, 
     if (!h || !s) return LB_ERR_ARG;
     int rc = need_ready(h);
     if (rc) return rc;
-    if (solver < 0 || solver > 2) return fail(h, LB_ERR_ARG, "unknown solver");
+    if (solver < 0 || solver > 3) return fail(h, LB_ERR_ARG, "unknown solver");
     if (m < 1) m = 10;
     if (m > 30) return fail(h, LB_ERR_ARG, "restart length must be <= 30");
     cudaSetDevice(h->device);
-    if ((rc = ensure_krylov(h, m, solver == LB_SOLVER_FGMRES_ML))) return rc;
+    if ((rc = ensure_krylov(h, m, solver == LB_SOLVER_FGMRES_ML || solver == LB_SOLVER_FGMRES))) return rc;
     if (!h->d_qext) {
         cudaError_t e = cudaMalloc(&h->d_qext, sizeof(float) * h->psi_elems);
         if (e != cudaSuccess) return cuda_fail(h, e, "angular source buffer");
@@ -437,6 +454,13 @@ int lb_boltzmann_solve(lb_handle* h, double* s, int solver, int m, double rtol, 
     if ((rc = launch_m2d(h, h->d_x, h->d_sigl, nullptr, h->d_qext, h->d_psi))) return rc;
     if ((rc = launch_sweep(h, h->d_psi))) return rc;
     return download_angular(h, h->d_psi, s);
+}
+
+int lb_set_right_precond_diag(lb_handle* h, int nm, const double* d) {
+    if (!h || nm < 0 || nm > kMaxRowCoefs || (nm > 0 && !d)) return h ? fail(h, LB_ERR_ARG, "lb_set_right_precond_diag: bad arguments") : LB_ERR_ARG;
+    if (nm == 0 || !d) h->pdiag.clear();
+    else h->pdiag.assign(d, d + nm);
+    return LB_OK;
 }
 
 int lb_mg_set_problem(lb_handle* h, int G, int Ls, const double* sigt, const double* sigs, const double* dd,
@@ -504,12 +528,12 @@ int lb_mg_update_inputs(lb_handle* h, const double* sigt, const double* sigs, co
 
 int lb_mg_solve(lb_handle* h, int solver, int m, double rtol, double atol, int maxit, int* iters) {
     if (!h || h->device < 0 || h->G < 1 || !h->d_phi_all) return h ? fail(h, LB_ERR_STATE, "lb_mg_solve: problem not set") : LB_ERR_ARG;
-    if (solver < 0 || solver > 2) return fail(h, LB_ERR_ARG, "unknown solver");
+    if (solver < 0 || solver > 3) return fail(h, LB_ERR_ARG, "unknown solver");
     if (m < 1) m = 10;
     if (m > 30) return fail(h, LB_ERR_ARG, "restart length must be <= 30");
     cudaSetDevice(h->device);
     const int G = h->G, Nm = h->Nm;
-    int rc = ensure_krylov(h, m, solver == LB_SOLVER_FGMRES_ML);
+    int rc = ensure_krylov(h, m, solver == LB_SOLVER_FGMRES_ML || solver == LB_SOLVER_FGMRES);
     if (rc) return rc;
     const size_t NENK = (size_t)h->NENK, n = h->kry_n;
     mg_prepare(h);
@@ -518,7 +542,12 @@ int lb_mg_solve(lb_handle* h, int solver, int m, double rtol, double atol, int m
         if ((rc = mg_group_setup(h, g))) break;
         double* phi = h->d_phi_all + (size_t)g * n;
         k_copy(h, phi, h->d_b, n);
-        KrylovResult kr = moment_solve(h, h->d_b, phi, solver, m, rtol, atol, maxit, mg_table(h, g, g));
+        int sv = solver, budget = 0;
+        if (solver == LB_SOLVER_FGMRES_ML) {
+            if (g < (int)h->lp_groups.size() && !h->lp_groups[g]) sv = LB_SOLVER_GMRES;   // gated off for this group
+            if (g < (int)h->lp_budget.size()) budget = h->lp_budget[g];
+        }
+        KrylovResult kr = moment_solve(h, h->d_b, phi, sv, m, rtol, atol, maxit, mg_table(h, g, g), budget);
         if (iters) iters[g] = kr.nmv;
         if ((rc = kr.status)) break;
         k_dose_tally(h, phi, h->d_unc, g == 0 ? 1.0 : 0.0, h->d_dd + (size_t)g * Nm, h->d_mat,
@@ -527,6 +556,46 @@ int lb_mg_solve(lb_handle* h, int solver, int m, double rtol, double atol, int m
     cudaError_t e = cudaStreamSynchronize(h->stream);
     if (!rc && e != cudaSuccess) rc = cuda_fail(h, e, "multigroup solve");
     return rc;
+}
+
+int lb_lp_set_groups(lb_handle* h, int G, const int* enabled, const int* budget) {
+    if (!h || G < 0 || (G > 0 && !enabled)) return h ? fail(h, LB_ERR_ARG, "lb_lp_set_groups: bad arguments") : LB_ERR_ARG;
+    h->lp_groups.assign(G, 1);
+    h->lp_budget.assign(budget ? G : 0, 0);
+    for (int g = 0; g < G; ++g) {
+        h->lp_groups[g] = enabled[g] != 0;
+        if (budget) h->lp_budget[g] = std::max(0, budget[g]);
+    }
+    return LB_OK;
+}
+
+int lb_lp_calibrate(lb_handle* h, int m, double rtol, int* plain_iters, int* learned_iters) {
+    if (!h || h->device < 0 || h->G < 1 || !h->d_phi_all)
+        return h ? fail(h, LB_ERR_STATE, "lb_lp_calibrate: multigroup problem not set") : LB_ERR_ARG;
+    if (!mlp_ready(h)) return fail(h, LB_ERR_STATE, "lb_lp_calibrate: no enabled network");
+    if (m < 1 || m > 30) return fail(h, LB_ERR_ARG, "lb_lp_calibrate: restart length must be in 1..30");
+    cudaSetDevice(h->device);
+    int rc = ensure_krylov(h, m, true);
+    if (rc) return rc;
+    const int G = h->G;
+    const size_t n = h->kry_n;
+    mg_prepare(h);
+    for (int g = 0; g < G; ++g) {
+        if ((rc = mg_group_setup(h, g))) return rc;
+        double* phi = h->d_phi_all + (size_t)g * n;
+        // learned FGMRES from the first-flight moments (its answer is discarded) ...
+        k_copy(h, phi, h->d_b, n);
+        KrylovResult kl = moment_solve(h, h->d_b, phi, LB_SOLVER_FGMRES_ML, m, rtol, 0.0, 0, mg_table(h, g, g));
+        if (kl.status) return kl.status;
+        // ... then plain GMRES, whose answer feeds the groups below
+        k_copy(h, phi, h->d_b, n);
+        KrylovResult kp = moment_solve(h, h->d_b, phi, LB_SOLVER_GMRES, m, rtol, 0.0, 0, mg_table(h, g, g));
+        if (kp.status) return kp.status;
+        if (plain_iters) plain_iters[g] = kp.nmv;
+        if (learned_iters) learned_iters[g] = kl.nmv;
+    }
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    return e == cudaSuccess ? LB_OK : cuda_fail(h, e, "lb_lp_calibrate");
 }
 
 int lb_mg_get_results(lb_handle* h, double* flux, double* dose) {

@@ -364,6 +364,56 @@ __device__ __forceinline__ void update_tab(const SweepArgs& a, float* base, floa
     else *reinterpret_cast<float4*>(base + 4 * (size_t)e) = v;
 }
 
+// update_tab with the element's 16-byte record and its source already loaded (the cluster kernel
+// fetches both for the next element of a block while it updates the current one).
+template <bool kCG>
+__device__ __forceinline__ void update_tab_pre(const SweepArgs& a, float* base, float4 dir, int item, int4 gn, float4 q,
+                                               const float* s_sigt, const float4* s_gtab, const ElemTab* s_tab) {
+    constexpr int F[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
+    const int e = item & 0xFFFFFF;
+    const int upm = (item >> 24) & 0xF;
+    const int outm = (item >> 28) & 0xF;
+    const unsigned nw[4] = {(unsigned)gn.x, (unsigned)gn.y, (unsigned)gn.z, (unsigned)gn.w};
+    const int t = (int)((nw[0] >> 30) | ((nw[1] >> 30) << 2) | ((nw[2] >> 30) << 4) | ((nw[3] >> 30) << 6));
+    const ElemTab* T = s_tab + t;
+    if (outm != __float_as_int(T->s1.y)) {
+        Update u;
+        assemble_g<kCG, true>(base, dir, item, geom_from_rec(gn, s_gtab), s_sigt, u, q);
+        finish<kCG>(base, item, u);
+        return;
+    }
+    const float4 c4 = T->c;
+    const float c[4] = {c4.x, c4.y, c4.z, c4.w};
+    float r[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+        if ((upm >> f) & 1) {
+            const unsigned wd = nw[f];
+            const float4 u4 = ld4<kCG>(base + 4 * (size_t)(wd & 0xFFFFFFu));
+            const float u0 = pick(u4, (wd >> 24) & 3);
+            const float u1 = pick(u4, (wd >> 26) & 3);
+            const float u2 = pick(u4, (wd >> 28) & 3);
+            const float U = u0 + u1 + u2;
+            const float cf = c[f];
+            const float t3 = U * kThird;
+            r[F[f][0]] = fmaf(-cf, fmaf(kFiveThirds, u0, t3), r[F[f][0]]);
+            r[F[f][1]] = fmaf(-cf, fmaf(kFiveThirds, u1, t3), r[F[f][1]]);
+            r[F[f][2]] = fmaf(-cf, fmaf(kFiveThirds, u2, t3), r[F[f][2]]);
+            r[3 - f] = fmaf(cf * kFourThirds, U, r[3 - f]);
+        }
+    }
+    const float4 A = T->a, B = T->b, S0 = T->s0;
+    const float id = T->s1.x;
+    const float v0 = (r[0] + r[1]) + (r[2] + r[3]);
+    const float v1 = fmaf(B.x, r[0], fmaf(B.y, r[1], fmaf(B.z, r[2], B.w * r[3])));
+    const float z0 = fmaf(S0.y, v0, -4.0f * v1) * S0.w;
+    const float z1 = fmaf(S0.x, v1, -S0.z * v0) * S0.w;
+    const float4 v = make_float4((r[0] - fmaf(A.x, z0, z1)) * id, (r[1] - fmaf(A.y, z0, z1)) * id,
+                                 (r[2] - fmaf(A.z, z0, z1)) * id, (r[3] - fmaf(A.w, z0, z1)) * id);
+    if (kCG) __stcg(reinterpret_cast<float4*>(base + 4 * (size_t)e), v);
+    else *reinterpret_cast<float4*>(base + 4 * (size_t)e) = v;
+}
+
 __device__ __forceinline__ void load_sigt(const SweepArgs& a, float* s_sigt) {
     for (int m = threadIdx.x; m < 256; m += blockDim.x) s_sigt[m] = (m < a.Nm) ? a.sigt[m] : 0.f;
     __syncthreads();
@@ -484,7 +534,7 @@ __global__ void __launch_bounds__(1024, MINB) sweep_levels_pf_kernel(SweepArgs a
 // has about a third as many block levels as element levels.  The element update is the level
 // kernel's, so the results are bit-identical.
 // ---------------------------------------------------------------------------------------------
-template <int NT, int MINB, bool TAB>
+template <int NT, int MINB, bool TAB, bool PF>
 __global__ void __launch_bounds__(NT, MINB) sweep_cluster_kernel(SweepArgs a) {
     __shared__ float s_sigt[256];
     extern __shared__ float4 s_gtab_dyn[];
@@ -513,6 +563,45 @@ __global__ void __launch_bounds__(NT, MINB) sweep_cluster_kernel(SweepArgs a) {
                 // slot fields, consumed 16 bits at a time from the low end
                 unsigned long long pk = (unsigned long long)(unsigned)r.y | ((unsigned long long)(unsigned)r.z << 32);
                 unsigned pw = (unsigned)r.w;
+                if (PF && a.ngeom > 0) {
+                    // The next element's record and source do not depend on the current update (the
+                    // block's elements are distinct and only this thread writes them), so they are
+                    // loaded one element ahead: the chain per element keeps only its upstream reads.
+                    unsigned f = (unsigned)(pk & 0xFFFFu);
+                    pk = (pk >> 16) | ((unsigned long long)(pw & 0xFFFFu) << 48);
+                    pw >>= 16;
+                    int e = e0 + (int)(f & 7u);
+                    int4 gn = __ldg(&a.rec[e]);
+                    float4 q = ld4<false>(base + 4 * (size_t)e);
+#pragma unroll 1
+                    for (int k = 0; k < kClusterSize; ++k) {
+                        const unsigned fn = (unsigned)(pk & 0xFFFFu);
+                        pk = (pk >> 16) | ((unsigned long long)(pw & 0xFFFFu) << 48);
+                        pw >>= 16;
+                        const bool more = k + 1 < kClusterSize && (fn & 7u) != 7u;
+                        const int en = e0 + (int)(fn & 7u);
+                        int4 gn_n = gn;
+                        float4 q_n = q;
+                        if (more) {
+                            gn_n = __ldg(&a.rec[en]);
+                            q_n = ld4<false>(base + 4 * (size_t)en);
+                        }
+                        const int item = e | (int)(((f >> 3) & 0xFu) << 24) | (int)(((f >> 7) & 0xFu) << 28);
+                        if (TAB) {
+                            update_tab_pre<false>(a, base, dir, item, gn, q, s_sigt, s_gtab, s_tab);
+                        } else {
+                            Update up;
+                            assemble_g<false, true>(base, dir, item, geom_from_rec(gn, s_gtab), s_sigt, up, q);
+                            finish<false>(base, item, up);
+                        }
+                        if (!more) break;
+                        f = fn;
+                        e = en;
+                        gn = gn_n;
+                        q = q_n;
+                    }
+                    continue;
+                }
 #pragma unroll 1
                 for (int k = 0; k < kClusterSize; ++k) {
                     const unsigned f = (unsigned)(pk & 0xFFFFu);
@@ -880,14 +969,14 @@ struct Config {
                    // 5 blocks of elements (cluster records), 6 the same with per-type element tables
     int threads;
     int dpc;       // directions per CTA (kind 0); minimum CTAs per SM (kinds 2, 5)
-    int ilp;
+    int ilp;       // updates in flight per thread (kind 0); 2 = next element's record and source prefetched (5, 6)
 };
 
 const Config kConfigs[] = {
     {4, 1024, 2, 1}, {4, 512, 2, 1}, {4, 512, 3, 1}, {4, 1024, 3, 1}, {4, 512, 6, 1},
     {0, 1024, 1, 1}, {0, 512, 1, 1}, {2, 1024, 1, 1}, {3, 512, 0, 1}, {1, 256, 0, 0},
     {4, 768, 2, 1}, {0, 1024, 1, 2}, {0, 1024, 1, 3}, {0, 768, 1, 3}, {5, 1024, 1, 1}, {5, 512, 2, 1}, {5, 768, 2, 1}, {5, 1024, 2, 1},
-    {6, 512, 2, 1}, {6, 768, 2, 1},
+    {6, 512, 2, 1}, {6, 768, 2, 1}, {5, 512, 2, 2}, {6, 512, 2, 2},
 };
 constexpr int kNumConfigs = sizeof(kConfigs) / sizeof(kConfigs[0]);
 constexpr int kFinalists = 3;   // candidates timed a second time before one is kept
@@ -961,14 +1050,14 @@ cudaError_t launch_flags(const SweepArgs& a, int sm_count, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-template <int NT, int MINB, bool TAB>
+template <int NT, int MINB, bool TAB, bool PF = false>
 cudaError_t launch_cluster(const SweepArgs& a, int sm_count, cudaStream_t s) {
     const size_t smem = (sizeof(float4) * 3 + (TAB ? sizeof(ElemTab) : 0)) * (size_t)a.ngeom;
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_cluster_kernel<NT, MINB, TAB>, NT, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_cluster_kernel<NT, MINB, TAB, PF>, NT, smem);
     if (per_sm < 1) per_sm = 1;
     int grid = std::min(a.NI, sm_count * per_sm);
-    sweep_cluster_kernel<NT, MINB, TAB><<<grid, NT, smem, s>>>(a);
+    sweep_cluster_kernel<NT, MINB, TAB, PF><<<grid, NT, smem, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -1073,12 +1162,14 @@ int launch_sweep(Handle* h, float* psi) {
         cudaFuncGetAttributes(&fa, sweep_levels_kernel<2, 2>);
         cudaFuncGetAttributes(&fa, sweep_dataflow_kernel);
         cudaFuncGetAttributes(&fa, sweep_group_kernel<2, 768>);
-        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<1024, 1, false>);
-        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<1024, 2, false>);
-        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<768, 2, false>);
-        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2, false>);
-        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2, true>);
-        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<768, 2, true>);
+        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<1024, 1, false, false>);
+        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<1024, 2, false, false>);
+        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<768, 2, false, false>);
+        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2, false, false>);
+        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2, true, false>);
+        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<768, 2, true, false>);
+        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2, false, true>);
+        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2, true, true>);
     }
     Config cfg = kConfigs[cfg_idx];
     // the element-flag schedule keeps one bit per element in shared memory
@@ -1115,6 +1206,9 @@ int launch_sweep(Handle* h, float* psi) {
         e = (cfg.threads == 256) ? launch_flags<256>(a, h->sm_count, h->stream)
           : (cfg.threads == 1024) ? launch_flags<1024>(a, h->sm_count, h->stream)
                                   : launch_flags<512>(a, h->sm_count, h->stream);
+    } else if ((cfg.kind == 5 || cfg.kind == 6) && cfg.ilp == 2) {
+        e = cfg.kind == 6 ? launch_cluster<512, 2, true, true>(a, h->sm_count, h->stream)
+                          : launch_cluster<512, 2, false, true>(a, h->sm_count, h->stream);
     } else if (cfg.kind == 5) {
         if (cfg.threads == 1024) e = cfg.dpc == 2 ? launch_cluster<1024, 2, false>(a, h->sm_count, h->stream)
                                                   : launch_cluster<1024, 1, false>(a, h->sm_count, h->stream);

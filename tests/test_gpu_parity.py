@@ -58,10 +58,10 @@ def test_transport_inverse_matches_oracle(case):
     assert T.timers()["sweep"][1] >= 1
 
 
-@pytest.mark.parametrize("cfg", range(20))
+@pytest.mark.parametrize("cfg", range(22))
 def test_every_sweep_schedule_matches_oracle(cfg, monkeypatch):
     """Each launch candidate of the sweep autotuner (levels, prefetching levels, element flags,
-    grouped directions, dataflow, cluster levels) reproduces the oracle's T^{-1} on a two-material mesh."""
+    grouped directions, dataflow, cluster levels with and without element prefetch) reproduces the oracle's T^{-1} on a two-material mesh."""
     monkeypatch.setenv("LB_SWEEP_CONFIG", str(cfg))
     m, (k, w), sigt, sigs = SWEEP_CASES["two_material"]()
     o, ang, xs = _pair(m, k, w, sigt, sigs)
@@ -73,7 +73,7 @@ def test_every_sweep_schedule_matches_oracle(cfg, monkeypatch):
     assert rel_l2(out, ref) < TOL
 
 
-CLUSTER_CONFIGS = range(14, 20)   # launch candidates of the cluster schedule (plain, type tables)
+CLUSTER_CONFIGS = range(14, 22)   # launch candidates of the cluster schedule (plain, type tables, prefetch)
 
 
 def _sweep_case(m, k, w, sigt, seed):
@@ -215,3 +215,28 @@ def test_gmres_iteration_limit_reports_noconv():
     with pytest.raises(_lib.LionboltError) as ei:
         L.MatInv(q)
     assert ei.value.status == _lib.LB_ERR_NOCONV
+
+
+@pytest.mark.parametrize("m", [5, 20])
+def test_fgmres_pinned_to_sparskit_fgmres(m):
+    """The device FGMRES(m) with a fixed per-moment diagonal right preconditioner (z_j = d_j v_j,
+    d_j = 1 / (1 - 0.6 c g^l)) against the oracle's SPARSKIT fgmres (iters.f:2511-2795) in moment space
+    with the same preconditioner, right-hand side D T^-1 q and initial guess: the same operator
+    count to +-1, across restarts (m = 5), and the same angular flux to 1e-5."""
+    prob = P.config0()
+    mesh = prob.mesh
+    o, ang, xs = _pair(mesh, prob.k, prob.w, prob.sigt[0], prob.sigs[0, 0])
+    q = np.random.default_rng(12).uniform(0, 1, size=mesh.NENK * prob.NI)
+    lofj = np.concatenate([[l] * (2 * l + 1) for l in range(prob.Ls + 1)])
+    d = 1.0 / (1.0 - 0.6 * 0.9 * 0.8 ** lofj)
+    _, psi_ref, info = o.moment_solve(prob.Ls, prob.sigs[0, 0], q=q, m=m, rtol=1e-6, pdiag=d, want_psi=True)
+    assert info["status"] == 0
+    L = BoltzmannOp(m=m, rtol=1e-6, atol=0.0).Build(mesh, ang, xs)
+    L.set_right_precond_diag(d)
+    out = q.copy()
+    L.MatInv(out, solver="FGMRES")
+    assert abs(L.iters - info["iters"]) <= 1, (L.iters, info["iters"])
+    assert rel_l2(out, psi_ref) < TOL
+    # the preconditioner is in effect: plain GMRES takes another number of operator applications
+    _, _, plain = o.moment_solve(prob.Ls, prob.sigs[0, 0], q=q, m=m, rtol=1e-6)
+    assert plain["iters"] != info["iters"]

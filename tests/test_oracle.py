@@ -132,3 +132,93 @@ def test_oracle_gmres_and_si_agree():
     # the GMRES answer satisfies (I - T^-1 K) psi = T^-1 q
     r = o.boltzmann_matvec(xg) - o.transport_inv(q)
     assert np.linalg.norm(r) < 1e-9 * np.linalg.norm(xg)
+
+
+# ---- moment-space restatement (used for the 768k-tet fixture) -------------------------------------
+@pytest.mark.parametrize("case", ["config0", "two_material_jittered"])
+def test_streamed_sweep_is_the_literal_sweep(case):
+    """The natural-order per-direction sweep of the moment-space path gives the literal
+    encode / Sweep / decode result bit for bit, and D is the quadrature sum of Y_j w psi."""
+    from helpers import jittered
+    if case == "config0":
+        m, (k, w), sigt = P.config0().mesh, O.sn_quadrature(4, 8), [0.2]
+    else:
+        m = jittered(P.config1_small(n=(4, 4, 8)).mesh, 0.05)
+        (k, w), sigt = O.sn_quadrature(4, 8), [0.05, 0.4]
+    o = O.Oracle(m)
+    assert o.set_angular(k, w, 3) == 0
+    o.set_xs(sigt, np.zeros((m.Nm, 4)))
+    q = np.random.default_rng(3).uniform(size=m.NENK * k.shape[0])
+    y, psi = o.moment_transport(3, q=q, want_psi=True)
+    assert np.array_equal(psi, o.transport_inv(q))
+    Ysh = np.stack([O.real_sh(3, d) for d in k])
+    assert rel_l2(y, (Ysh * w[:, None]).T @ psi.reshape(k.shape[0], -1)) < 1e-14
+
+
+def test_moment_solve_matches_angular_solve():
+    """config0 (6,000 tets, 80 directions, P3, c = 0.9): the moment-space GMRES and the literal
+    angular-space GMRES of BoltzmannOp%MatInv converge to the same angular flux (<= 1e-10)."""
+    prob = P.config0()
+    m = prob.mesh
+    o = O.Oracle(m)
+    assert o.set_angular(prob.k, prob.w, prob.Ls) == 0
+    o.set_xs(prob.sigt[0], prob.sigs[0, 0])
+    q = np.random.default_rng(4).uniform(size=m.NENK * prob.NI)
+    ref, info = o.boltzmann_solve(q, "GMRES", m=20, rtol=1e-13, atol=0.0)
+    assert info["status"] == 0
+    phi, psi, inf2 = o.moment_solve(prob.Ls, prob.sigs[0, 0], q=q, m=20, rtol=1e-13, want_psi=True)
+    assert inf2["status"] == 0
+    assert rel_l2(psi, ref) < 1e-10
+    assert rel_l2(np.sqrt(4 * np.pi) * phi[0], o.fluence(ref)) < 1e-10
+
+
+def test_moment_multigroup_matches_angular_multigroup():
+    """The moment-space group loop (downscatter sources from resident group moments, beam first-
+    collision source from Y(Omega_b)) against the literal angular-space loop with tapes, on the
+    768k-tet problem's physics (P5, 2 materials, 4 groups) on a 6 x 6 x 12-hex box: <= 1e-10."""
+    prob = P.config1_small(n=(6, 6, 12), G=4, Ng=6, Nc=12)
+    o = O.Oracle(prob.mesh)
+    assert o.set_angular(prob.k, prob.w, prob.Ls) == 0
+    flux_ref, dose_ref, _ = o.multigroup(prob, "GMRES", m=20, rtol=1e-13)
+    r = o.mg_moment(prob, m=20, rtol=1e-13, rtol_snap=1e-6)
+    assert rel_l2(r["dose"], dose_ref) < 1e-10
+    for g in range(prob.G):
+        assert rel_l2(r["flux"][g], flux_ref[g]) < 1e-10, g
+    # the 1e-6 snapshots are 1e-6 solves of the same groups: close, not equal, and cheaper
+    assert 0 < rel_l2(r["dose_snap"], r["dose"]) < 1e-4
+    assert np.all(r["iters_snap"] < r["iters"])
+
+
+def test_dgemv_scattering_path_matches_loop_path():
+    """The per-node dgemv loop of ScatteringAlgebra.f90:39-48 through the bundled OpenBLAS equals
+    the oracle's own per-node loop, on all nodes and on a node range (other nodes untouched)."""
+    prob = P.config1_small(n=(2, 2, 4))
+    o = O.Oracle(prob.mesh)
+    assert o.set_angular_no_schedule(prob.k, prob.w, prob.Ls) == 0
+    o.set_xs(prob.sigt[0], prob.sigs[0, 0])
+    x = np.random.default_rng(8).normal(size=prob.mesh.NENK * prob.NI)
+    ref = o.scatter_apply(x)
+    assert rel_l2(o.scatter_apply_dgemv(x), ref) < 1e-14
+    n = prob.mesh.NENK
+    part = o.scatter_apply_dgemv(x, 40, 100).reshape(prob.NI, n)
+    xr, rr = x.reshape(prob.NI, n), ref.reshape(prob.NI, n)
+    assert rel_l2(part[:, 40:100], rr[:, 40:100]) < 1e-14
+    assert np.array_equal(part[:, :40], xr[:, :40]) and np.array_equal(part[:, 100:], xr[:, 100:])
+
+
+def test_moment_fgmres_with_diagonal_preconditioner():
+    """SPARSKIT fgmres (iters.f:2511-2795) in moment space with a fixed per-moment right
+    preconditioner z_j = d_j v_j (d_j = 1 / (1 - 0.6 c g^l)) reaches the GMRES answer, across
+    restarts (m = 5), along another iteration path."""
+    prob = P.config0()
+    o = O.Oracle(prob.mesh)
+    assert o.set_angular_streamed(prob.k, prob.w) == 0
+    o.set_sigt(prob.sigt[0])
+    q = np.random.default_rng(6).uniform(size=prob.mesh.NENK * prob.NI)
+    lofj = np.concatenate([[l] * (2 * l + 1) for l in range(prob.Ls + 1)])
+    d = 1.0 / (1.0 - 0.6 * 0.9 * 0.8 ** lofj)
+    phi_g, _, ig = o.moment_solve(prob.Ls, prob.sigs[0, 0], q=q, m=5, rtol=1e-11)
+    phi_f, _, inf = o.moment_solve(prob.Ls, prob.sigs[0, 0], q=q, m=5, rtol=1e-11, pdiag=d)
+    assert ig["status"] == 0 and inf["status"] == 0
+    assert rel_l2(phi_f, phi_g) < 1e-9
+    assert inf["iters"] != ig["iters"]
