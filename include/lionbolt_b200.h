@@ -196,15 +196,23 @@ int lb_mesh_types(lb_handle* h, int* ntypes);
  * rotation (c, s) taking (x, y) to (r, 0); x or y NaN gives c = 1, s = 0, r = 0.  Diagnostic. */
 int lb_givens(double x, double y, double* c, double* s, double* r);
 
-/* Block schedule of the sweep (schedule 5): the mesh's elements in blocks of 6 consecutive ids (a hex of
- * a box mesh split into 6 tets), swept as units over each direction's block-level graph.  Built by
- * lb_set_quadrature when every direction's block graph is acyclic.  lb_cluster_info: *nblocks = number
- * of blocks (0: no block schedule), *max_levels = largest block-level count of a direction.
- * lb_get_cluster_schedule: rec[NI][nblocks][4] block records in execution order (x = block index;
- * y, z, w = two 16-bit slots each in execution order: element offset in the block (3 b, 7 = empty),
- * upstream-face mask << 3, outflow-face mask << 7), starts[NI][nblocks + 1] block-level starts,
- * nlevels[NI].  Diagnostics for tests; no counterpart in the reference. */
+/* Block schedule of the sweep (schedules 5 and 6): blocks of up to 6 face-connected elements swept as
+ * units over each direction's block-level graph.  Blocks are 6 consecutive element ids when those are
+ * face-connected (a hex of a box mesh split into 6 tets); otherwise they are grown greedily from face
+ * neighbours.  A direction whose block graph has a cycle sweeps the blocks on the cycle element by
+ * element (one record per element), so every sweepable mesh has a block schedule and record counts
+ * differ between directions.  Built by lb_set_quadrature.
+ *   lb_cluster_info: *nblocks = number of blocks (0: no block schedule), *max_levels = largest
+ *     block-level count of a direction.
+ *   lb_cluster_layout: rec_base[NI + 1] = offset of each direction's records, blk_elem[nblocks][6]
+ *     (optional) = block members (-1: empty), *max_records = largest record count of a direction.
+ *   lb_get_cluster_schedule: rec[rec_base[NI]][4] records in execution order (x = block index; y, z, w =
+ *     two 16-bit slots each in execution order: member position in the block (3 b, 7 = empty),
+ *     upstream-face mask << 3, outflow-face mask << 7), starts[NI][max_records + 1] block-level
+ *     starts (relative to rec_base[i]), nlevels[NI].
+ * Diagnostics for tests; no counterpart in the reference. */
 int lb_cluster_info(lb_handle* h, int* nblocks, int* max_levels);
+int lb_cluster_layout(lb_handle* h, long long* rec_base, int* blk_elem, int* max_records);
 int lb_get_cluster_schedule(lb_handle* h, int* rec, int* starts, int* nlevels);
 
 

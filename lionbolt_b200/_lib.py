@@ -70,6 +70,7 @@ SIGNATURES = {
     "lb_lp_calibrate": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, _c_int_p, _c_int_p]),
     "lb_givens": (ctypes.c_int, [ctypes.c_double, ctypes.c_double, _c_double_p, _c_double_p, _c_double_p]),
     "lb_cluster_info": (ctypes.c_int, [_vp, _c_int_p, _c_int_p]),
+    "lb_cluster_layout": (ctypes.c_int, [_vp, _c_ll_p, _c_int_p, _c_int_p]),
     "lb_get_cluster_schedule": (ctypes.c_int, [_vp, _c_int_p, _c_int_p, _c_int_p]),
     "lb_mg_update_inputs": (ctypes.c_int, [_vp, _c_double_p, _c_double_p, _c_double_p, _c_double_p, _c_double_p]),
     "lb_mark": (ctypes.c_int, [_vp, ctypes.c_int]),

@@ -96,7 +96,8 @@ int build_work(lb_batch* b, const std::vector<int>& ids, int threads) {
             double c = 0.0;
             if (h->nclusters > 0) {
                 // block schedule: block levels, one thread per block of kClusterSize elements
-                x.crec = h->d_crec + (size_t)i * h->nclusters;
+                x.crec = h->d_crec + h->crec_base_h[i];
+                x.blk_elem = h->d_blk_elem;
                 x.cl_start = h->d_cl_start + h->cl_base_h[i];
                 x.ncl = h->ncl_h[i];
                 if (h->ngeom > 0) {

@@ -123,7 +123,7 @@ static int dev_upload(Handle* h, T** p, const T* src, size_t count, const char* 
 }
 
 static void free_all(Handle* h) {
-    void* ptrs[] = {h->d_geom, h->d_rec, h->d_crec, h->d_cl_start, h->d_cl_base, h->d_ncl, h->d_gtab, h->d_tmat, h->d_mat, h->d_items, h->d_groups, h->d_pitems, h->d_pbase, h->d_chunks, h->d_lvl_start, h->d_lvl_base, h->d_nlev, h->d_done, h->d_status, h->d_dirs, h->d_sigt,
+    void* ptrs[] = {h->d_geom, h->d_rec, h->d_crec, h->d_crec_base, h->d_blk_elem, h->d_cl_start, h->d_cl_base, h->d_ncl, h->d_gtab, h->d_tmat, h->d_mat, h->d_items, h->d_groups, h->d_pitems, h->d_pbase, h->d_chunks, h->d_lvl_start, h->d_lvl_base, h->d_nlev, h->d_done, h->d_status, h->d_dirs, h->d_sigt,
                     h->d_psi, h->d_qext, h->d_Ym2d, h->d_Yd2m, h->d_sigl, h->d_lofj, h->d_V, h->d_Z, h->d_x,
                     h->d_b, h->d_t, h->d_red, h->d_unc, h->d_phi_all, h->d_src, h->d_dose, h->d_flux,
                     h->d_sigl_mg, h->d_yb, h->d_dd};
@@ -463,31 +463,143 @@ int lb_set_mesh(lb_handle* h, int NE, int NN, const double* rg, const int* node,
 //   block (3 b, 7 = empty) | upstream-face mask << 3 | outflow-face mask << 7.
 // Built on device handles; when some direction's block graph has a cycle no cluster schedule is
 // kept and the sweep uses the element schedules.
+// Blocks of the cluster schedule.  Box meshes number the 6 tets of a hex consecutively, so blocks of
+// kClusterSize consecutive ids are face-connected and need no member table (blk_elem stays empty).
+// Other meshes get blocks grown greedily: elements are visited in Morton order of their centroids, and
+// a block grows from its first element by the unassigned face neighbour sharing the most faces with
+// the block's members (then the earliest in Morton order), up to kClusterSize elements.
+static void form_blocks(Handle* h, std::vector<int>& blk_elem, std::vector<int>& blk_of, std::vector<int>& blk_pos) {
+    constexpr int K = kClusterSize;
+    const int NE = h->NE;
+    blk_elem.clear();
+    blk_of.assign(NE, 0);
+    blk_pos.assign(NE, 0);
+    bool consecutive = true;
+    for (int b0 = 0; b0 < NE && consecutive; b0 += K) {
+        const int n = std::min(K, NE - b0);
+        // face-connected: a flood fill from the first member reaches all n
+        int reached = 1, mask = 1;
+        for (bool grew = true; grew;) {
+            grew = false;
+            for (int q = 0; q < n; ++q) {
+                if (!((mask >> q) & 1)) continue;
+                for (int f = 0; f < 4; ++f) {
+                    const int ep = h->nbr[(size_t)(b0 + q) * 4 + f] - b0;
+                    if (ep >= 0 && ep < n && !((mask >> ep) & 1)) { mask |= 1 << ep; ++reached; grew = true; }
+                }
+            }
+        }
+        consecutive = reached == n;
+    }
+    if (consecutive) {
+        for (int e = 0; e < NE; ++e) { blk_of[e] = e / K; blk_pos[e] = e % K; }
+        return;
+    }
+    // Morton order of the centroids (21 bits per axis)
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int v = 0; v < h->NN; ++v)
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = std::min(lo[d], h->rg[(size_t)v * 3 + d]);
+            hi[d] = std::max(hi[d], h->rg[(size_t)v * 3 + d]);
+        }
+    auto spread = [](uint64_t x) {
+        x &= 0x1FFFFF;
+        x = (x | x << 32) & 0x1F00000000FFFFull;
+        x = (x | x << 16) & 0x1F0000FF0000FFull;
+        x = (x | x << 8) & 0x100F00F00F00F00Full;
+        x = (x | x << 4) & 0x10C30C30C30C30C3ull;
+        x = (x | x << 2) & 0x1249249249249249ull;
+        return x;
+    };
+    std::vector<std::pair<uint64_t, int>> key(NE);
+    for (int e = 0; e < NE; ++e) {
+        uint64_t code = 0;
+        for (int d = 0; d < 3; ++d) {
+            double c = 0.0;
+            for (int k = 0; k < 4; ++k) c += h->rg[(size_t)h->node[(size_t)e * 4 + k] * 3 + d];
+            const double t = (0.25 * c - lo[d]) / std::max(hi[d] - lo[d], 1e-300);
+            code |= spread((uint64_t)std::min(2097151.0, std::max(0.0, t * 2097151.0))) << d;
+        }
+        key[e] = {code, e};
+    }
+    std::sort(key.begin(), key.end());
+    std::vector<int> rank(NE);
+    for (int q = 0; q < NE; ++q) rank[key[q].second] = q;
+    std::vector<int> owner(NE, -1), members;
+    int nb = 0;
+    for (int q = 0; q < NE; ++q) {
+        const int seed = key[q].second;
+        if (owner[seed] >= 0) continue;
+        members.assign(1, seed);
+        owner[seed] = nb;
+        while ((int)members.size() < K) {
+            int best = -1, best_shared = 0;
+            for (int m : members)
+                for (int f = 0; f < 4; ++f) {
+                    const int c = h->nbr[(size_t)m * 4 + f];
+                    if (c < 0 || owner[c] >= 0) continue;
+                    int shared = 0;
+                    for (int g = 0; g < 4; ++g) {
+                        const int cn = h->nbr[(size_t)c * 4 + g];
+                        shared += cn >= 0 && owner[cn] == nb;
+                    }
+                    if (best < 0 || shared > best_shared || (shared == best_shared && rank[c] < rank[best])) {
+                        best = c;
+                        best_shared = shared;
+                    }
+                }
+            if (best < 0) break;
+            owner[best] = nb;
+            members.push_back(best);
+        }
+        for (int k = 0; k < K; ++k) blk_elem.push_back(k < (int)members.size() ? members[k] : -1);
+        for (int k = 0; k < (int)members.size(); ++k) { blk_of[members[k]] = nb; blk_pos[members[k]] = k; }
+        ++nb;
+    }
+}
+
+// Block schedule of every direction: units on levels.  A unit is a block, or part of one: Kahn's
+// algorithm runs over the units of the direction, and whenever no unit is ready while elements remain
+// (the direction's block graph has a cycle), every element whose upstream neighbours are all done
+// leaves its unit for a new unit with the other such elements of its block.  Those elements are
+// mutually independent, so the new unit is valid and ready, and the sweep always progresses.  A record
+// per unit: the block index, then up to kClusterSize 16-bit slots in execution order (position in the
+// block, upstream-face mask << 3, outflow-face mask << 7; position 7 = empty slot), the unit's elements
+// ordered by element level.
 static int build_cluster_schedule(Handle* h) {
     constexpr int K = kClusterSize;
     h->nclusters = 0;
     h->max_cluster_levels = 0;
+    h->max_cluster_records = 0;
     h->cl_start_h.clear();
     h->crec_h.clear();
     h->cl_base_h.clear();
     h->ncl_h.clear();
-    for (void** p : {(void**)&h->d_crec, (void**)&h->d_cl_start, (void**)&h->d_cl_base, (void**)&h->d_ncl})
+    h->crec_base_h.clear();
+    h->blk_elem_h.clear();
+    for (void** p : {(void**)&h->d_crec, (void**)&h->d_cl_start, (void**)&h->d_cl_base, (void**)&h->d_ncl,
+                     (void**)&h->d_crec_base, (void**)&h->d_blk_elem})
         if (*p) {
             cudaFree(*p);
             *p = nullptr;
         }
     const int NE = h->NE, NI = h->NI;
     if (NE < K) return LB_OK;
-    const int NC = (NE + K - 1) / K;
-    std::vector<int4> crec((size_t)NI * NC);
+    std::vector<int> blk_elem, blk_of, blk_pos;
+    form_blocks(h, blk_elem, blk_of, blk_pos);
+    const int NC = blk_elem.empty() ? (NE + K - 1) / K : (int)(blk_elem.size() / K);
+    std::vector<std::vector<int4>> crec(NI);
     std::vector<std::vector<int>> cstart(NI);
     bool cyclic = false;
 #pragma omp parallel reduction(|| : cyclic)
     {
-        std::vector<int> lev(NE), indeg(NC), ostart(NC + 1), odst, fill(NC), cur, nxt, members, ord;
+        std::vector<int> lev(NE), unit(NE), ublk, pend, epend, dstart(NE + 1), ddst, cur, nxt, members, ord, waiting;
+        std::vector<int> usize, newunit;
+        std::vector<char> done(NE);
         std::vector<uint16_t> fld(NE);
         std::vector<unsigned long long> key;
         std::vector<int4> tmp;
+        std::vector<std::vector<int>> umem;
 #pragma omp for schedule(dynamic, 1)
         for (int i = 0; i < NI; ++i) {
             if (cyclic) continue;
@@ -497,93 +609,146 @@ static int build_cluster_schedule(Handle* h) {
                 for (int es = st[L]; es < st[L + 1]; ++es) lev[it[es] & 0xFFFFFF] = L;
             for (int es = 0; es < NE; ++es) {
                 const int e = it[es] & 0xFFFFFF;
-                fld[e] = (uint16_t)((e % K) | (((it[es] >> 24) & 0xF) << 3) | (((it[es] >> 28) & 0xF) << 7));
+                fld[e] = (uint16_t)(blk_pos[e] | (((it[es] >> 24) & 0xF) << 3) | (((it[es] >> 28) & 0xF) << 7));
             }
-            // block edges A -> B, one per cross-block upstream face (duplicates are harmless)
-            std::fill(ostart.begin(), ostart.end(), 0);
-            std::fill(indeg.begin(), indeg.end(), 0);
-            for (int e = 0; e < NE; ++e) {
-                const int upm = (fld[e] >> 3) & 0xF;
+            // element edges y -> x (y upstream of x), as downstream lists
+            std::fill(dstart.begin(), dstart.end(), 0);
+            epend.assign(NE, 0);
+            for (int x = 0; x < NE; ++x) {
+                const int upm = (fld[x] >> 3) & 0xF;
                 for (int f = 0; f < 4; ++f)
-                    if ((upm >> f) & 1) {
-                        const int a = h->nbr[(size_t)e * 4 + f] / K, b = e / K;
-                        if (a != b) {
-                            ++ostart[a + 1];
-                            ++indeg[b];
-                        }
-                    }
+                    if ((upm >> f) & 1) { ++dstart[h->nbr[(size_t)x * 4 + f] + 1]; ++epend[x]; }
             }
-            for (int c = 0; c < NC; ++c) ostart[c + 1] += ostart[c];
-            odst.resize(ostart[NC]);
-            for (int c = 0; c < NC; ++c) fill[c] = ostart[c];
-            for (int e = 0; e < NE; ++e) {
-                const int upm = (fld[e] >> 3) & 0xF;
-                for (int f = 0; f < 4; ++f)
-                    if ((upm >> f) & 1) {
-                        const int a = h->nbr[(size_t)e * 4 + f] / K, b = e / K;
-                        if (a != b) odst[fill[a]++] = b;
-                    }
+            for (int e = 0; e < NE; ++e) dstart[e + 1] += dstart[e];
+            ddst.resize(dstart[NE]);
+            {
+                std::vector<int> fill(dstart.begin(), dstart.end() - 1);
+                for (int x = 0; x < NE; ++x) {
+                    const int upm = (fld[x] >> 3) & 0xF;
+                    for (int f = 0; f < 4; ++f)
+                        if ((upm >> f) & 1) ddst[fill[h->nbr[(size_t)x * 4 + f]]++] = x;
+                }
             }
-            // longest-path levels (Kahn, level by level)
+            // units start as the blocks; pend[u] = edges into u from elements of other, unfinished units
+            ublk.resize(NC);
+            umem.assign(NC, {});
+            for (int c = 0; c < NC; ++c) ublk[c] = c;
+            for (int e = 0; e < NE; ++e) { unit[e] = blk_of[e]; umem[unit[e]].push_back(e); done[e] = 0; }
+            pend.assign(NC, 0);
+            for (int y = 0; y < NE; ++y)
+                for (int j = dstart[y]; j < dstart[y + 1]; ++j)
+                    if (unit[ddst[j]] != unit[y]) ++pend[unit[ddst[j]]];
             cur.clear();
+            waiting.clear();
             for (int c = 0; c < NC; ++c)
-                if (indeg[c] == 0) cur.push_back(c);
-            int4* out = crec.data() + (size_t)i * NC;
-            int pos = 0;
+                if (pend[c] == 0 && !umem[c].empty()) cur.push_back(c);
+            for (int e = 0; e < NE; ++e)
+                if (epend[e] == 0 && pend[unit[e]] > 0) waiting.push_back(e);
+            std::vector<int4>& out = crec[i];
+            out.clear();
             cstart[i].clear();
-            while (!cur.empty()) {
-                cstart[i].push_back(pos);
+            int ndone = 0;
+            while (ndone < NE) {
+                if (cur.empty()) {
+                    // stalled on a cycle of units: the ready elements of every blocked unit form new units
+                    newunit.clear();
+                    std::sort(waiting.begin(), waiting.end(), [&](int x, int y) { return unit[x] < unit[y]; });
+                    for (size_t q = 0; q < waiting.size();) {
+                        const int u = unit[waiting[q]];
+                        size_t r = q;
+                        while (r < waiting.size() && unit[waiting[r]] == u) ++r;
+                        const int nu = (int)umem.size();
+                        umem.emplace_back(waiting.begin() + q, waiting.begin() + r);
+                        ublk.push_back(ublk[u]);
+                        pend.push_back(0);
+                        for (size_t t = q; t < r; ++t) unit[waiting[t]] = nu;
+                        std::vector<int>& m0 = umem[u];
+                        m0.erase(std::remove_if(m0.begin(), m0.end(), [&](int x) { return unit[x] == nu; }), m0.end());
+                        // edges from the moved elements to the rest of their old unit now cross units
+                        for (size_t t = q; t < r; ++t)
+                            for (int j = dstart[waiting[t]]; j < dstart[waiting[t] + 1]; ++j)
+                                if (unit[ddst[j]] == u) ++pend[u];
+                        newunit.push_back(nu);
+                        q = r;
+                    }
+                    waiting.clear();
+                    if (newunit.empty()) break;   // an element-level cycle: no block schedule
+                    cur.swap(newunit);
+                }
+                cstart[i].push_back((int)out.size());
                 const int n = (int)cur.size();
                 tmp.resize(n);
                 key.resize(n);
                 for (int q = 0; q < n; ++q) {
                     const int c = cur[q];
-                    members.clear();
-                    for (int e = c * K; e < std::min(NE, c * K + K); ++e) members.push_back(e);
+                    members = umem[c];
                     std::sort(members.begin(), members.end(),
                               [&](int x, int y) { return lev[x] != lev[y] ? lev[x] < lev[y] : x < y; });
                     uint32_t sl[6];
                     for (int k = 0; k < 6; ++k) sl[k] = k < (int)members.size() ? fld[members[k]] : 7u;
-                    tmp[q] = make_int4(c, (int)(sl[0] | (sl[1] << 16)), (int)(sl[2] | (sl[3] << 16)),
+                    tmp[q] = make_int4(ublk[c], (int)(sl[0] | (sl[1] << 16)), (int)(sl[2] | (sl[3] << 16)),
                                        (int)(sl[4] | (sl[5] << 16)));
                     key[q] = ((unsigned long long)(uint32_t)tmp[q].y * 0x9E3779B97F4A7C15ull) ^
                              ((unsigned long long)(uint32_t)tmp[q].z << 21) ^ (uint32_t)tmp[q].w;
                 }
-                // blocks with equal patterns next to each other (a warp then runs one element sequence)
+                // units with equal patterns next to each other (a warp then runs one element sequence)
                 ord.resize(n);
                 for (int q = 0; q < n; ++q) ord[q] = q;
                 std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return key[x] < key[y]; });
-                for (int q = 0; q < n; ++q) out[pos + q] = tmp[ord[q]];
-                pos += n;
+                for (int q = 0; q < n; ++q) out.push_back(tmp[ord[q]]);
                 nxt.clear();
                 for (int c : cur)
-                    for (int j = ostart[c]; j < ostart[c + 1]; ++j)
-                        if (--indeg[odst[j]] == 0) nxt.push_back(odst[j]);
+                    for (int y : umem[c]) {
+                        done[y] = 1;
+                        ++ndone;
+                    }
+                for (int c : cur)
+                    for (int y : umem[c])
+                        for (int j = dstart[y]; j < dstart[y + 1]; ++j) {
+                            const int x = ddst[j];
+                            const int ux = unit[x];
+                            if (ux != c && --pend[ux] == 0) nxt.push_back(ux);
+                            if (--epend[x] == 0 && !done[x]) waiting.push_back(x);
+                        }
+                // elements whose units became ready do not wait
+                waiting.erase(std::remove_if(waiting.begin(), waiting.end(), [&](int x) { return pend[unit[x]] == 0; }),
+                              waiting.end());
                 cur.swap(nxt);
             }
-            cstart[i].push_back(pos);
-            if (pos != NC) cyclic = true;
+            cstart[i].push_back((int)out.size());
+            if (ndone != NE) cyclic = true;   // an element-level cycle: no block schedule
         }
     }
     if (cyclic) return LB_OK;
     std::vector<int> cl_start, cl_base(NI), ncl(NI);
-    int maxl = 0;
+    std::vector<long long> base(NI + 1, 0);
+    int maxl = 0, maxr = 0;
     for (int i = 0; i < NI; ++i) {
         cl_base[i] = (int)cl_start.size();
         ncl[i] = (int)cstart[i].size() - 1;
         maxl = std::max(maxl, ncl[i]);
+        maxr = std::max(maxr, (int)crec[i].size());
         cl_start.insert(cl_start.end(), cstart[i].begin(), cstart[i].end());
+        base[i + 1] = base[i] + (long long)crec[i].size();
     }
-    int rc = dev_upload(h, &h->d_crec, crec.data(), crec.size(), "upload cluster records");
+    std::vector<int4> all((size_t)base[NI]);
+    for (int i = 0; i < NI; ++i) std::copy(crec[i].begin(), crec[i].end(), all.begin() + base[i]);
+    crec.clear();
+    int rc = dev_upload(h, &h->d_crec, all.data(), all.size(), "upload cluster records");
+    if (!rc) rc = dev_upload(h, &h->d_crec_base, base.data(), base.size(), "upload cluster record offsets");
+    if (!rc && !blk_elem.empty()) rc = dev_upload(h, &h->d_blk_elem, blk_elem.data(), blk_elem.size(), "upload blocks");
     if (!rc) rc = dev_upload(h, &h->d_cl_start, cl_start.data(), cl_start.size(), "upload cluster levels");
     if (!rc) rc = dev_upload(h, &h->d_cl_base, cl_base.data(), cl_base.size(), "upload cluster level offsets");
     if (!rc) rc = dev_upload(h, &h->d_ncl, ncl.data(), ncl.size(), "upload cluster level counts");
     if (rc) return rc;
     h->nclusters = NC;
     h->max_cluster_levels = maxl;
+    h->max_cluster_records = maxr;
     h->cl_start_h = cl_start;
     h->cl_base_h = cl_base;
-    if (h->device < 0) h->crec_h = std::move(crec);   // host-only handles keep the records for queries
+    h->crec_base_h = base;
+    h->blk_elem_h = blk_elem;
+    if (h->device < 0) h->crec_h = std::move(all);   // host-only handles keep the records for queries
     h->ncl_h = ncl;
     return LB_OK;
 }
@@ -901,11 +1066,26 @@ int lb_cluster_info(lb_handle* h, int* nblocks, int* max_levels) {
     return LB_OK;
 }
 
+int lb_cluster_layout(lb_handle* h, long long* rec_base, int* blk_elem, int* max_records) {
+    if (!h || !rec_base || !max_records) return LB_ERR_ARG;
+    if (!h->angle_ready) return fail(h, LB_ERR_STATE, "lb_cluster_layout: quadrature not set");
+    if (h->nclusters <= 0) return fail(h, LB_ERR_STATE, "lb_cluster_layout: the mesh has no block schedule");
+    std::copy(h->crec_base_h.begin(), h->crec_base_h.end(), rec_base);
+    *max_records = h->max_cluster_records;
+    if (blk_elem) {
+        if (h->blk_elem_h.empty())
+            for (int q = 0; q < h->nclusters * kClusterSize; ++q) blk_elem[q] = q < h->NE ? q : -1;
+        else
+            std::copy(h->blk_elem_h.begin(), h->blk_elem_h.end(), blk_elem);
+    }
+    return LB_OK;
+}
+
 int lb_get_cluster_schedule(lb_handle* h, int* rec, int* starts, int* nlevels) {
     if (!h || !rec || !starts || !nlevels) return LB_ERR_ARG;
     if (!h->angle_ready) return fail(h, LB_ERR_STATE, "lb_get_cluster_schedule: quadrature not set");
     if (h->nclusters <= 0) return fail(h, LB_ERR_STATE, "lb_get_cluster_schedule: the mesh has no block schedule");
-    const size_t n = (size_t)h->NI * h->nclusters;
+    const size_t n = (size_t)h->crec_base_h[h->NI];
     if (h->device < 0) {
         std::memcpy(rec, h->crec_h.data(), sizeof(int4) * n);
     } else {
@@ -913,9 +1093,10 @@ int lb_get_cluster_schedule(lb_handle* h, int* rec, int* starts, int* nlevels) {
         cudaError_t e = cudaMemcpy(rec, h->d_crec, sizeof(int4) * n, cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) return cuda_fail(h, e, "lb_get_cluster_schedule");
     }
+    const size_t ld = (size_t)h->max_cluster_records + 1;
     for (int i = 0; i < h->NI; ++i) {
         nlevels[i] = h->ncl_h[i];
-        for (int L = 0; L <= h->ncl_h[i]; ++L) starts[(size_t)i * (h->nclusters + 1) + L] = h->cl_start_h[h->cl_base_h[i] + L];
+        for (int L = 0; L <= h->ncl_h[i]; ++L) starts[(size_t)i * ld + L] = h->cl_start_h[h->cl_base_h[i] + L];
     }
     return LB_OK;
 }

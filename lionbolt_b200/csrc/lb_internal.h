@@ -95,8 +95,17 @@ struct Handle {
     float4* d_gtab = nullptr;      // [ngeom][3] (snx, sny, snz)
     int* d_tmat = nullptr;         // [ngeom] material of each type
     int ngeom = 0;                 // number of types; 0: no table (use d_geom)
-    // cluster schedule: blocks of kClusterSize consecutive elements swept as units (0 blocks: none)
-    int4* d_crec = nullptr;        // [NI][nclusters] block records in block-level order
+    // cluster schedule: blocks of up to kClusterSize face-connected elements swept as units (0 blocks:
+    // none).  Blocks are kClusterSize consecutive ids when those are face-connected (box meshes: one hex
+    // each); otherwise they are grown greedily from face neighbours and listed in blk_elem.  A direction
+    // sweeps "units": whole blocks, except blocks on a dependency cycle of that direction's block graph,
+    // which are split into single elements, so the number of records differs between directions.
+    int4* d_crec = nullptr;        // block records in block-level order, direction i's from crec_base[i]
+    long long* d_crec_base = nullptr;   // [NI + 1]
+    int* d_blk_elem = nullptr;     // [nclusters][kClusterSize] members (-1: empty); null for consecutive ids
+    std::vector<long long> crec_base_h;
+    std::vector<int> blk_elem_h;
+    int max_cluster_records = 0;   // largest record count of a direction
     int* d_cl_start = nullptr;     // block-level starts, per direction (ncl[i] + 1 entries)
     int* d_cl_base = nullptr;      // [NI] offset of direction i's starts in d_cl_start
     int* d_ncl = nullptr;          // [NI] block levels per direction
@@ -240,6 +249,7 @@ struct BatchWork {
     int problem;
     int ngeom;              // element types of the problem (0: no type table)
     const int4* crec;       // the direction's block records (nullptr: element schedule)
+    const int* blk_elem;    // the problem's block members (nullptr: blocks of consecutive ids)
     const int* cl_start;    // [ncl + 1] block-level starts of the direction
     const int4* rec;        // the problem's 16-byte element records (type table)
     const float4* gtab;     // [ngeom][3] face vectors of the types

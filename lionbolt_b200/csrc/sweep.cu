@@ -69,7 +69,9 @@ struct SweepArgs {
     const float4* __restrict__ gtab;  // [ngeom][3] face vectors of the element types
     const int* __restrict__ tmat;     // [ngeom] material of the element types
     int ngeom;
-    const int4* __restrict__ crec;    // [NI][nclusters] block records (cluster schedule)
+    const int4* __restrict__ crec;    // block records (cluster schedule), direction i's from crec_base[i]
+    const long long* __restrict__ crec_base;
+    const int* __restrict__ blk_elem; // [nclusters][kClusterSize] block members, or null: consecutive ids
     const int* __restrict__ cl_start;
     const int* __restrict__ cl_base;
     const int* __restrict__ ncl;
@@ -551,7 +553,7 @@ __global__ void __launch_bounds__(NT, MINB) sweep_cluster_kernel(SweepArgs a) {
             build_tab(s_gtab, s_sigt, a.ngeom, dir, s_tab);
             __syncthreads();
         }
-        const int4* rec = a.crec + (size_t)i * a.nclusters;
+        const int4* rec = a.crec + __ldg(&a.crec_base[i]);
         float* base = a.psi + (size_t)i * (size_t)a.NENK;
         int s1 = __ldg(&ls[0]);
         for (int L = 0; L < nl; ++L) {
@@ -560,6 +562,7 @@ __global__ void __launch_bounds__(NT, MINB) sweep_cluster_kernel(SweepArgs a) {
             for (int cs = s0 + threadIdx.x; cs < s1; cs += nt) {
                 const int4 r = __ldcs(rec + cs);
                 const int e0 = r.x * kClusterSize;
+                const int* mem = a.blk_elem ? a.blk_elem + e0 : nullptr;   // the block's members
                 // slot fields, consumed 16 bits at a time from the low end
                 unsigned long long pk = (unsigned long long)(unsigned)r.y | ((unsigned long long)(unsigned)r.z << 32);
                 unsigned pw = (unsigned)r.w;
@@ -570,7 +573,7 @@ __global__ void __launch_bounds__(NT, MINB) sweep_cluster_kernel(SweepArgs a) {
                     unsigned f = (unsigned)(pk & 0xFFFFu);
                     pk = (pk >> 16) | ((unsigned long long)(pw & 0xFFFFu) << 48);
                     pw >>= 16;
-                    int e = e0 + (int)(f & 7u);
+                    int e = mem ? __ldg(&mem[f & 7u]) : e0 + (int)(f & 7u);
                     int4 gn = __ldg(&a.rec[e]);
                     float4 q = ld4<false>(base + 4 * (size_t)e);
 #pragma unroll 1
@@ -579,7 +582,7 @@ __global__ void __launch_bounds__(NT, MINB) sweep_cluster_kernel(SweepArgs a) {
                         pk = (pk >> 16) | ((unsigned long long)(pw & 0xFFFFu) << 48);
                         pw >>= 16;
                         const bool more = k + 1 < kClusterSize && (fn & 7u) != 7u;
-                        const int en = e0 + (int)(fn & 7u);
+                        const int en = !more ? e : mem ? __ldg(&mem[fn & 7u]) : e0 + (int)(fn & 7u);
                         int4 gn_n = gn;
                         float4 q_n = q;
                         if (more) {
@@ -608,7 +611,8 @@ __global__ void __launch_bounds__(NT, MINB) sweep_cluster_kernel(SweepArgs a) {
                     pk = (pk >> 16) | ((unsigned long long)(pw & 0xFFFFu) << 48);
                     pw >>= 16;
                     if ((f & 7u) == 7u) break;
-                    const int item = (e0 + (int)(f & 7u)) | (int)(((f >> 3) & 0xFu) << 24) | (int)(((f >> 7) & 0xFu) << 28);
+                    const int eo = mem ? __ldg(&mem[f & 7u]) : e0 + (int)(f & 7u);
+                    const int item = eo | (int)(((f >> 3) & 0xFu) << 24) | (int)(((f >> 7) & 0xFu) << 28);
                     if (TAB) {
                         update_tab<false>(a, base, dir, item, s_sigt, s_gtab, s_tab);
                     } else {
@@ -678,6 +682,7 @@ __global__ void __launch_bounds__(NT) sweep_batch_kernel(const BatchWork* __rest
                 for (int cs = s0 + threadIdx.x; cs < s1; cs += NT) {
                     const int4 r = __ldcs(crec + cs);
                     const int e0 = r.x * kClusterSize;
+                    const int* mem = W->blk_elem ? W->blk_elem + e0 : nullptr;
                     unsigned long long pk = (unsigned long long)(unsigned)r.y | ((unsigned long long)(unsigned)r.z << 32);
                     unsigned pw = (unsigned)r.w;
 #pragma unroll 1
@@ -686,7 +691,7 @@ __global__ void __launch_bounds__(NT) sweep_batch_kernel(const BatchWork* __rest
                         pk = (pk >> 16) | ((unsigned long long)(pw & 0xFFFFu) << 48);
                         pw >>= 16;
                         if ((f & 7u) == 7u) break;
-                        const int e = e0 + (int)(f & 7u);
+                        const int e = mem ? __ldg(&mem[f & 7u]) : e0 + (int)(f & 7u);
                         const int item = e | (int)(((f >> 3) & 0xFu) << 24) | (int)(((f >> 7) & 0xFu) << 28);
                         const Geom g = ngeom > 0 ? load_geom_tab(rec, s_gt, e) : load_geom(geom, e);
                         Update up;
@@ -1123,6 +1128,8 @@ int launch_sweep(Handle* h, float* psi) {
     a.tmat = h->d_tmat;
     a.ngeom = h->ngeom;
     a.crec = h->d_crec;
+    a.crec_base = h->d_crec_base;
+    a.blk_elem = h->d_blk_elem;
     a.cl_start = h->d_cl_start;
     a.cl_base = h->d_cl_base;
     a.ncl = h->d_ncl;

@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from helpers import jittered, rel_l2, scatter_mms, scatter_moment, transport_mms
+from helpers import golden_mesh, jittered, rel_l2, scatter_mms, scatter_moment, transport_mms
 from lionbolt_b200 import AngularClass, BoltzmannOp, MultigroupSolver, ScatteringOp, TransportOp, XSType
 from lionbolt_b200 import _lib
 from lionbolt_b200 import mesh as M
@@ -89,9 +89,10 @@ def _sweep_case(m, k, w, sigt, seed):
 @pytest.mark.parametrize("cfg", CLUSTER_CONFIGS)
 def test_cluster_schedule_wide_levels_and_cyclic_blocks(cfg, monkeypatch):
     """The cluster schedule (6-tet blocks swept as units) against the oracle on a two-material
-    32^3-hex box whose block levels (over a thousand blocks) take several passes of a CTA, and on a
-    jittered mesh whose block graphs have cycles in some directions, where the launcher runs the
-    plain level kernel instead."""
+    32^3-hex box whose block levels (over a thousand blocks) take several passes of a CTA, on a
+    jittered mesh whose block graphs have cycles in some directions (blocks on a cycle are swept
+    element by element there), and on the reference's unstructured het_cube mesh (blocks grown from
+    face neighbours, listed in a member table)."""
     monkeypatch.setenv("LB_SWEEP_CONFIG", str(cfg))
     k, w = P.quadrature(2, 4)
     two = M.box_mesh(32, 32, 32, (0, 0, 0), (4, 4, 4), material=lambda c: (c[:, 0] > 2.5).astype(np.int32), Nm=2)
@@ -100,7 +101,10 @@ def test_cluster_schedule_wide_levels_and_cyclic_blocks(cfg, monkeypatch):
     assert T._h.sweep_config()["schedule"].startswith("cluster levels")
     m, (k, w), sigt, sigs = SWEEP_CASES["jittered"]()
     T = _sweep_case(m, k, w, sigt, cfg + 20)
-    assert T._h.sweep_config()["schedule"] == "levels"
+    assert T._h.sweep_config()["schedule"].startswith("cluster levels")
+    het = golden_mesh("het_cube_spherical_beam")
+    T = _sweep_case(het, *P.quadrature(2, 4), np.array([0.07, 0.19]), cfg + 40)
+    assert T._h.sweep_config()["schedule"].startswith("cluster levels")
 
 
 def test_transport_mms_matches_oracle():

@@ -231,62 +231,97 @@ def _cluster_schedule(hh, NE, NI):
     nb, ml = np.zeros(1, np.int32), np.zeros(1, np.int32)
     assert hh.lib.lb_cluster_info(hh.h, _lib.iptr(nb), _lib.iptr(ml)) == 0
     if nb[0] == 0:
-        return 0, 0, None, None, None
-    rec = np.zeros((NI, nb[0], 4), np.int32)
-    st = np.zeros((NI, nb[0] + 1), np.int32)
+        return None
+    base = np.zeros(NI + 1, np.int64)
+    mem = np.zeros((nb[0], 6), np.int32)
+    mr = np.zeros(1, np.int32)
+    assert hh.lib.lb_cluster_layout(hh.h, base.ctypes.data_as(_lib._c_ll_p), _lib.iptr(mem), _lib.iptr(mr)) == 0
+    rec = np.zeros((base[NI], 4), np.int32)
+    st = np.zeros((NI, mr[0] + 1), np.int32)
     nl = np.zeros(NI, np.int32)
     assert hh.lib.lb_get_cluster_schedule(hh.h, _lib.iptr(rec), _lib.iptr(st), _lib.iptr(nl)) == 0
-    return int(nb[0]), int(ml[0]), rec, st, nl
+    return dict(nb=int(nb[0]), max_levels=int(ml[0]), base=base, members=mem, rec=rec, starts=st, nlevels=nl)
 
 
-def test_cluster_schedule_respects_every_dependency():
-    """The block schedule (blocks of 6 consecutive tets swept as units) against the reference schedule:
-    every block once per direction, every element once with the reference's upstream mask, every
-    upstream neighbour in another block on an earlier block level and every upstream neighbour in the
-    same block in an earlier slot.  A box mesh has nx + ny + nz - 2 block levels in an oblique
-    direction; a jittered mesh has cyclic block graphs and no block schedule."""
-    m = P.config1_small(n=(6, 6, 12)).mesh
-    k, w = P.quadrature(6, 12)
+def _check_cluster_schedule(m, k, w):
+    """Every element once per direction with the reference's upstream mask, every record's elements
+    members of its block, every upstream neighbour in another record on an earlier block level and
+    every upstream neighbour in the same record in an earlier slot."""
     hh = HostHandle()
-    nb0, ml0 = np.zeros(1, np.int32), np.zeros(1, np.int32)
-    assert hh.lib.lb_cluster_info(hh.h, _lib.iptr(nb0), _lib.iptr(ml0)) == _lib.LB_ERR_STATE   # no quadrature yet
-    assert hh.mesh(m) == 0 and hh.quad(k, w) == 0
+    assert hh.mesh(m) == 0 and hh.quad(k, w) == 0, hh.error()
     NE, NI = m.NE, k.shape[0]
     sl, up, nlev, ls = hh.schedule(NE, NI)
-    nb, ml, rec, st, nl = _cluster_schedule(hh, NE, NI)
-    assert nb == NE // 6 and ml == 6 + 6 + 12 - 2
+    cs = _cluster_schedule(hh, NE, NI)
+    assert cs is not None
+    mem = cs["members"]
+    assert sorted(mem[mem >= 0].tolist()) == list(range(NE))
     nbr = m.neighbors
+    split = 0
     for i in range(NI):
         upm = np.zeros(NE, np.int64)
         upm[sl[i]] = up[i]
-        blk_level = np.empty(nb, np.int64)
-        for L in range(nl[i]):
-            blk_level[rec[i, st[i, L]:st[i, L + 1], 0]] = L
-        assert st[i, nl[i]] == nb and sorted(rec[i, :, 0]) == list(range(nb))
-        words = rec[i, :, 1:].astype(np.uint32)
-        slots = np.stack([words & 0xFFFF, words >> 16], axis=2).reshape(nb, 6)
+        rec = cs["rec"][cs["base"][i]:cs["base"][i + 1]]
+        nr = rec.shape[0]
+        split += nr - cs["nb"]
+        rec_level = np.empty(nr, np.int64)
+        st = cs["starts"][i]
+        for L in range(cs["nlevels"][i]):
+            rec_level[st[L]:st[L + 1]] = L
+        assert st[cs["nlevels"][i]] == nr
+        words = rec[:, 1:].astype(np.uint32)
+        slots = np.stack([words & 0xFFFF, words >> 16], axis=2).reshape(nr, 6)
         off = slots & 7
         seen = np.zeros(NE, np.int64)
+        rec_of = np.full(NE, -1, np.int64)
         slot_of = np.full(NE, -1, np.int64)
-        for b in range(nb):
-            e0 = rec[i, b, 0] * 6
+        for r in range(nr):
             for kk in range(6):
-                if off[b, kk] == 7:
+                if off[r, kk] == 7:
                     continue
-                e = e0 + int(off[b, kk])
+                e = int(mem[rec[r, 0], off[r, kk]])
+                assert e >= 0
                 seen[e] += 1
-                slot_of[e] = kk
-                assert ((slots[b, kk] >> 3) & 15) == upm[e]
+                rec_of[e], slot_of[e] = r, kk
+                assert ((slots[r, kk] >> 3) & 15) == upm[e]
         assert np.all(seen == 1)
         for f in range(4):
             e = np.nonzero((upm >> f) & 1)[0]
             ne = nbr[e, f]
-            other = ne // 6 != e // 6
-            assert np.all(blk_level[ne[other] // 6] < blk_level[e[other] // 6])
+            other = rec_of[ne] != rec_of[e]
+            assert np.all(rec_level[rec_of[ne[other]]] < rec_level[rec_of[e[other]]])
             assert np.all(slot_of[ne[~other]] < slot_of[e[~other]])
+    return cs, split
+
+
+def test_cluster_schedule_respects_every_dependency():
+    """The block schedule against the reference schedule.  A box mesh: blocks of 6 consecutive tets
+    (one hex), nx + ny + nz - 2 block levels in an oblique direction and no block split.  A jittered
+    box: blocks on dependency cycles are split into single elements in the directions that need it.
+    The reference's unstructured meshes: blocks grown from face neighbours."""
+    m = P.config1_small(n=(6, 6, 12)).mesh
+    hh = HostHandle()
+    nb0, ml0 = np.zeros(1, np.int32), np.zeros(1, np.int32)
+    assert hh.lib.lb_cluster_info(hh.h, _lib.iptr(nb0), _lib.iptr(ml0)) == _lib.LB_ERR_STATE   # no quadrature yet
+    cs, split = _check_cluster_schedule(m, *P.quadrature(6, 12))
+    assert cs["nb"] == m.NE // 6 and cs["max_levels"] == 6 + 6 + 12 - 2 and split == 0
+    assert np.array_equal(cs["members"].ravel(), np.arange(m.NE))
     jit = jittered(M.box_mesh(6, 5, 4, (0, 0, 0), (3.0, 2.5, 2.0)), 0.07)
+    cs, split = _check_cluster_schedule(jit, *P.quadrature(4, 8))
+    assert split > 0
+    for name, quad in (("simple_cube", (4, 8)), ("het_cube_spherical_beam", (2, 4))):
+        g = golden_mesh(name)
+        cs, split = _check_cluster_schedule(g, *P.quadrature(*quad))
+        sizes = (cs["members"] >= 0).sum(axis=1)
+        assert sizes.mean() > 4.5, (name, sizes.mean())        # mostly full blocks
+        assert split > 0                                        # block graphs of unstructured meshes have cycles
+
+
+def test_cluster_queries_need_a_block_schedule():
     hj = HostHandle()
-    assert hj.mesh(jit) == 0 and hj.quad(*P.quadrature(4, 8)) == 0
-    assert _cluster_schedule(hj, jit.NE, 32)[0] == 0
+    assert hj.mesh(M.box_mesh(1, 1, 1)) == 0 and hj.quad(*P.quadrature(2, 4)) == 0
+    nb, ml = np.zeros(1, np.int32), np.zeros(1, np.int32)
+    assert hj.lib.lb_cluster_info(hj.h, _lib.iptr(nb), _lib.iptr(ml)) == 0 and nb[0] == 1
+    hs = HostHandle()
+    assert hs.mesh(M.box_mesh(1, 1, 1)) == 0
     one = np.zeros(4, np.int32)
-    assert hj.lib.lb_get_cluster_schedule(hj.h, _lib.iptr(one), _lib.iptr(one), _lib.iptr(one)) == _lib.LB_ERR_STATE
+    assert hs.lib.lb_get_cluster_schedule(hs.h, _lib.iptr(one), _lib.iptr(one), _lib.iptr(one)) == _lib.LB_ERR_STATE
