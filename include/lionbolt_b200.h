@@ -167,6 +167,19 @@ int lb_mg_solve(lb_handle* h, int solver, int m, double rtol, double atol, int m
 /* flux[G][NENK] scalar fluence (collided + uncollided), dose[NENK]; either may be NULL. */
 int lb_mg_get_results(lb_handle* h, double* flux, double* dose);
 
+/* Uncollided fluence of a planar beam with a rectangular field, at the DG nodes, computed on the device:
+ * replaces ExternalBeam%RayTrace (RayTracing.f90:152-379), FluenceQuadrature (FluenceQuadrature.f90:16-32)
+ * and the projection of FCSSource (FCSSource.f90:134-169).  The 4 quadrature points of every element
+ * whose point lies in the field (InField.f90:47-63: |((x - origin) perpendicular to axis) . e1| <=
+ * width1/2, the same for e2) are traced back to their projection on the beam plane (origin, e1, e2)
+ * through the mesh; exp(-sum sigma_t * length) (attn[Nm]: total cross sections of the beam's group) is
+ * projected onto the element's linear DG basis.  The result (unit fluence at the plane) becomes the
+ * uncollided flux of the handle's multigroup problem (call after lb_mg_set_problem / lb_mg_update_inputs,
+ * which overwrite it) and is copied to unc[NENK] when unc is not NULL.  origin, axis, e1, e2: [3],
+ * axis, e1, e2 orthonormal. */
+int lb_beam_uncollided(lb_handle* h, const double* origin, const double* axis, const double* e1, const double* e2,
+                       double width1, double width2, const double* attn, double* unc);
+
 /* Records CUDA event `slot` (0..15) on the handle's stream; lb_elapsed_ms returns the device time
  * between two recorded slots (synchronising on the later one). */
 int lb_mark(lb_handle* h, int slot);

@@ -67,6 +67,8 @@ SIGNATURES = {
     "lb_mesh_types": (ctypes.c_int, [_vp, _c_int_p]),
     "lb_set_right_precond_diag": (ctypes.c_int, [_vp, ctypes.c_int, _c_double_p]),
     "lb_lp_set_groups": (ctypes.c_int, [_vp, ctypes.c_int, _c_int_p, _c_int_p]),
+    "lb_beam_uncollided": (ctypes.c_int, [_vp, _c_double_p, _c_double_p, _c_double_p, _c_double_p, ctypes.c_double,
+                                          ctypes.c_double, _c_double_p, _c_double_p]),
     "lb_lp_calibrate": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, _c_int_p, _c_int_p]),
     "lb_givens": (ctypes.c_int, [ctypes.c_double, ctypes.c_double, _c_double_p, _c_double_p, _c_double_p]),
     "lb_cluster_info": (ctypes.c_int, [_vp, _c_int_p, _c_int_p]),

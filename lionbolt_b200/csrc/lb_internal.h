@@ -184,6 +184,12 @@ struct Handle {
 
     cudaEvent_t marks[16] = {};
 
+    // planar-beam ray walk (beam.cu): face planes, coordinates, connectivity, neighbours on the device
+    double4* d_beam_plane = nullptr;
+    double* d_beam_xyz = nullptr;
+    int* d_beam_node = nullptr;
+    int* d_beam_nbr = nullptr;
+    int beam_mesh_version = -1;
     // learned preconditioner state (mlp.cu)
     void* mlp = nullptr;
     // per-group use of the learned path in multigroup solves (empty: every group) and the operator

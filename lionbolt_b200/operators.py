@@ -113,6 +113,16 @@ class _Op:
     def timers(self):
         return self._h.timers()
 
+    def beam_uncollided(self, origin, axis, e1, e2, width1, width2, attn):
+        """Uncollided fluence [NENK] of a planar rectangular beam at the DG nodes, ray-traced on the device
+        (RayTracing.f90, FluenceQuadrature.f90, FCSSource.f90); it also becomes the uncollided flux of
+        the handle's multigroup problem."""
+        args = [as_f64(np.asarray(v, dtype=np.float64).ravel()) for v in (origin, axis, e1, e2)]
+        at = as_f64(np.atleast_1d(np.asarray(attn, dtype=np.float64)))
+        unc = np.zeros(self.mesh.NENK)
+        self._h.call("lb_beam_uncollided", *[dptr(a) for a in args], float(width1), float(width2), dptr(at), dptr(unc))
+        return unc
+
     # ---- learned right preconditioner (per-cell MLP, used by solver="FGMRES_ML") ----------------
     NIN, NOUT = 19, 16
 

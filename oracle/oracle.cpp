@@ -1522,4 +1522,133 @@ int or_mg_moment(void* h, int G, int Ls, const double* sigt, const double* sigs,
     return 0;
 }
 
+
+// ------------------------------------------------------------------------------------------
+//  Planar beam, uncollided fluence at the DG nodes: RayTracing.f90:152-201 (quadrature points of
+//  the elements in the field, ray from the point's projection Rp on the beam plane), TraceVector
+//  RayTracing.f90:205-379 (Moller-Trumbore against every region-boundary face, per-material path
+//  lengths from the sorted intersections; the single-material branch takes the one front-facing
+//  boundary hit), InField.f90:47-63 (rectangle), FluenceQuadrature.f90:28-32 (Beer's law) and the
+//  projection of FCSSource.f90:134-169 (phi0ek = M_ref^-1 sum_q w_q N_k(q) phi0q).  A region is the
+//  set of elements of one material; its faces are the element faces on the mesh boundary or next to
+//  another material.  The 4-point tetrahedral rule of the absent NittanyPhysics library
+//  (PrepTetrahedralQuadrature) is restated from its published form: barycentric (a, b, b, b),
+//  a = (5 + 3 sqrt 5)/20, b = (5 - sqrt 5)/20, weights 1/24 on the reference tetrahedron.
+//  origin, axis, e1, e2 [3]: beam frame; w1, w2: field widths; attn [Nm]; unc [NENK] out.
+// ------------------------------------------------------------------------------------------
+int or_beam_uncollided(void* hp, const double* origin, const double* axis, const double* e1, const double* e2,
+                       double w1, double w2, const double* attn, double* unc) {
+    Oracle* o = static_cast<Oracle*>(hp);
+    const int NE = o->NE, Nm = o->Nm;
+    const double TOL = 1.0e-8, FTOL = 1.0e-12;
+    const double qa = (5.0 + 3.0 * std::sqrt(5.0)) / 20.0, qb = (5.0 - std::sqrt(5.0)) / 20.0;
+    // region faces: (element, local face) per material
+    std::vector<std::vector<std::pair<int, int>>> rf(Nm);
+    for (int e = 0; e < NE; ++e)
+        for (int f = 0; f < 4; ++f) {
+            const int n = o->nbr[(size_t)e * 4 + f];
+            if (n < 0 || o->mat[n] != o->mat[e]) rf[o->mat[e]].push_back({e, f});
+        }
+    // reference-element mass matrix inverse (IMr) and shape functions at the points
+    double Mi[16];
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) Mi[i * 4 + j] = (i == j ? 2.0 : 1.0) / 120.0;
+    invert(4, Mi);
+    int status = 0;
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int e = 0; e < NE; ++e) {
+        double phiq[4], load[4] = {0, 0, 0, 0};
+        for (int kq = 0; kq < 4; ++kq) {
+            double v[3] = {0, 0, 0};
+            for (int k = 0; k < 4; ++k)
+                for (int d = 0; d < 3; ++d) v[d] += (k == kq ? qa : qb) * o->rg[(size_t)o->node[(size_t)e * 4 + k] * 3 + d];
+            // InField, rectangle
+            double u[3], vv[3];
+            for (int d = 0; d < 3; ++d) u[d] = v[d] - origin[d];
+            const double ua = dot3(u, axis);
+            for (int d = 0; d < 3; ++d) vv[d] = u[d] - ua * axis[d];
+            const bool in = std::fabs(dot3(vv, e1)) <= 0.5 * w1 + FTOL && std::fabs(dot3(vv, e2)) <= 0.5 * w2 + FTOL;
+            phiq[kq] = 0.0;
+            if (!in) continue;
+            // Rp = origin + ((v - origin).e1) e1 + ((v - origin).e2) e2, r = v - Rp
+            double Rp[3], r[3];
+            const double a1 = dot3(u, e1), a2 = dot3(u, e2);
+            for (int d = 0; d < 3; ++d) {
+                Rp[d] = origin[d] + a1 * e1[d] + a2 * e2[d];
+                r[d] = v[d] - Rp[d];
+            }
+            const double length = norm2_scaled(r, 3);
+            std::vector<double> pathlen(Nm, 0.0);
+            bool success = false;
+            double tsingle = 0.0;
+            for (int reg = 0; reg < Nm; ++reg) {
+                std::vector<double> llist;
+                for (auto [fe, ff] : rf[reg]) {
+                    const double* v0 = &o->rg[(size_t)o->node[(size_t)fe * 4 + F2K[ff][0]] * 3];
+                    const double* v1 = &o->rg[(size_t)o->node[(size_t)fe * 4 + F2K[ff][1]] * 3];
+                    const double* v2 = &o->rg[(size_t)o->node[(size_t)fe * 4 + F2K[ff][2]] * 3];
+                    double edge1[3], edge2[3], nref[3], pvec[3], tvec[3], qvec[3];
+                    for (int d = 0; d < 3; ++d) { edge1[d] = v1[d] - v0[d]; edge2[d] = v2[d] - v0[d]; }
+                    const double* n = &o->nrm[(size_t)fe * 12 + ff * 3];
+                    double det = dot3(n, r);
+                    if (Nm == 1) { if (det > -TOL) continue; }
+                    else if (std::fabs(det) < TOL) continue;
+                    cross3(edge1, edge2, nref);
+                    if (dot3(n, nref) < 0.0)
+                        for (int d = 0; d < 3; ++d) std::swap(edge1[d], edge2[d]);
+                    cross3(r, edge2, pvec);
+                    det = dot3(edge1, pvec);
+                    if (std::fabs(det) < TOL) continue;
+                    for (int d = 0; d < 3; ++d) tvec[d] = Rp[d] - v0[d];
+                    const double uu = dot3(tvec, pvec);
+                    cross3(tvec, edge1, qvec);
+                    const double vq = dot3(r, qvec);
+                    if (det > 0.0) {
+                        if (uu < -TOL || uu > det + TOL) continue;
+                        if (vq < -TOL || uu + vq > det + TOL) continue;
+                    } else {
+                        if (uu > TOL || uu < det - TOL) continue;
+                        if (vq > TOL || uu + vq < det - TOL) continue;
+                    }
+                    const double t = dot3(edge2, qvec) / det;
+                    if (Nm == 1) { success = true; tsingle = t; break; }
+                    if (t > 1.0) continue;
+                    llist.push_back(t);
+                }
+                if (Nm == 1) break;
+                if (llist.size() == 1 && std::fabs(llist[0]) < 1.0e-12) continue;
+                if (llist.empty()) continue;
+                std::sort(llist.begin(), llist.end());
+                size_t nkeep = 1;
+                for (size_t i = 1; i < llist.size(); ++i)
+                    if (std::fabs(llist[i] - llist[nkeep - 1]) > 1.0e-12) llist[nkeep++] = llist[i];
+                llist.resize(nkeep);
+                for (size_t il = 0; il + 1 < llist.size(); il += 2) pathlen[reg] += llist[il + 1] - llist[il];
+                if (llist.size() % 2 == 1) pathlen[reg] += 1.0 - llist.back();
+            }
+            if (Nm == 1) {
+                if (!success) {
+#pragma omp critical
+                    status = 1;
+                    continue;
+                }
+                pathlen[0] = (1.0 - tsingle) * length;
+            } else {
+                for (int m = 0; m < Nm; ++m) pathlen[m] *= length;
+            }
+            double tau = 0.0;
+            for (int m = 0; m < Nm; ++m) tau += attn[m] * pathlen[m];
+            phiq[kq] = std::exp(-tau);
+        }
+        for (int k = 0; k < 4; ++k)
+            for (int kq = 0; kq < 4; ++kq) load[k] += (1.0 / 24.0) * (k == kq ? qa : qb) * phiq[kq];
+        for (int k = 0; k < 4; ++k) {
+            double c = 0.0;
+            for (int j = 0; j < 4; ++j) c += Mi[k * 4 + j] * load[j];
+            unc[(size_t)e * 4 + k] = c;
+        }
+    }
+    return status;
+}
+
 }  // extern "C"

@@ -44,6 +44,7 @@ _SIG = {
                                      ctypes.c_double, ctypes.c_double, ctypes.c_int, _D, _D, _I]),
     "or_set_angular_streamed": (ctypes.c_int, [_V, ctypes.c_int, _D, _D]),
     "or_set_blas": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p]),
+    "or_beam_uncollided": (ctypes.c_int, [_V, _D, _D, _D, _D, ctypes.c_double, ctypes.c_double, _D, _D]),
     "or_scatter_apply_dgemv": (ctypes.c_int, [_V, _D, ctypes.c_long, ctypes.c_long]),
     "or_set_sigt": (ctypes.c_int, [_V, _D]),
     "or_moment_transport": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, _D, _D]),
@@ -379,3 +380,15 @@ class Oracle:
         if snap:
             out.update(flux_snap=fs, dose_snap=ds, iters_snap=its)
         return out
+
+    def beam_uncollided(self, origin, axis, e1, e2, w1, w2, attn):
+        """Uncollided fluence of a planar rectangular beam at the DG nodes [NENK] (reference ray tracing
+        against region faces, Beer's law, projection onto the DG basis)."""
+        f = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+        args = [f(origin), f(axis), f(e1), f(e2)]
+        at = f(np.atleast_1d(attn))
+        unc = np.zeros(self.NENK)
+        st = self.lib.or_beam_uncollided(self.h, *[_d(a) for a in args], float(w1), float(w2), _d(at), _d(unc))
+        if st:
+            raise RuntimeError("oracle ray tracing found no boundary intersection")
+        return unc
