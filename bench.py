@@ -45,11 +45,13 @@ def parse():
     p.add_argument("--mesh", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
                    help="hexes per axis of a reduced box with the same physics (profiling cases)")
     p.add_argument("--groups", type=int, default=None, help="energy groups of the reduced box")
-    p.add_argument("--workload", default="dose", choices=["dose", "gemm", "batch", "mesh"],
+    p.add_argument("--workload", default="dose", choices=["dose", "gemm", "batch", "mesh", "beam"],
                    help="dose: multigroup dose solve (default); gemm: standalone moment-to-discrete and "
                         "discrete-to-moment contractions at the 768k-tet size, split-BF16 vs cuBLAS FP32 vs FP64; "
                         "batch: 64 independent problems (8^3..32^3 hexes, S8/S12/S16, 1-10 groups, P3) solved "
-                        "together; mesh: sweep throughput of a within-group solve on --mesh-file")
+                        "together; mesh: sweep throughput of a within-group solve on --mesh-file; beam: the "
+                        "ray-traced first-collision data of the dose workload's beam (--mesh reduces it)")
+    p.add_argument("--batch-count", type=int, default=64, help="problems of --workload batch (profiling cases)")
     p.add_argument("--mesh-file", default=os.path.join(ROOT, "tests", "golden", "mesh_het_cube_spherical_beam.npz"),
                    help="mesh of --workload mesh: .npz fixture, gmsh .msh, or 'jittered' (768k-tet box, moved nodes)")
     p.add_argument("--no-subbench", action="store_true",
@@ -366,6 +368,7 @@ def real_sh(Ls, dirs):
 # kernel of each sweep schedule the autotuner can pick
 SWEEP_KERNELS = {"cluster levels": "sweep_cluster_kernel", "cluster levels+type tables": "sweep_cluster_kernel",
                  "cluster levels+element prefetch": "sweep_cluster_kernel",
+                 "cluster levels+element prefetch+previous in registers": "sweep_cluster_kernel",
                  "cluster levels+type tables+element prefetch": "sweep_cluster_kernel",
                  "levels": "sweep_levels_kernel",
                  "levels+prefetch": "sweep_levels_pf_kernel", "element flags": "sweep_flags_kernel",
@@ -479,7 +482,7 @@ def run_batch(args, steps=None, warmup=None, emit=True):
     from lionbolt_b200 import problems as P
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
-    probs = P.batch_problems(count=64, seed=20261203)
+    probs = P.batch_problems(count=args.batch_count, seed=20261203)
     bs = BatchSolver(device=local)
     for p in probs:
         bs.add_problem(p)
@@ -500,11 +503,12 @@ def run_batch(args, steps=None, warmup=None, emit=True):
     NE = np.array([p.mesh.NE for p in probs])
     NI = np.array([p.NI for p in probs])
     upd = float(sum(int(NE[i]) * int(NI[i]) * int(it[i].sum()) for i in range(len(probs))))
-    line = {"metric": "batched dose solves (config3): 64 independent problems per step", "value": 64 * steps / (t / 1e3),
+    nprob = len(probs)
+    line = {"metric": f"batched dose solves (config3): {nprob} independent problems per step", "value": nprob * steps / (t / 1e3),
             "unit": "dose solves/s", "n_gpus": 1, "steps": steps, "warmup": warmup,
             "ms_per_step": t / steps, "higher_is_better": True, "dtype": "f32 sweep / split-bf16 moments / f64 Krylov",
             "data": "synthetic",
-            "config": {"workload": "64 problems: hexes per axis U{8..32} x 6 tets, S8/S12/S16, 1-10 groups, P3, "
+            "config": {"workload": f"{nprob} problems: hexes per axis U{{8..32}} x 6 tets, S8/S12/S16, 1-10 groups, P3, "
                                    f"GMRES({args.m}) to {args.rtol:g}, seed 20261203",
                        "tets_total": int(NE.sum()), "groups_total": int(sum(p.G for p in probs))},
             "updates_per_s": upd / (t / steps / 1e3),
@@ -840,6 +844,15 @@ def main():
         return 0
     if args.workload == "mesh":
         run_mesh(args)
+        return 0
+    if args.workload == "beam":
+        from lionbolt_b200 import MultigroupSolver
+        prob, wl = workload(args)
+        mg = MultigroupSolver().set_problem(prob)
+        line = beam_subbench(prob, mg)
+        line["mesh"] = wl
+        print(json.dumps(line), flush=True)
+        mg.Destroy()
         return 0
     return run_ours(args)
 

@@ -209,8 +209,10 @@ class Handle:
                  dirs_per_cta=int(cfg[2]), ilp=int(cfg[3]))
         if kind in (5, 6):
             d["min_ctas_per_sm"] = d.pop("dirs_per_cta")
-            if d["ilp"] == 2:
+            if d["ilp"] >= 2:
                 d["schedule"] += "+element prefetch"
+            if d["ilp"] == 3:
+                d["schedule"] += "+previous in registers"
         return d
 
     def mesh_types(self):

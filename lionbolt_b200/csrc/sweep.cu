@@ -138,9 +138,10 @@ __device__ __forceinline__ Geom load_geom(const float4* __restrict__ geom, int e
     return g;
 }
 
-template <bool kCG, bool kHaveQ = false>
+template <bool kCG, bool kHaveQ = false, bool kPrev = false>
 __device__ __forceinline__ void assemble_g(const float* base, float4 dir, int item, const Geom& G, const float* s_sigt,
-                                           Update& u, float4 qpre);
+                                           Update& u, float4 qpre, int prev_e = -1,
+                                           float4 prev_v = make_float4(0.f, 0.f, 0.f, 0.f));
 
 // Element from its 16-byte record (one 128-bit load) and the type table in shared memory.  The type
 // index sits in the bits that otherwise carry the material, so the element update reads it as the
@@ -183,9 +184,11 @@ __device__ __forceinline__ void assemble(const SweepArgs& a, const float* base, 
     assemble_g<kCG, kHaveQ>(base, dir, item, G, s_sigt, u, qpre);
 }
 
-template <bool kCG, bool kHaveQ>
+// kPrev: the solution of element prev_e (the thread's previous update) is passed in registers and used
+// instead of a load when it is an upstream neighbour.
+template <bool kCG, bool kHaveQ, bool kPrev>
 __device__ __forceinline__ void assemble_g(const float* base, float4 dir, int item, const Geom& G, const float* s_sigt,
-                                           Update& u, float4 qpre) {
+                                           Update& u, float4 qpre, int prev_e, float4 prev_v) {
     // gmsh face -> local nodes; the vertex opposite face f is 3 - f
     constexpr int F[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
     const int e = item & 0xFFFFFF;
@@ -209,7 +212,7 @@ __device__ __forceinline__ void assemble_g(const float* base, float4 dir, int it
         if ((upm >> f) & 1) {
             const unsigned wd = nw[f];
             const int ep = (int)(wd & 0xFFFFFFu);
-            const float4 u4 = ld4<kCG>(base + 4 * (size_t)ep);
+            const float4 u4 = (kPrev && ep == prev_e) ? prev_v : ld4<kCG>(base + 4 * (size_t)ep);
             const float u0 = pick(u4, (wd >> 24) & 3);
             const float u1 = pick(u4, (wd >> 26) & 3);
             const float u2 = pick(u4, (wd >> 28) & 3);
@@ -536,7 +539,7 @@ __global__ void __launch_bounds__(1024, MINB) sweep_levels_pf_kernel(SweepArgs a
 // has about a third as many block levels as element levels.  The element update is the level
 // kernel's, so the results are bit-identical.
 // ---------------------------------------------------------------------------------------------
-template <int NT, int MINB, bool TAB, bool PF>
+template <int NT, int MINB, bool TAB, int PF>
 __global__ void __launch_bounds__(NT, MINB) sweep_cluster_kernel(SweepArgs a) {
     __shared__ float s_sigt[256];
     extern __shared__ float4 s_gtab_dyn[];
@@ -576,6 +579,8 @@ __global__ void __launch_bounds__(NT, MINB) sweep_cluster_kernel(SweepArgs a) {
                     int e = mem ? __ldg(&mem[f & 7u]) : e0 + (int)(f & 7u);
                     int4 gn = __ldg(&a.rec[e]);
                     float4 q = ld4<false>(base + 4 * (size_t)e);
+                    int prev_e = -1;
+                    float4 prev_v = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll 1
                     for (int k = 0; k < kClusterSize; ++k) {
                         const unsigned fn = (unsigned)(pk & 0xFFFFu);
@@ -592,6 +597,13 @@ __global__ void __launch_bounds__(NT, MINB) sweep_cluster_kernel(SweepArgs a) {
                         const int item = e | (int)(((f >> 3) & 0xFu) << 24) | (int)(((f >> 7) & 0xFu) << 28);
                         if (TAB) {
                             update_tab_pre<false>(a, base, dir, item, gn, q, s_sigt, s_gtab, s_tab);
+                        } else if (PF == 2) {
+                            Update up;
+                            assemble_g<false, true, true>(base, dir, item, geom_from_rec(gn, s_gtab), s_sigt, up, q,
+                                                          prev_e, prev_v);
+                            finish<false>(base, item, up);
+                            prev_e = e;
+                            prev_v = make_float4(up.r[0], up.r[1], up.r[2], up.r[3]);
                         } else {
                             Update up;
                             assemble_g<false, true>(base, dir, item, geom_from_rec(gn, s_gtab), s_sigt, up, q);
@@ -974,14 +986,15 @@ struct Config {
                    // 5 blocks of elements (cluster records), 6 the same with per-type element tables
     int threads;
     int dpc;       // directions per CTA (kind 0); minimum CTAs per SM (kinds 2, 5)
-    int ilp;       // updates in flight per thread (kind 0); 2 = next element's record and source prefetched (5, 6)
+    int ilp;       // updates in flight per thread (kind 0); kinds 5, 6: 2 = next element's record and source
+                   // prefetched, 3 = the same and the previous element's solution kept in registers
 };
 
 const Config kConfigs[] = {
     {4, 1024, 2, 1}, {4, 512, 2, 1}, {4, 512, 3, 1}, {4, 1024, 3, 1}, {4, 512, 6, 1},
     {0, 1024, 1, 1}, {0, 512, 1, 1}, {2, 1024, 1, 1}, {3, 512, 0, 1}, {1, 256, 0, 0},
     {4, 768, 2, 1}, {0, 1024, 1, 2}, {0, 1024, 1, 3}, {0, 768, 1, 3}, {5, 1024, 1, 1}, {5, 512, 2, 1}, {5, 768, 2, 1}, {5, 1024, 2, 1},
-    {6, 512, 2, 1}, {6, 768, 2, 1}, {5, 512, 2, 2}, {6, 512, 2, 2},
+    {6, 512, 2, 1}, {6, 768, 2, 1}, {5, 512, 2, 2}, {6, 512, 2, 2}, {5, 512, 2, 3},
 };
 constexpr int kNumConfigs = sizeof(kConfigs) / sizeof(kConfigs[0]);
 constexpr int kFinalists = 3;   // candidates timed a second time before one is kept
@@ -1055,7 +1068,7 @@ cudaError_t launch_flags(const SweepArgs& a, int sm_count, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-template <int NT, int MINB, bool TAB, bool PF = false>
+template <int NT, int MINB, bool TAB, int PF = 0>
 cudaError_t launch_cluster(const SweepArgs& a, int sm_count, cudaStream_t s) {
     const size_t smem = (sizeof(float4) * 3 + (TAB ? sizeof(ElemTab) : 0)) * (size_t)a.ngeom;
     int per_sm = 0;
@@ -1169,14 +1182,15 @@ int launch_sweep(Handle* h, float* psi) {
         cudaFuncGetAttributes(&fa, sweep_levels_kernel<2, 2>);
         cudaFuncGetAttributes(&fa, sweep_dataflow_kernel);
         cudaFuncGetAttributes(&fa, sweep_group_kernel<2, 768>);
-        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<1024, 1, false, false>);
-        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<1024, 2, false, false>);
-        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<768, 2, false, false>);
-        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2, false, false>);
-        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2, true, false>);
-        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<768, 2, true, false>);
-        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2, false, true>);
-        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2, true, true>);
+        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<1024, 1, false, 0>);
+        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<1024, 2, false, 0>);
+        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<768, 2, false, 0>);
+        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2, false, 0>);
+        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2, true, 0>);
+        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<768, 2, true, 0>);
+        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2, false, 1>);
+        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2, true, 1>);
+        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2, false, 2>);
     }
     Config cfg = kConfigs[cfg_idx];
     // the element-flag schedule keeps one bit per element in shared memory
@@ -1213,9 +1227,10 @@ int launch_sweep(Handle* h, float* psi) {
         e = (cfg.threads == 256) ? launch_flags<256>(a, h->sm_count, h->stream)
           : (cfg.threads == 1024) ? launch_flags<1024>(a, h->sm_count, h->stream)
                                   : launch_flags<512>(a, h->sm_count, h->stream);
-    } else if ((cfg.kind == 5 || cfg.kind == 6) && cfg.ilp == 2) {
-        e = cfg.kind == 6 ? launch_cluster<512, 2, true, true>(a, h->sm_count, h->stream)
-                          : launch_cluster<512, 2, false, true>(a, h->sm_count, h->stream);
+    } else if ((cfg.kind == 5 || cfg.kind == 6) && cfg.ilp >= 2) {
+        e = cfg.kind == 6   ? launch_cluster<512, 2, true, 1>(a, h->sm_count, h->stream)
+            : cfg.ilp == 3 ? launch_cluster<512, 2, false, 2>(a, h->sm_count, h->stream)
+                           : launch_cluster<512, 2, false, 1>(a, h->sm_count, h->stream);
     } else if (cfg.kind == 5) {
         if (cfg.threads == 1024) e = cfg.dpc == 2 ? launch_cluster<1024, 2, false>(a, h->sm_count, h->stream)
                                                   : launch_cluster<1024, 1, false>(a, h->sm_count, h->stream);
