@@ -559,8 +559,11 @@ def run_mesh(args):
                                                                          XSType(sigt, sigs))
     h = L._h
     q = np.random.default_rng(0).uniform(size=m.NENK * k.shape[0])
-    for _ in range(max(args.warmup, 3)):      # the first sweeps of a handle time the schedule candidates
+    # the first sweeps of a handle time the schedule candidates: warm up until the tuner has chosen
+    for w in range(100):
         L.MatInv(q.copy())
+        if w + 1 >= args.warmup and h.sweep_config() is not None:
+            break
     h.reset_timers()
     with ClockSampler(local) as clocks:
         for _ in range(args.steps):

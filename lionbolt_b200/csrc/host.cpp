@@ -745,6 +745,8 @@ static int build_cluster_schedule(Handle* h) {
     h->nclusters = NC;
     h->max_cluster_levels = maxl;
     h->max_cluster_records = maxr;
+    h->cluster_levels_total = 0;
+    for (int i = 0; i < NI; ++i) h->cluster_levels_total += ncl[i];
     h->cl_start_h = cl_start;
     h->cl_base_h = cl_base;
     h->crec_base_h = base;

@@ -106,6 +106,7 @@ struct Handle {
     std::vector<long long> crec_base_h;
     std::vector<int> blk_elem_h;
     int max_cluster_records = 0;   // largest record count of a direction
+    long long cluster_levels_total = 0;   // block levels summed over the directions
     int* d_cl_start = nullptr;     // block-level starts, per direction (ncl[i] + 1 entries)
     int* d_cl_base = nullptr;      // [NI] offset of direction i's starts in d_cl_start
     int* d_ncl = nullptr;          // [NI] block levels per direction
@@ -215,7 +216,8 @@ void real_sh(int Ls, const double* dir, double* Y);
 // ---- learned preconditioner (mlp.cu) ----
 void mlp_destroy(Handle* h);
 bool mlp_ready(Handle* h);
-int mlp_apply_precond(Handle* h, const double* v, double* z);
+// z = preconditioner(v); v * vscale is the vector the network's features are taken from (z in v's units)
+int mlp_apply_precond(Handle* h, const double* v, double* z, double vscale);
 // Appends `count` training samples drawn from the residual r and error err (device moment vectors).
 int mlp_sample(Handle* h, const double* r, const double* err, long long count, unsigned long long seed);
 

@@ -240,7 +240,9 @@ __global__ void __launch_bounds__(lp::kThreads, 2) lp_apply_kernel(const float* 
                                                                   double* __restrict__ z, const float* __restrict__ chord,
                                                                   const int* __restrict__ mat,
                                                                   const float2* __restrict__ matxs, long long NE,
-                                                                  long long NENK, int nm, int nmom) {
+                                                                  long long NENK, int nm, int nmom, double vscale) {
+    // vscale: v * vscale is the vector whose features the network sees (an unnormalised Krylov basis
+    // vector times its scale); the correction is returned in v's units
     extern __shared__ __align__(16) unsigned char smraw[];
     InferSmem& sm = *reinterpret_cast<InferSmem*>(smraw);
     load_infer_weights(sm, w);
@@ -263,7 +265,7 @@ __global__ void __launch_bounds__(lp::kThreads, 2) lp_apply_kernel(const float* 
                 sum = d.x + d.y;
             }
             sum += __shfl_xor_sync(0xffffffffu, sum, 1);
-            avg[j] = (float)(0.25 * sum);
+            avg[j] = (float)(0.25 * vscale * sum);
             ss = fmaf(avg[j], avg[j], ss);
         }
         const float s = sqrtf(ss / (float)nmom);
@@ -287,7 +289,7 @@ __global__ void __launch_bounds__(lp::kThreads, 2) lp_apply_kernel(const float* 
             const float* O = sm.o[warp] + c * 17;
             for (int j = 0; j < nm; ++j) {
                 const double2 d = __ldg(reinterpret_cast<const double2*>(v + (size_t)j * NENK + off));
-                const double corr = j < nmom ? (double)s * (double)O[j] : 0.0;
+                const double corr = j < nmom ? (double)s * (double)O[j] / vscale : 0.0;
                 *reinterpret_cast<double2*>(z + (size_t)j * NENK + off) = make_double2(d.x + corr, d.y + corr);
             }
         }
@@ -575,7 +577,7 @@ static int infer_grid(Handle* h, const void* kernel, long long ntiles) {
     return (int)std::max<long long>(1, std::min<long long>(blocks, (long long)h->sm_count * per_sm));
 }
 
-int mlp_apply_precond(Handle* h, const double* v, double* z) {
+int mlp_apply_precond(Handle* h, const double* v, double* z, double vscale) {
     MlpState* s = S(h);
     if (!s || !s->have_weights) return fail(h, LB_ERR_STATE, "learned preconditioner: no weights loaded");
     int rc = ensure_cell_data(h, s);
@@ -585,7 +587,8 @@ int mlp_apply_precond(Handle* h, const double* v, double* z) {
     Timer t;
     timer_begin(h, LB_T_PRECOND, t);
     lp_apply_kernel<<<grid, lp::kThreads, sizeof(InferSmem), h->stream>>>(
-        s->d_w, v, z, s->d_chord, h->d_mat, s->d_matxs, (long long)h->NE, h->NENK, h->nm, std::min(h->nm, lp::NMOM));
+        s->d_w, v, z, s->d_chord, h->d_mat, s->d_matxs, (long long)h->NE, h->NENK, h->nm, std::min(h->nm, lp::NMOM),
+        vscale);
     cudaError_t e = cudaGetLastError();
     timer_end(h, t);
     return e == cudaSuccess ? LB_OK : cuda_fail(h, e, "preconditioner kernel");
@@ -792,7 +795,7 @@ int lb_lp_apply(lb_handle* h, const double* v, double* z) {
         if (dz) cudaFree(dz);
         return cuda_fail(h, e, "lb_lp_apply buffers");
     }
-    rc = mlp_apply_precond(h, dv, dz);
+    rc = mlp_apply_precond(h, dv, dz, 1.0);
     if (!rc) {
         e = cudaMemcpyAsync(z, dz, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);

@@ -95,16 +95,23 @@ struct KrylovResult {
 };
 
 using DevOp = std::function<int(const double* in, double* out)>;
+// Right preconditioner: out = P(in), with in * scale the normalised basis vector (P may use it to fix
+// the magnitude of its input; a linear P ignores it).
+using PrecOp = std::function<int(const double* in, double scale, double* out)>;
 
 // Restarted GMRES(m) / FGMRES(m) (right preconditioner `prec`), SPARSKIT semantics.
 static KrylovResult gmres_device(Handle* h, size_t n, const double* rhs, double* sol, int m, double rtol, double atol,
-                                 int maxit, const DevOp& matvec, const DevOp* prec) {
+                                 int maxit, const DevOp& matvec, const PrecOp* prec) {
     KrylovResult res;
     int rc = 0;
     double* V = h->d_V;
     double* Z = h->d_Z;
     GmresHost gh(m);
-    std::vector<double> hh(m + 2), h2(m + 2), cc(m + 2), coef;
+    std::vector<double> hh(m + 2), h2(m + 2), cc(m + 2), cw(m + 2), coef;
+    // The stored basis vectors W_i are not normalised: V_i = sc[i] W_i.  The scale factors enter the
+    // coefficients of every pass instead, which saves the two full-vector passes of a normalisation
+    // (v0 = r / alpha, v_k = w / h_k) per Arnoldi step.  The (flexible) Z_i are stored the same way.
+    std::vector<double> sc(m + 2, 1.0);
     const int ldg = m + 2;
     std::vector<double> G((size_t)ldg * ldg, 0.0);   // Gram matrix V^T V of the current cycle's basis
     double rn = vnorm(h, rhs, n, &rc);
@@ -123,7 +130,7 @@ static KrylovResult gmres_device(Handle* h, size_t n, const double* rhs, double*
         fpar5 = alpha;
         gh.start(alpha);
         if (alpha <= fpar4) { res.status = LB_OK; res.nmv = nmv; res.resid = alpha; return res; }
-        k_scale(h, V, 1.0 / alpha, n);
+        sc[0] = 1.0 / alpha;
         G[0] = 1.0;
         int k = 0;
         bool breakdown = false;
@@ -131,7 +138,7 @@ static KrylovResult gmres_device(Handle* h, size_t n, const double* rhs, double*
             ++k;
             const double* vin = V + (size_t)(k - 1) * n;
             if (prec) {
-                if ((rc = (*prec)(vin, Z + (size_t)(k - 1) * n))) { res.status = rc; return res; }
+                if ((rc = (*prec)(vin, sc[k - 1], Z + (size_t)(k - 1) * n))) { res.status = rc; return res; }
                 vin = Z + (size_t)(k - 1) * n;
             }
             double* vk = V + (size_t)k * n;
@@ -144,13 +151,20 @@ static KrylovResult gmres_device(Handle* h, size_t n, const double* rhs, double*
             // non-orthogonality h2 / hk enters G for the next steps (this replaces the second projection
             // pass of classical Gram-Schmidt with re-orthogonalisation: 2k + 5 vector passes per step
             // instead of 3k + 5).
+            // (vk holds A W_{k-1} = A V_{k-1} / sc[k-1]; the dots below are of the stored vectors)
+            const double s1 = sc[k - 1];
             double nrm0 = 0.0, nrm1 = 0.0;
             if ((rc = k_dots_norm(h, V, n, k, vk, n, hh.data(), &nrm0))) { res.status = rc; return res; }
+            for (int i = 0; i < k; ++i) hh[i] *= sc[i] * s1;
             if (!gram_solve(G, ldg, k, hh.data(), cc.data()))
                 for (int i = 0; i < k; ++i) cc[i] = hh[i];
-            if ((rc = k_axpy_dots(h, vk, V, n, k, cc.data(), n, h2.data(), &nrm1))) { res.status = rc; return res; }
-            for (int i = 0; i < k; ++i) hh[i] = cc[i];
-            const double hk = std::sqrt(std::max(0.0, nrm1));
+            for (int i = 0; i < k; ++i) cw[i] = cc[i] * sc[i] / s1;
+            if ((rc = k_axpy_dots(h, vk, V, n, k, cw.data(), n, h2.data(), &nrm1))) { res.status = rc; return res; }
+            for (int i = 0; i < k; ++i) {
+                hh[i] = cc[i];
+                h2[i] *= sc[i] * s1;
+            }
+            const double hk = s1 * std::sqrt(std::max(0.0, nrm1));
             if (std::isnan(hk)) { res.status = fail(h, LB_ERR_NAN, "RESIDUAL NORM is NaN."); return res; }
             if (!(hk > 0.0)) {
                 for (int i = 0; i < k; ++i) gh.H[k][i + 1] = hh[i];
@@ -159,7 +173,7 @@ static KrylovResult gmres_device(Handle* h, size_t n, const double* rhs, double*
                 --k;
                 break;
             }
-            if ((rc = k_axpy_scale(h, vk, V, n, 0, h2.data(), 1.0 / hk, n))) { res.status = rc; return res; }
+            sc[k] = s1 / hk;
             for (int i = 0; i < k; ++i) G[(size_t)i * ldg + k] = G[(size_t)k * ldg + i] = h2[i] / hk;
             G[(size_t)k * ldg + k] = 1.0;
             alpha = gh.add_column(k, hh.data(), hk);
@@ -173,7 +187,8 @@ static KrylovResult gmres_device(Handle* h, size_t n, const double* rhs, double*
             res.status = fail(h, LB_ERR_BREAKDOWN, "GMRES : Anticipated breakdown / division by zero.");
             return res;
         }
-        // sol += sum_i y_i V_i (or Z_i): multi-axpy with negated coefficients
+        // sol += sum_i y_i V_i (or Z_i): multi-axpy with negated coefficients, on the stored vectors
+        for (int i = 0; i < kk; ++i) coef[i] *= sc[i];
         if ((rc = k_multi_axpy(h, sol, prec ? Z : V, n, kk, coef.data(), n))) { res.status = rc; return res; }
         if (breakdown) continue;
         if ((nmv < maxit || maxit <= 0) && fpar5 > fpar4) continue;
@@ -230,7 +245,7 @@ static KrylovResult moment_solve(Handle* h, const double* b, double* phi, int so
             return bad;
         }
         const size_t NENK = (size_t)h->NENK;
-        DevOp pc = [h, NENK, n](const double* in, double* out) {
+        PrecOp pc = [h, NENK, n](const double* in, double, double* out) {
             if (h->pdiag.empty()) return k_copy(h, out, in, n);
             return k_scale_rows(h, out, in, h->pdiag.data(), h->nm, NENK);
         };
@@ -244,7 +259,7 @@ static KrylovResult moment_solve(Handle* h, const double* b, double* phi, int so
         // Learned path: FGMRES(m) with the network as right preconditioner, capped at `budget` operator
         // applications (plain GMRES's count on this group in calibration), else 4m, and never beyond
         // the caller's limit.
-        DevOp pc = [h](const double* in, double* out) { return mlp_apply_precond(h, in, out); };
+        PrecOp pc = [h](const double* in, double scale, double* out) { return mlp_apply_precond(h, in, out, scale); };
         int cap = budget > 0 ? budget : 4 * m;
         if (maxit > 0) cap = std::min(cap, maxit);
         KrylovResult kr = gmres_device(h, n, b, phi, m, rtol, atol, cap, mv, &pc);

@@ -1193,6 +1193,12 @@ int launch_sweep(Handle* h, float* psi) {
         cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2, false, 2>);
     }
     Config cfg = kConfigs[cfg_idx];
+    // the autotuner skips the block schedule where it has more barrier levels than the element schedule
+    // (unstructured meshes, whose blocks are split on cycles): it cannot win there; a forced
+    // configuration still runs it
+    if ((cfg.kind == 5 || cfg.kind == 6) && h->sweep_cfg_forced >= kNumConfigs &&
+        h->cluster_levels_total > (long long)h->total_levels)
+        cfg = Config{0, 1024, 1, 2};
     // the element-flag schedule keeps one bit per element in shared memory
     if (cfg.kind == 3 && (size_t)((h->NE + 31) / 32) * 4 > 200 * 1024) cfg = Config{0, 1024, 1, 1};
     // the cluster schedule needs block records (built when every direction's block graph is acyclic)
@@ -1319,6 +1325,9 @@ int sweep_config(Handle* h, int* kind, int* threads, int* dpc, int* ilp) {
     int c = h->sweep_cfg_forced >= 0 && h->sweep_cfg_forced < kNumConfigs ? h->sweep_cfg_forced : h->sweep_cfg;
     if (c < 0) return -1;
     Config cfg = kConfigs[c];
+    if ((cfg.kind == 5 || cfg.kind == 6) && h->sweep_cfg_forced >= kNumConfigs &&
+        h->cluster_levels_total > (long long)h->total_levels)
+        cfg = Config{0, 1024, 1, 2};   // what the launcher runs instead
     if (cfg.kind == 5 && h->nclusters <= 0) cfg = Config{0, 1024, 1, 2};   // what the launcher runs instead
     if (cfg.kind == 6 && (h->nclusters <= 0 || h->ngeom <= 0))
         cfg = h->nclusters > 0 ? Config{5, 512, 2, 1} : Config{0, 1024, 1, 2};

@@ -46,7 +46,10 @@ def test_oblique_beam_on_a_two_material_box_matches_oracle(theta):
     prob = P.config1_small(n=(6, 6, 12))
     m = prob.mesh
     axis, e1, e2 = _frame(theta, 20.0)
-    origin = np.array([10.0, 10.0, 0.0]) - 3.0 * axis           # the beam plane before the mesh
+    # the beam plane beyond the mesh (40 cm from its centre along the axis; half its diagonal is 24.5 cm),
+    # as the reference's inputs place their beam origins: TraceVector counts no path in a region whose
+    # boundary the segment does not cross, so a plane through the mesh would leave such points unattenuated
+    origin = np.array([10.0, 10.0, 20.0]) - 40.0 * axis
     args = (origin, axis, e1, e2, 9.0, 7.0, [0.11, 0.297])
     gpu = _op(m).beam_uncollided(*args)
     ref = O.Oracle(m).beam_uncollided(*args)

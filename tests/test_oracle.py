@@ -230,7 +230,7 @@ def test_beam_ray_tracing_matches_closed_form(nmat):
     and the per-material branch), Beer's law and the FCSSource projection against the closed form of
     a normally incident beam through layers aligned with the mesh (4 x 4 x 8 hexes, 1 cm).  The beam
     plane lies 1 cm before the mesh, as the reference's inputs place their beam origins outside the
-    mesh (TraceVector drops a lone intersection at t ~ 0, RayTracing.f90:329-333)."""
+    mesh (TraceVector drops a lone intersection at t ~ 0, RayTracing.f90:327-335)."""
     from helpers import layered_beam_reference
     mat = None if nmat == 1 else (lambda c: ((c[:, 2] > 2.0) & (c[:, 2] < 4.0)).astype(np.int32))
     m = M.box_mesh(4, 4, 8, (0, 0, 0), (4.0, 4.0, 8.0), material=mat, Nm=nmat)
