@@ -13,6 +13,7 @@
 #include "lb_internal.h"
 #include "gmres_host.h"
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <functional>
 #include <omp.h>
@@ -119,6 +120,11 @@ static KrylovResult gmres_device(Handle* h, size_t n, const double* rhs, double*
     const double fpar4 = rtol * rn + atol;
     double fpar5 = 0.0;
     int nmv = 0;
+    // Stagnation: the operator applies FP32 sweeps, so a tolerance below what they resolve leaves the true
+    // residual at a floor while the cycle's residual estimate keeps reaching the target; five restarts in a
+    // row that do not lower the true residual by 1 % end the solve instead of cycling without end.
+    double best = HUGE_VAL;
+    int stalled = 0;
     while (true) {
         // r = rhs - A sol
         if ((rc = matvec(sol, V))) { res.status = rc; return res; }
@@ -130,6 +136,19 @@ static KrylovResult gmres_device(Handle* h, size_t n, const double* rhs, double*
         fpar5 = alpha;
         gh.start(alpha);
         if (alpha <= fpar4) { res.status = LB_OK; res.nmv = nmv; res.resid = alpha; return res; }
+        if (alpha < 0.99 * best) {
+            best = alpha;
+            stalled = 0;
+        } else if (++stalled >= 5) {
+            char msg[200];
+            std::snprintf(msg, sizeof msg,
+                          "GMRES stagnated: the true residual stays at %.3e against a target of %.3e (below what the "
+                          "FP32 sweep resolves)", alpha, fpar4);
+            res.status = fail(h, LB_ERR_NOCONV, msg);
+            res.nmv = nmv;
+            res.resid = alpha;
+            return res;
+        }
         sc[0] = 1.0 / alpha;
         G[0] = 1.0;
         int k = 0;

@@ -81,13 +81,13 @@ def test_preconditioner_kernel_matches_reference():
 def test_fgmres_without_network_is_plain_gmres():
     prob = P.config1_small(n=(4, 4, 8), G=2, Ng=4, Nc=8)
     a = MultigroupSolver().set_problem(prob)
-    it_a = a.solve("GMRES", m=20, rtol=1e-8)
+    it_a = a.solve("GMRES", m=20, rtol=1e-6)
     fa, da = a.results()
-    it_b = a.solve("FGMRES_ML", m=20, rtol=1e-8)
+    it_b = a.solve("FGMRES_ML", m=20, rtol=1e-6)
     fb, db = a.results()
     # same method; only the sweep launch shape (autotuner trials in the first solve) may differ
     assert np.abs(it_a - it_b).max() <= 1
-    assert rel_l2(db, da) < 1e-9
+    assert rel_l2(db, da) < 1e-7
 
 
 def _train_problems(G, n):

@@ -244,3 +244,17 @@ def test_fgmres_pinned_to_sparskit_fgmres(m):
     # the preconditioner is in effect: plain GMRES takes another number of operator applications
     _, _, plain = o.moment_solve(prob.Ls, prob.sigs[0, 0], q=q, m=m, rtol=1e-6)
     assert plain["iters"] != info["iters"]
+
+
+def test_gmres_stagnation_below_the_fp32_floor_is_reported():
+    """A tolerance below what the FP32 sweep resolves leaves the true residual at a floor: the solve
+    stops after five restarts without progress with LB_ERR_NOCONV (this case used to cycle through
+    about 200,000 operator applications before its residual dipped under 1e-8 by chance)."""
+    import time
+    prob = P.config1_small(n=(4, 4, 8), G=2, Ng=4, Nc=8)
+    mg = MultigroupSolver().set_problem(prob)
+    t0 = time.perf_counter()
+    with pytest.raises(_lib.LionboltError) as ei:
+        mg.solve("GMRES", m=20, rtol=1e-8)
+    assert ei.value.status == _lib.LB_ERR_NOCONV and "stagnated" in str(ei.value)
+    assert time.perf_counter() - t0 < 20
