@@ -213,8 +213,6 @@ class Handle:
                 d["schedule"] += "+element prefetch"
             if d["ilp"] >= 3:
                 d["schedule"] += "+previous in registers"
-            if d["ilp"] == 4:
-                d["schedule"] += "+records past L1"
         return d
 
     def mesh_types(self):

@@ -86,16 +86,6 @@ __device__ __forceinline__ float pick(const float4& v, int idx) {
     return r;
 }
 
-// 16-byte element record that does not take an L1 line (a direction reads each record once; L1 is
-// kept for the solution lines that downstream elements read back)
-__device__ __forceinline__ int4 ld_rec_na(const int4* p) {
-    int4 r;
-    asm volatile("ld.global.nc.L1::no_allocate.v4.s32 {%0, %1, %2, %3}, [%4];"
-                 : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
-                 : "l"(p));
-    return r;
-}
-
 __device__ __forceinline__ int ld_acquire(const int* p) {
     int v;
     asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -587,7 +577,7 @@ __global__ void __launch_bounds__(NT, MINB) sweep_cluster_kernel(SweepArgs a) {
                     pk = (pk >> 16) | ((unsigned long long)(pw & 0xFFFFu) << 48);
                     pw >>= 16;
                     int e = mem ? __ldg(&mem[f & 7u]) : e0 + (int)(f & 7u);
-                    int4 gn = PF == 3 ? ld_rec_na(&a.rec[e]) : __ldg(&a.rec[e]);
+                    int4 gn = __ldg(&a.rec[e]);
                     float4 q = ld4<false>(base + 4 * (size_t)e);
                     int prev_e = -1;
                     float4 prev_v = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -601,7 +591,7 @@ __global__ void __launch_bounds__(NT, MINB) sweep_cluster_kernel(SweepArgs a) {
                         int4 gn_n = gn;
                         float4 q_n = q;
                         if (more) {
-                            gn_n = PF == 3 ? ld_rec_na(&a.rec[en]) : __ldg(&a.rec[en]);
+                            gn_n = __ldg(&a.rec[en]);
                             q_n = ld4<false>(base + 4 * (size_t)en);
                         }
                         const int item = e | (int)(((f >> 3) & 0xFu) << 24) | (int)(((f >> 7) & 0xFu) << 28);
@@ -997,15 +987,14 @@ struct Config {
     int threads;
     int dpc;       // directions per CTA (kind 0); minimum CTAs per SM (kinds 2, 5)
     int ilp;       // updates in flight per thread (kind 0); kinds 5, 6: 2 = next element's record and source
-                   // prefetched, 3 = the same and the previous element's solution kept in registers, 4 = the
-                   // same with element records loaded without taking L1 lines
+                   // prefetched, 3 = the same and the previous element's solution kept in registers
 };
 
 const Config kConfigs[] = {
     {4, 1024, 2, 1}, {4, 512, 2, 1}, {4, 512, 3, 1}, {4, 1024, 3, 1}, {4, 512, 6, 1},
     {0, 1024, 1, 1}, {0, 512, 1, 1}, {2, 1024, 1, 1}, {3, 512, 0, 1}, {1, 256, 0, 0},
     {4, 768, 2, 1}, {0, 1024, 1, 2}, {0, 1024, 1, 3}, {0, 768, 1, 3}, {5, 1024, 1, 1}, {5, 512, 2, 1}, {5, 768, 2, 1}, {5, 1024, 2, 1},
-    {6, 512, 2, 1}, {6, 768, 2, 1}, {5, 512, 2, 2}, {6, 512, 2, 2}, {5, 512, 2, 3}, {5, 512, 2, 4},
+    {6, 512, 2, 1}, {6, 768, 2, 1}, {5, 512, 2, 2}, {6, 512, 2, 2}, {5, 512, 2, 3},
 };
 constexpr int kNumConfigs = sizeof(kConfigs) / sizeof(kConfigs[0]);
 constexpr int kFinalists = 3;   // candidates timed a second time before one is kept
@@ -1202,7 +1191,6 @@ int launch_sweep(Handle* h, float* psi) {
         cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2, false, 1>);
         cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2, true, 1>);
         cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2, false, 2>);
-        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2, false, 3>);
     }
     Config cfg = kConfigs[cfg_idx];
     // the autotuner skips the block schedule where it has more barrier levels than the element schedule
@@ -1247,7 +1235,6 @@ int launch_sweep(Handle* h, float* psi) {
                                   : launch_flags<512>(a, h->sm_count, h->stream);
     } else if ((cfg.kind == 5 || cfg.kind == 6) && cfg.ilp >= 2) {
         e = cfg.kind == 6   ? launch_cluster<512, 2, true, 1>(a, h->sm_count, h->stream)
-            : cfg.ilp == 4 ? launch_cluster<512, 2, false, 3>(a, h->sm_count, h->stream)
             : cfg.ilp == 3 ? launch_cluster<512, 2, false, 2>(a, h->sm_count, h->stream)
                            : launch_cluster<512, 2, false, 1>(a, h->sm_count, h->stream);
     } else if (cfg.kind == 5) {
