@@ -216,10 +216,15 @@ __global__ void __launch_bounds__(kM2dThreads, 1) m2d_tc_kernel(const int* __res
             const long long n = tile * kTM + r;
             const bool valid = n < NENK;
             double raw[HM];
+            {
+                // one pointer stepped by a row (NENK) per moment instead of a 64-bit index per load
+                const double* sp = src + (size_t)(side * HM) * (size_t)NENK + (valid ? n : 0);
+                const int jn = valid ? nm - side * HM : 0;   // moments of this half that exist
 #pragma unroll
-            for (int k = 0; k < HM; ++k) {
-                const int j = side * HM + k;
-                raw[k] = (valid && j < nm) ? __ldcs(&src[(size_t)j * NENK + n]) : 0.0;
+                for (int k = 0; k < HM; ++k) {
+                    raw[k] = k < jn ? __ldcs(sp) : 0.0;
+                    sp += NENK;
+                }
             }
             const int m = valid ? __ldg(&mat[n >> 2]) : 0;
             if (u > 0 && !bar_wait(&done[b], (u - 1) & 1u, err)) break;
@@ -270,15 +275,25 @@ __global__ void __launch_bounds__(kM2dThreads, 1) m2d_tc_kernel(const int* __res
                 float v[16];
                 tmem_ld16(lane_base + (uint32_t)(b * 256 + g * 16), v);
                 if (valid) {
+                    const int i0 = half * NH + g * 16;
+                    const size_t o0 = (size_t)i0 * (size_t)NENK + (size_t)n;
+                    // plain (write-back) stores: the tile's 512-byte row pieces stay in L2 until the
+                    // neighbouring tiles' pieces join them (evict-first stores: 5 % slower)
+                    if (!qadd && i0 + 16 <= NI) {
+                        // the common case, one pointer stepped by a row per direction
+                        float* qp = q + o0;
 #pragma unroll
-                    for (int k = 0; k < 16; ++k) {
-                        const int i = half * NH + g * 16 + k;
-                        if (i < NI) {
-                            float o = v[k];
-                            if (qadd) o += qadd[(size_t)i * NENK + n];
-                            // plain (write-back) stores: the tile's 512-byte row pieces stay in L2 until
-                            // the neighbouring tiles' pieces join them (evict-first stores: 5 % slower)
-                            q[(size_t)i * NENK + n] = o;
+                        for (int k = 0; k < 16; ++k) {
+                            *qp = v[k];
+                            qp += NENK;
+                        }
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < 16; ++k) {
+                            if (i0 + k < NI) {
+                                const size_t o = o0 + (size_t)k * (size_t)NENK;
+                                q[o] = qadd ? v[k] + qadd[o] : v[k];
+                            }
                         }
                     }
                 }
@@ -391,10 +406,15 @@ __global__ void __launch_bounds__(kD2mThreads, 1) d2m_tc_kernel(const int* __res
             const int s = (int)(c % kStages);
             const uint32_t u = (uint32_t)(c / kStages);
             float v[24];
+            {
+                const int i0 = ch * kKC + side * 24;
+                const float* pp = psi + (size_t)i0 * (size_t)NENK + (valid ? n : 0);
+                const int kn = valid ? NI - i0 : 0;   // directions of this half-chunk that exist
 #pragma unroll
-            for (int k = 0; k < 24; ++k) {
-                const int i = ch * kKC + side * 24 + k;
-                v[k] = (valid && i < NI) ? __ldcs(&psi[(size_t)i * NENK + n]) : 0.f;
+                for (int k = 0; k < 24; ++k) {
+                    v[k] = k < kn ? __ldcs(pp) : 0.f;
+                    pp += NENK;
+                }
             }
             if (u > 0 && !bar_wait(&done[s], (u - 1) & 1u, err)) break;
             unsigned char* A = sA + s * abuf;
@@ -424,8 +444,16 @@ __global__ void __launch_bounds__(kD2mThreads, 1) d2m_tc_kernel(const int* __res
             const long long n = tile * kTM + r;
             const bool valid = n < NENK;
             double xv[16];
+            const bool hx = xin && valid;
+            const size_t nn = valid ? (size_t)n : 0;
+            {
+                const double* xp = hx ? xin + nn : nullptr;
 #pragma unroll
-            for (int k = 0; k < 16; ++k) xv[k] = (xin && valid && k < nm) ? xin[(size_t)k * NENK + n] : 0.0;
+                for (int k = 0; k < 16; ++k) {
+                    xv[k] = (hx && k < nm) ? *xp : 0.0;
+                    if (hx) xp += NENK;
+                }
+            }
             if (!bar_wait(&dfull[b], u & 1u, err)) break;
             tc_after_sync();
 #pragma unroll
@@ -433,18 +461,23 @@ __global__ void __launch_bounds__(kD2mThreads, 1) d2m_tc_kernel(const int* __res
                 float v[16];
                 tmem_ld16(lane_base + (uint32_t)(b * 64 + g * 16), v);
                 if (valid) {
+                    // one pointer stepped by a row per moment
+                    double* op = out + (size_t)(g * 16) * (size_t)NENK + nn;
+                    const int jn = nm - g * 16;
 #pragma unroll
                     for (int k = 0; k < 16; ++k) {
-                        const int j = g * 16 + k;
-                        if (j < nm) out[(size_t)j * NENK + n] = beta * (double)v[k] + alpha * xv[k];
+                        if (k < jn) *op = beta * (double)v[k] + alpha * xv[k];
+                        op += NENK;
                     }
                 }
                 // the next group's inputs
                 if (g + 1 < KT) {
+                    const double* xp = hx ? xin + (size_t)((g + 1) * 16) * (size_t)NENK + nn : nullptr;
+                    const int jn = nm - (g + 1) * 16;
 #pragma unroll
                     for (int k = 0; k < 16; ++k) {
-                        const int j = (g + 1) * 16 + k;
-                        xv[k] = (xin && valid && j < nm) ? xin[(size_t)j * NENK + n] : 0.0;
+                        xv[k] = (hx && k < jn) ? *xp : 0.0;
+                        if (hx) xp += NENK;
                     }
                 }
             }
