@@ -229,20 +229,21 @@ __global__ void __launch_bounds__(kM2dThreads, 1) m2d_tc_kernel(const int* __res
             const int m = valid ? __ldg(&mat[n >> 2]) : 0;
             if (u > 0 && !bar_wait(&done[b], (u - 1) & 1u, err)) break;
             unsigned char* A = sA + b * abuf;
+            // this half's sigma_l(j) row of the node's material (the table is padded to nmpad with zeros, and
+            // raw[] is zero past the moments that exist, so no per-value bounds test is needed)
+            const float* sg = sigl + (size_t)m * nmpad + side * HM;
+            const int jn = valid ? nm - side * HM : 0;
+            const double* ap = (x && add && valid) ? add + (size_t)(side * HM) * (size_t)NENK + n : nullptr;
 #pragma unroll
             for (int cl = 0; cl < HM / 8; ++cl) {
                 float v[8];
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
-                    const int j = side * HM + cl * 8 + k;
-                    double sv = 0.0;
-                    if (valid && j < nm) {
-                        if (x) {
-                            sv = (double)__ldg(&sigl[(size_t)m * nmpad + j]) * raw[cl * 8 + k];
-                            if (add) sv += __ldcs(&add[(size_t)j * NENK + n]);
-                        } else {
-                            sv = raw[cl * 8 + k];
-                        }
+                    const int kk = cl * 8 + k;
+                    double sv = raw[kk];
+                    if (x) {
+                        sv = (double)__ldg(&sg[kk]) * sv;
+                        if (ap && kk < jn) sv += __ldcs(ap + (size_t)kk * (size_t)NENK);
                     }
                     v[k] = (float)sv;
                 }
