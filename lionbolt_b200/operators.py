@@ -312,6 +312,20 @@ class MultigroupSolver(_Op):
         self._h.call("lb_mg_get_results", dptr(flux), dptr(dose))
         return flux, dose
 
+    def write_results(self, path, particle="photon", energy_grid=None, uncollided=True, problem_type="general"):
+        """Results file of the last solve in the reference's layout (LionboltHDF5.f90, Main.f90:118-231,
+        :449-469, :807-821): the mesh, the particle group with its energy grid, ordinates and per-group
+        fluence (and the beam's uncollided fluence in group 1), the dose deposition in the root."""
+        from . import lionbolt_hdf5
+        flux, dose = self.results()
+        unc = None
+        if uncollided and np.any(self.prob.unc):
+            unc = np.zeros_like(flux)
+            unc[0] = self.prob.unc
+        E = energy_grid if energy_grid is not None else self.prob.energy
+        return lionbolt_hdf5.write_results(path, self.mesh, self.prob.w, self.prob.k, flux, dose, particle=particle,
+                                           energy_grid=E, uncollided=unc, problem_type=problem_type)
+
 
 class BatchSolver:
     """Many independent multigroup dose problems solved together on one GPU (lb_batch_* C ABI):

@@ -39,6 +39,7 @@ class Problem:
     dd: np.ndarray         # [G, Nm]
     unc: np.ndarray        # [NENK] uncollided scalar flux of the beam (group 0)
     beam_dir: np.ndarray   # [3]
+    energy: np.ndarray = None   # [G + 1] group bounds (MeV), when the builder defines them
 
     @property
     def NI(self):
@@ -136,7 +137,7 @@ def multigroup_box(n=(40, 40, 80), size=(20.0, 20.0, 40.0), Ng=12, Nc=24, G=20, 
     bdir = np.array([np.sin(th), 0.0, np.cos(th)])
     layers = [(0.0, slab[0], st_water[0]), (slab[0], slab[1], slab_scale * st_water[0]), (slab[1], sz, st_water[0])]
     unc = beam_uncollided(m, bdir, (0.5 * sx, 0.5 * sy), beam_width, layers)
-    return Problem(name, m, k, w, Ng, Nc, G, Ls, sigt, sigs, dd, unc, bdir)
+    return Problem(name, m, k, w, Ng, Nc, G, Ls, sigt, sigs, dd, unc, bdir, energy)
 
 
 def config1():
