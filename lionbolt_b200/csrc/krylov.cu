@@ -259,30 +259,16 @@ __global__ void __launch_bounds__(256) group_source_kernel(double* __restrict__ 
                                                           const double* __restrict__ unc,
                                                           const double* __restrict__ ybeam, const int* __restrict__ mat,
                                                           long long NENK, int Nm, int nm, int nmpad) {
-    // Moments in chunks of JC accumulators with the source groups g' outermost: JC independent loads of
-    // phi_{g'} in flight per thread; every accumulator still sums g' = 0, 1, ... in order.
-    constexpr int JC = 12;
     const size_t nvec = (size_t)nm * NENK;
-    const size_t tstride = (size_t)G * Nm * nmpad;   // g' -> g' + 1 in the (g', g, m, j) table
     for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < NENK; n += (long long)gridDim.x * blockDim.x) {
         const int m = mat[n >> 2];
         const double u = unc ? unc[n] : 0.0;
         const float* t0 = tab + ((size_t)g * Nm + m) * nmpad;   // (g' = 0, g)
-        for (int j0 = 0; j0 < nm; j0 += JC) {
-            double acc[JC];
-#pragma unroll
-            for (int jj = 0; jj < JC; ++jj)
-                acc[jj] = (j0 + jj < nm) ? (double)t0[j0 + jj] * ybeam[j0 + jj] * u : 0.0;
-            const float* tg = t0 + j0;
-            const double* pg = phi_all + (size_t)j0 * NENK + n;
-            for (int gp = 0; gp < g; ++gp, tg += tstride, pg += nvec) {
-#pragma unroll
-                for (int jj = 0; jj < JC; ++jj)
-                    if (j0 + jj < nm) acc[jj] += (double)tg[jj] * pg[(size_t)jj * NENK];
-            }
-#pragma unroll
-            for (int jj = 0; jj < JC; ++jj)
-                if (j0 + jj < nm) src[(size_t)(j0 + jj) * NENK + n] = acc[jj];
+        for (int j = 0; j < nm; ++j) {
+            double acc = (double)t0[j] * ybeam[j] * u;
+            for (int gp = 0; gp < g; ++gp)
+                acc += (double)tab[(((size_t)gp * G + g) * Nm + m) * nmpad + j] * phi_all[(size_t)gp * nvec + (size_t)j * NENK + n];
+            src[(size_t)j * NENK + n] = acc;
         }
     }
 }
