@@ -19,6 +19,7 @@
 // accumulators synchronised by mbarriers; every wait is bounded and sets an error flag instead of
 // hanging.
 #include "lb_internal.h"
+#include <cuda.h>
 #include <algorithm>
 #include <cstdlib>
 
@@ -523,6 +524,257 @@ __global__ void __launch_bounds__(kD2mThreads, 1) d2m_tc_kernel(const int* __res
     if (warp == kD2mMma) tmem_free(tmem, 128);
 }
 
+// ---------------------------------------------------------------------------------------------
+// D2M with the angular vector streamed by the tensor-memory accelerator: the same product as
+// d2m_tc_kernel, with psi brought into a ring of kT32 shared-memory stages by
+// cp.async.bulk.tensor (a 2-D tensor map over psi[NI][NENK], box = 128 nodes x kKT directions;
+// directions past NI and nodes past NENK are filled with zeros), so no thread waits on a global
+// load.  Chunks of kKT = 32 directions (two MMA K-steps):
+//   warp 0 lane 0    TMA issue: waits for a free FP32 stage, arms its barrier with the byte count and
+//                    issues the copy;
+//   warps 1-16       converters, two sets of 8 warps taking alternate chunks: threads t and t + 128 of a
+//                    set take node t & 127 of the tile and 16 directions each, read them from the FP32
+//                    stage (then release it), split them into BF16 planes and write the A stage;
+//   warps 17-20      epilogue, as d2m_tc_kernel;
+//   warp 21          lane 0 issues the MMAs; the warp owns the TMEM allocation.
+// Every wait is bounded (error flag), as in the other kernels.  No cluster, no multicast.
+// ---------------------------------------------------------------------------------------------
+constexpr int kKT = 32;        // directions per K chunk
+constexpr int kT32 = 5;        // FP32 stages (TMA ring)
+constexpr int kTA = 2;         // BF16 A stages
+constexpr int kD2tSets = 2;    // converter sets of 8 warps, taking alternate chunks
+constexpr int kD2tConv = 1;    // first converter warp
+constexpr int kD2tEpi = kD2tConv + 8 * kD2tSets;   // first epilogue warp
+constexpr int kD2tMma = kD2tEpi + 4;               // the MMA warp
+constexpr int kD2tThreads = 32 * (kD2tMma + 1);
+
+__device__ __forceinline__ void bar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+template <int KT>
+__global__ void __launch_bounds__(kD2tThreads, 1) d2m_tma_kernel(const __grid_constant__ CUtensorMap psi_map,
+                                                      const int* __restrict__ active,
+                                                      const __nv_bfloat16* __restrict__ Dw, const double* xin,
+                                                      double alpha, double beta, double* out, long long NENK, int NI,
+                                                      int NIpad, int nm, int nmpad, long long ntiles, int* err) {
+    if (active && *active == 0) return;
+    extern __shared__ __align__(1024) unsigned char sm[];
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int NKpad = (NIpad + kKT - 1) / kKT * kKT;
+    const size_t bplane = (size_t)nmpad * NKpad * 2;
+    const size_t aplane = (size_t)kTM * kKT * 2;
+    const size_t abuf = ((3 * aplane + 1023) / 1024) * 1024;
+    constexpr size_t fbuf = (size_t)kTM * kKT * 4;                       // one FP32 stage
+    unsigned char* sB = sm;
+    unsigned char* sF = sm + ((3 * bplane + 1023) / 1024) * 1024;       // [kT32] FP32 stages
+    unsigned char* sA = sF + kT32 * fbuf;                                // [kTA] A stages
+    uint64_t* tfull = reinterpret_cast<uint64_t*>(sA + kTA * abuf);      // [kT32]
+    uint64_t* tempty = tfull + kT32;                                     // [kT32]
+    uint64_t* afull = tempty + kT32;                                     // [kTA]
+    uint64_t* adone = afull + kTA;                                       // [kTA]
+    uint64_t* dfull = adone + kTA;                                       // [2]
+    uint64_t* dempty = dfull + 2;                                        // [2]
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(dempty + 2);
+    {   // B = Dw planes [3][nmpad][NIpad] staged K-major: rows = moments, K = directions
+        const int cc = NKpad / 8;
+        const int total = 3 * nmpad * cc;
+        for (int u = tid; u < total; u += blockDim.x) {
+            const int p = u / (nmpad * cc);
+            const int rem = u % (nmpad * cc);
+            const int r = rem / cc, c = rem % cc;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (c * 8 < NIpad) v = __ldg(reinterpret_cast<const uint4*>(Dw + ((size_t)p * nmpad + r) * NIpad) + c);
+            *reinterpret_cast<uint4*>(sB + p * bplane + (size_t)c * nmpad * 16 + (size_t)r * 16) = v;
+        }
+    }
+    if (tid == 0) {
+        for (int k = 0; k < kT32; ++k) {
+            bar_init(&tfull[k], 1);
+            bar_init(&tempty[k], 256);
+        }
+        for (int k = 0; k < kTA; ++k) {
+            bar_init(&afull[k], 256);
+            bar_init(&adone[k], 1);
+        }
+        for (int k = 0; k < 2; ++k) {
+            bar_init(&dfull[k], 1);
+            bar_init(&dempty[k], 128);
+        }
+    }
+    if (warp == kD2tMma) tmem_alloc(tslot, 128);
+    fence_async_smem();
+    tc_before_sync();
+    __syncthreads();
+    tc_after_sync();
+    const uint32_t tmem = *tslot;
+    const int nchunks = NKpad / kKT;
+    const long long my_tiles = (ntiles - 1 - (long long)blockIdx.x) / gridDim.x + 1;
+    const long long nch = my_tiles * nchunks;
+    if (warp == 0) {
+        // ---- TMA issue ----
+        if ((tid & 31) == 0) {
+            for (long long c = 0; c < nch; ++c) {
+                const int s = (int)(c % kT32);
+                const uint32_t u = (uint32_t)(c / kT32);
+                if (u > 0 && !bar_wait(&tempty[s], (u - 1) & 1u, err)) break;
+                const long long tile = blockIdx.x + (c / nchunks) * gridDim.x;
+                const int ch = (int)(c % nchunks);
+                bar_expect_tx(&tfull[s], (uint32_t)fbuf);
+                tma_load_2d(sF + s * fbuf, &psi_map, (int)(tile * kTM), ch * kKT, &tfull[s]);
+            }
+        }
+    } else if (warp < kD2tEpi) {
+        // ---- converters: FP32 stage -> BF16 planes of the A stage; set `set` takes chunks c = set mod kD2tSets ----
+        const int t = tid - 32 * kD2tConv;
+        const int row = t & 127, side = (t >> 7) & 1, set = t >> 8;
+        for (long long c = set; c < nch; c += kD2tSets) {
+            const int s = (int)(c % kT32);
+            const int sa = (int)(c % kTA);
+            if (!bar_wait(&tfull[s], (uint32_t)(c / kT32) & 1u, err)) break;
+            const float* F = reinterpret_cast<const float*>(sF + s * fbuf) + (size_t)(side * 16) * kTM + row;
+            float v[16];
+#pragma unroll
+            for (int k = 0; k < 16; ++k) v[k] = F[(size_t)k * kTM];
+            bar_arrive(&tempty[s]);
+            const uint32_t ua = (uint32_t)(c / kTA);
+            if (ua > 0 && !bar_wait(&adone[sa], (ua - 1) & 1u, err)) break;
+            unsigned char* A = sA + sa * abuf;
+#pragma unroll
+            for (int cl = 0; cl < 2; ++cl) {
+                float w[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) w[k] = v[cl * 8 + k];
+                uint4 hi, mid, lo;
+                split8(w, hi, mid, lo);
+                unsigned char* rp = A + (size_t)(side * 2 + cl) * kTM * 16 + (size_t)row * 16;
+                *reinterpret_cast<uint4*>(rp) = hi;
+                *reinterpret_cast<uint4*>(rp + aplane) = mid;
+                *reinterpret_cast<uint4*>(rp + 2 * aplane) = lo;
+            }
+            fence_async_smem();
+            bar_arrive(&afull[sa]);
+        }
+    } else if (warp < kD2tMma) {
+        // ---- epilogue: a warp reads TMEM lanes 32(w%4).. (the hardware's lane quarter of warp w), i.e.
+        // tile nodes 32(w%4) + lane ----
+        const int r = ((warp & 3) << 5) | (tid & 31);
+        const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+        int it = 0;
+        for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+            const int b = it & 1;
+            const uint32_t u = (uint32_t)(it >> 1);
+            const long long n = tile * kTM + r;
+            const bool valid = n < NENK;
+            double xv[16];
+            const bool hx = xin && valid;
+            const size_t nn = valid ? (size_t)n : 0;
+            {
+                const double* xp = hx ? xin + nn : nullptr;
+#pragma unroll
+                for (int k = 0; k < 16; ++k) {
+                    xv[k] = (hx && k < nm) ? *xp : 0.0;
+                    if (hx) xp += NENK;
+                }
+            }
+            if (!bar_wait(&dfull[b], u & 1u, err)) break;
+            tc_after_sync();
+#pragma unroll
+            for (int g = 0; g < KT; ++g) {
+                float v[16];
+                tmem_ld16(lane_base + (uint32_t)(b * 64 + g * 16), v);
+                if (valid) {
+                    double* op = out + (size_t)(g * 16) * (size_t)NENK + nn;
+                    const int jn = nm - g * 16;
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) {
+                        if (k < jn) *op = beta * (double)v[k] + alpha * xv[k];
+                        op += NENK;
+                    }
+                }
+                if (g + 1 < KT) {
+                    const double* xp = hx ? xin + (size_t)((g + 1) * 16) * (size_t)NENK + nn : nullptr;
+                    const int jn = nm - (g + 1) * 16;
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) {
+                        xv[k] = (hx && k < jn) ? *xp : 0.0;
+                        if (hx) xp += NENK;
+                    }
+                }
+            }
+            tc_before_sync();
+            bar_arrive(&dempty[b]);
+        }
+    } else if ((tid & 31) == 0) {
+        // ---- MMA issue ----
+        const uint32_t idesc = idesc_bf16(kTM, nmpad);
+        const uint32_t lboA = kTM * 16, lboB = (uint32_t)nmpad * 16;
+        const uint32_t aBase = smem_u32(sA), bBase = smem_u32(sB);
+        long long c = 0;
+        int it = 0;
+        bool ok = true;
+        for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++it) {
+            const int b = it & 1;
+            const uint32_t ut = (uint32_t)(it >> 1);
+            if (ut > 0 && !bar_wait(&dempty[b], (ut - 1) & 1u, err)) break;
+            for (int ch = 0; ch < nchunks; ++ch, ++c) {
+                const int sa = (int)(c % kTA);
+                if (!bar_wait(&afull[sa], (uint32_t)(c / kTA) & 1u, err)) {
+                    ok = false;
+                    break;
+                }
+                tc_after_sync();
+                const uint32_t a0 = aBase + sa * (uint32_t)abuf;
+                for (int ks = 0; ks < kKT / 16; ++ks)
+                    for (int pr = 0; pr < 6; ++pr) {
+                        const uint64_t da = sdesc(a0 + kProdA[pr] * (uint32_t)aplane + ks * 2 * lboA, lboA, 128);
+                        const uint64_t db = sdesc(bBase + kProdB[pr] * (uint32_t)bplane +
+                                                      (uint32_t)(ch * (kKT / 8) + ks * 2) * lboB, lboB, 128);
+                        mma_bf16_ss(tmem + b * 64, da, db, idesc, (ch | ks | pr) ? 1u : 0u);
+                    }
+                mma_commit(&adone[sa]);
+                if (ch == nchunks - 1) mma_commit(&dfull[b]);
+            }
+        }
+    }
+    tc_before_sync();
+    __syncthreads();
+    if (warp == kD2tMma) tmem_free(tmem, 128);
+}
+
+size_t d2m_tma_smem(int NIpad, int nmpad) {
+    const int NKpad = (NIpad + kKT - 1) / kKT * kKT;
+    const size_t b = ((3 * (size_t)nmpad * NKpad * 2 + 1023) / 1024) * 1024;
+    const size_t a = ((3 * (size_t)kTM * kKT * 2 + 1023) / 1024) * 1024;
+    return b + kT32 * (size_t)kTM * kKT * 4 + kTA * a + 8 * (2 * kT32 + 2 * kTA + 4) + 16;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
 size_t m2d_tc_smem(int NH, int nmpad) {
     const size_t b = ((3 * (size_t)NH * nmpad * 2 + 1023) / 1024) * 1024;
     const size_t a = ((3 * (size_t)kTM * nmpad * 2 + 1023) / 1024) * 1024;
@@ -589,7 +841,65 @@ int launch_m2d_tc(Handle* h, const double* x, const float* sigl, const double* a
     return e == cudaSuccess ? LB_OK : cuda_fail(h, e, "m2d tensor-core kernel");
 }
 
+bool d2m_tma_enabled() {
+    static int on = -1;
+    if (on < 0) {
+        const char* e = std::getenv("LB_D2M_TMA");
+        on = (e && *e == '0') ? 0 : 1;
+    }
+    return on == 1;
+}
+
+// The TMA-fed D2M; LB_ERR_ARG when it does not apply (no tensor-map encoder, shape, alignment).
+int launch_d2m_tma(Handle* h, const float* psi, const double* xin, double alpha, double beta, double* out) {
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc || !d2m_tma_enabled()) return LB_ERR_ARG;
+    if (h->nmpad > 64 || h->nmpad % 16 || h->NIpad % 8 || ((uintptr_t)psi & 15) || (h->NENK * 4) % 16 ||
+        h->NENK >= (1LL << 31) || h->NI < 1)
+        return LB_ERR_ARG;
+    const size_t smem = std::max<size_t>(d2m_tma_smem(h->NIpad, h->nmpad), 116 * 1024);
+    if (smem > 227 * 1024) return LB_ERR_ARG;
+    int* err = tc_error_flag();
+    if (!err) return LB_ERR_OOM;
+    // tensor map over psi[NI][NENK] (FP32): box 128 nodes x kKT directions, zero fill outside
+    CUtensorMap map;
+    const cuuint64_t dims[2] = {(cuuint64_t)h->NENK, (cuuint64_t)h->NI};
+    const cuuint64_t strides[1] = {(cuuint64_t)h->NENK * 4};
+    const cuuint32_t box[2] = {(cuuint32_t)kTM, (cuuint32_t)kKT};
+    const cuuint32_t estr[2] = {1, 1};
+    if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(psi), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return LB_ERR_ARG;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(d2m_tma_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(d2m_tma_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(d2m_tma_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(d2m_tma_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        attr = true;
+    }
+    const long long ntiles = (h->NENK + kTM - 1) / kTM;
+    const long long grid = std::min<long long>(ntiles, (long long)h->sm_count);
+#define LB_D2MTMA(K)                                                                                                \
+    d2m_tma_kernel<K><<<(int)grid, kD2tThreads, smem, h->stream>>>(map, h->d_active, h->d_Yd2m, xin, alpha, beta, out, \
+                                                                h->NENK, h->NI, h->NIpad, h->nm, h->nmpad, ntiles, err)
+    switch (h->nmpad / 16) {
+        case 1: LB_D2MTMA(1); break;
+        case 2: LB_D2MTMA(2); break;
+        case 3: LB_D2MTMA(3); break;
+        default: LB_D2MTMA(4); break;
+    }
+#undef LB_D2MTMA
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? LB_OK : cuda_fail(h, e, "d2m TMA kernel");
+}
+
 int launch_d2m_tc(Handle* h, const float* psi, const double* xin, double alpha, double beta, double* out) {
+    {
+        const int rc = launch_d2m_tma(h, psi, xin, alpha, beta, out);
+        if (rc != LB_ERR_ARG) return rc;
+    }
     if (h->nmpad > 64 || h->nmpad % 16 || h->NIpad % 8) return LB_ERR_ARG;
     // one CTA per SM (two accumulators of up to 64 columns in a 128-column allocation)
     const size_t smem = std::max<size_t>(d2m_tc_smem(h->NIpad, h->nmpad), 116 * 1024);
