@@ -99,6 +99,28 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
 }
 
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = __uint_as_float(r[k]);
+}
+
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float (&v)[16]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};"
+        ::"r"(taddr), "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+          "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])), "r"(__float_as_uint(v[6])),
+          "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])), "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])),
+          "r"(__float_as_uint(v[11])), "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])),
+          "r"(__float_as_uint(v[14])), "r"(__float_as_uint(v[15]))
+        : "memory");
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
 // The warp calling this allocates ncols TMEM columns (power of two >= 32) and publishes the base.
 __device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)), "r"(ncols)
@@ -153,6 +175,18 @@ __device__ void stage_kmajor(const __nv_bfloat16* __restrict__ g, int rows, int 
 
 __device__ __forceinline__ void bar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Tensor-memory-accelerator load of a 2-D box (no multicast): the mbarrier completes when its bytes land.
+__device__ __forceinline__ void bar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -339,6 +373,7 @@ __global__ void __launch_bounds__(kM2dThreads, 1) m2d_tc_kernel(const int* __res
 //               and splits 24 directions of the chunk;
 //   next 4 warps  epilogue (TMEM lanes 32(w%4)..): out rows of the tile (two accumulators);
 //   last warp   lane 0 issues the MMAs; the warp owns the TMEM allocation.
+// The leading split product and the five smaller ones accumulate separately, as in d2m_tma_kernel.
 // ---------------------------------------------------------------------------------------------
 constexpr int kKC = 48;       // directions per K chunk (3 MMA K-steps)
 constexpr int kStages = 3;    // A ring depth
@@ -388,7 +423,7 @@ __global__ void __launch_bounds__(kD2mThreads, 1) d2m_tc_kernel(const int* __res
             bar_init(&dempty[k], 128);
         }
     }
-    if (warp == kD2mMma) tmem_alloc(tslot, 128);
+    if (warp == kD2mMma) tmem_alloc(tslot, 256);   // per tile buffer: leading-product and correction accumulators
     fence_async_smem();
     tc_before_sync();
     __syncthreads();
@@ -460,8 +495,15 @@ __global__ void __launch_bounds__(kD2mThreads, 1) d2m_tc_kernel(const int* __res
             tc_after_sync();
 #pragma unroll
             for (int g = 0; g < KT; ++g) {
-                float v[16];
-                tmem_ld16(lane_base + (uint32_t)(b * 64 + g * 16), v);
+                // the leading product's accumulator plus the correction products' accumulator (IEEE FP32)
+                float v[16], w[8];
+                tmem_ld16(lane_base + (uint32_t)(b * 128 + g * 16), v);
+                tmem_ld8(lane_base + (uint32_t)(b * 128 + 64 + g * 16), w);   // in halves: registers
+#pragma unroll
+                for (int k = 0; k < 8; ++k) v[k] += w[k];
+                tmem_ld8(lane_base + (uint32_t)(b * 128 + 64 + g * 16 + 8), w);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) v[8 + k] += w[k];
                 if (valid) {
                     // one pointer stepped by a row per moment
                     double* op = out + (size_t)(g * 16) * (size_t)NENK + nn;
@@ -512,7 +554,10 @@ __global__ void __launch_bounds__(kD2mThreads, 1) d2m_tc_kernel(const int* __res
                         const uint64_t da = sdesc(a0 + kProdA[pr] * (uint32_t)aplane + ks * 2 * lboA, lboA, 128);
                         const uint64_t db = sdesc(bBase + kProdB[pr] * (uint32_t)bplane +
                                                       (uint32_t)(ch * (kKC / 8) + ks * 2) * lboB, lboB, 128);
-                        mma_bf16_ss(tmem + b * 64, da, db, idesc, (ch | ks | pr) ? 1u : 0u);
+                        // product 5 (hi x hi) alone in columns b*128.., the five smaller ones in b*128 + 64..
+                        const bool lead = pr == 5;
+                        const uint32_t acc = lead ? (uint32_t)(ch | ks) : (uint32_t)(ch | ks | pr);
+                        mma_bf16_ss(tmem + b * 128 + (lead ? 0u : 64u), da, db, idesc, acc ? 1u : 0u);
                     }
                 mma_commit(&done[s]);
                 if (ch == nchunks - 1) mma_commit(&dfull[b]);
@@ -521,7 +566,7 @@ __global__ void __launch_bounds__(kD2mThreads, 1) d2m_tc_kernel(const int* __res
     }
     tc_before_sync();
     __syncthreads();
-    if (warp == kD2mMma) tmem_free(tmem, 128);
+    if (warp == kD2mMma) tmem_free(tmem, 256);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -532,32 +577,27 @@ __global__ void __launch_bounds__(kD2mThreads, 1) d2m_tc_kernel(const int* __res
 // load.  Chunks of kKT = 32 directions (two MMA K-steps):
 //   warp 0 lane 0    TMA issue: waits for a free FP32 stage, arms its barrier with the byte count and
 //                    issues the copy;
-//   warps 1-16       converters, two sets of 8 warps taking alternate chunks: threads t and t + 128 of a
-//                    set take node t & 127 of the tile and 16 directions each, read them from the FP32
-//                    stage (then release it), split them into BF16 planes and write the A stage;
-//   warps 17-20      epilogue, as d2m_tc_kernel;
-//   warp 21          lane 0 issues the MMAs; the warp owns the TMEM allocation.
+//   warps 1-8        converters (kD2tSets sets of 8 warps taking alternate chunks; one set: 14 warps,
+//                    at most 4 per SM sub-partition, so up to 128 registers a thread): threads t and
+//                    t + 128 of a set take node t & 127 of the tile and 16 directions each, read them
+//                    from the FP32 stage (then release it), split them into BF16 planes and write the
+//                    A stage;
+//   warps 9-12       epilogue, as d2m_tc_kernel (the warps index nodes by their TMEM lane quarter);
+//   warp 13          lane 0 issues the MMAs; the warp owns the TMEM allocation.
+// The leading split product (hi x hi) accumulates in its own TMEM accumulator and the five smaller
+// products in a second one, added in the epilogue: the tensor core's accumulation of the full-size
+// terms then runs over 18 MMAs per tile (288 directions) instead of all 108, which is where the split
+// product lost accuracy against an FP32 GEMM (the small terms' accumulator is 2^-8 of the result).
 // Every wait is bounded (error flag), as in the other kernels.  No cluster, no multicast.
 // ---------------------------------------------------------------------------------------------
 constexpr int kKT = 32;        // directions per K chunk
 constexpr int kT32 = 5;        // FP32 stages (TMA ring)
 constexpr int kTA = 2;         // BF16 A stages
-constexpr int kD2tSets = 2;    // converter sets of 8 warps, taking alternate chunks
+constexpr int kD2tSets = 1;    // converter sets of 8 warps, taking alternate chunks
 constexpr int kD2tConv = 1;    // first converter warp
 constexpr int kD2tEpi = kD2tConv + 8 * kD2tSets;   // first epilogue warp
 constexpr int kD2tMma = kD2tEpi + 4;               // the MMA warp
 constexpr int kD2tThreads = 32 * (kD2tMma + 1);
-
-__device__ __forceinline__ void bar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
-        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
-        : "memory");
-}
 
 template <int KT>
 __global__ void __launch_bounds__(kD2tThreads, 1) d2m_tma_kernel(const __grid_constant__ CUtensorMap psi_map,
@@ -609,7 +649,7 @@ __global__ void __launch_bounds__(kD2tThreads, 1) d2m_tma_kernel(const __grid_co
             bar_init(&dempty[k], 128);
         }
     }
-    if (warp == kD2tMma) tmem_alloc(tslot, 128);
+    if (warp == kD2tMma) tmem_alloc(tslot, 256);   // per tile buffer: leading-product and correction accumulators
     fence_async_smem();
     tc_before_sync();
     __syncthreads();
@@ -688,8 +728,12 @@ __global__ void __launch_bounds__(kD2tThreads, 1) d2m_tma_kernel(const __grid_co
             tc_after_sync();
 #pragma unroll
             for (int g = 0; g < KT; ++g) {
-                float v[16];
-                tmem_ld16(lane_base + (uint32_t)(b * 64 + g * 16), v);
+                // the leading product's accumulator plus the correction products' accumulator (IEEE FP32)
+                float v[16], w[16];
+                tmem_ld16(lane_base + (uint32_t)(b * 128 + g * 16), v);
+                tmem_ld16(lane_base + (uint32_t)(b * 128 + 64 + g * 16), w);
+#pragma unroll
+                for (int k = 0; k < 16; ++k) v[k] += w[k];
                 if (valid) {
                     double* op = out + (size_t)(g * 16) * (size_t)NENK + nn;
                     const int jn = nm - g * 16;
@@ -737,7 +781,10 @@ __global__ void __launch_bounds__(kD2tThreads, 1) d2m_tma_kernel(const __grid_co
                         const uint64_t da = sdesc(a0 + kProdA[pr] * (uint32_t)aplane + ks * 2 * lboA, lboA, 128);
                         const uint64_t db = sdesc(bBase + kProdB[pr] * (uint32_t)bplane +
                                                       (uint32_t)(ch * (kKT / 8) + ks * 2) * lboB, lboB, 128);
-                        mma_bf16_ss(tmem + b * 64, da, db, idesc, (ch | ks | pr) ? 1u : 0u);
+                        // product 5 (hi x hi) alone in columns b*128.., the five smaller ones in b*128 + 64..
+                        const bool lead = pr == 5;
+                        const uint32_t acc = lead ? (uint32_t)(ch | ks) : (uint32_t)(ch | ks | pr);
+                        mma_bf16_ss(tmem + b * 128 + (lead ? 0u : 64u), da, db, idesc, acc ? 1u : 0u);
                     }
                 mma_commit(&adone[sa]);
                 if (ch == nchunks - 1) mma_commit(&dfull[b]);
@@ -746,7 +793,7 @@ __global__ void __launch_bounds__(kD2tThreads, 1) d2m_tma_kernel(const __grid_co
     }
     tc_before_sync();
     __syncthreads();
-    if (warp == kD2tMma) tmem_free(tmem, 128);
+    if (warp == kD2tMma) tmem_free(tmem, 256);
 }
 
 size_t d2m_tma_smem(int NIpad, int nmpad) {
@@ -805,6 +852,16 @@ bool moments_tc_enabled() {
     return on == 1;
 }
 
+// The TMA-fed D2M (LB_MOMENTS_TMA=0: the register-fed kernel).
+bool moments_tma_enabled() {
+    static int on = -1;
+    if (on < 0) {
+        const char* e = std::getenv("LB_MOMENTS_TMA");
+        on = (e && *e == '0') ? 0 : 1;
+    }
+    return on == 1;
+}
+
 // Returns LB_ERR_ARG when the shape does not fit the tensor-core kernels (caller falls back).
 int launch_m2d_tc(Handle* h, const double* x, const float* sigl, const double* a, const float* qadd, float* q) {
     const int nhalves = h->NIpad > 256 ? 2 : 1;
@@ -841,19 +898,10 @@ int launch_m2d_tc(Handle* h, const double* x, const float* sigl, const double* a
     return e == cudaSuccess ? LB_OK : cuda_fail(h, e, "m2d tensor-core kernel");
 }
 
-bool d2m_tma_enabled() {
-    static int on = -1;
-    if (on < 0) {
-        const char* e = std::getenv("LB_D2M_TMA");
-        on = (e && *e == '0') ? 0 : 1;
-    }
-    return on == 1;
-}
-
 // The TMA-fed D2M; LB_ERR_ARG when it does not apply (no tensor-map encoder, shape, alignment).
 int launch_d2m_tma(Handle* h, const float* psi, const double* xin, double alpha, double beta, double* out) {
     EncodeTiledFn enc = encode_tiled();
-    if (!enc || !d2m_tma_enabled()) return LB_ERR_ARG;
+    if (!enc || !moments_tma_enabled()) return LB_ERR_ARG;
     if (h->nmpad > 64 || h->nmpad % 16 || h->NIpad % 8 || ((uintptr_t)psi & 15) || (h->NENK * 4) % 16 ||
         h->NENK >= (1LL << 31) || h->NI < 1)
         return LB_ERR_ARG;
