@@ -22,6 +22,7 @@
 #include <cuda.h>
 #include <algorithm>
 #include <cstdlib>
+#include <cstring>
 
 namespace lb {
 
@@ -189,6 +190,15 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
         : "memory");
 }
 
+// Tensor-memory-accelerator store of a 2-D box from shared memory (a bulk group; parts of the box outside
+// the tensor are not written).
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, const void* src, int x, int y) {
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];"
+                 ::"l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(src)), "r"(x), "r"(y)
+                 : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
 // ---------------------------------------------------------------------------------------------
 // M2D: q[i][n] = sum_j Y[i][j] xt[j][n] (+ qadd[i][n]),  xt[j][n] = sigl[mat(n)][j] x[j][n] + a[j][n].
 // One CTA per SM, warp-specialised, directions [half*NH, half*NH + NH) of every tile it takes:
@@ -204,8 +214,9 @@ constexpr int kM2dEpi = 12;                          // epilogue warps (three pe
 constexpr int kM2dMma = 8 + kM2dEpi;                 // the MMA warp
 constexpr int kM2dThreads = 32 * (kM2dMma + 1);
 
-template <int KT>
-__global__ void __launch_bounds__(kM2dThreads, 1) m2d_tc_kernel(const int* __restrict__ active, const double* __restrict__ x,
+template <int KT, bool TS>
+__global__ void __launch_bounds__(kM2dThreads, 1) m2d_tc_kernel(const __grid_constant__ CUtensorMap q_map,
+                                                      const int* __restrict__ active, const double* __restrict__ x,
                                                       const float* __restrict__ sigl, const double* __restrict__ add,
                                                       const float* __restrict__ qadd, const int* __restrict__ mat,
                                                       const __nv_bfloat16* __restrict__ Y, float* __restrict__ q,
@@ -224,6 +235,8 @@ __global__ void __launch_bounds__(kM2dThreads, 1) m2d_tc_kernel(const int* __res
     uint64_t* done = full + 2;
     uint64_t* empty = full + 4;
     uint32_t* tslot = reinterpret_cast<uint32_t*>(full + 6);
+    // TS: per epilogue warp two 2 KB staging buffers [16 directions][32 nodes] for the TMA stores
+    float* sS = reinterpret_cast<float*>(sA + 2 * abuf + 1024);
     const int half = blockIdx.x % nhalves;
     stage_kmajor(Y, NIpad, nmpad, half * NH, NH, sB, bplane);
     if (tid == 0)
@@ -299,6 +312,9 @@ __global__ void __launch_bounds__(kM2dThreads, 1) m2d_tc_kernel(const int* __res
         const int ngr = NH / 16, per = (ngr + kM2dEpi / 4 - 1) / (kM2dEpi / 4);
         const int g0 = (e >> 2) * per, g1 = min(ngr, g0 + per);
         const uint32_t lane_base = tmem + ((uint32_t)((e & 3) * 32) << 16);
+        const int lane = tid & 31;
+        float* stage = sS + (size_t)e * 1024;    // TS: this warp's two [16][32] buffers
+        int sidx = 0;
         int it = 0;
         for (long long tile = t0; tile < ntiles; tile += tstep, ++it) {
             const int b = it & 1;
@@ -310,6 +326,20 @@ __global__ void __launch_bounds__(kM2dThreads, 1) m2d_tc_kernel(const int* __res
             for (int g = g0; g < g1; ++g) {
                 float v[16];
                 tmem_ld16(lane_base + (uint32_t)(b * 256 + g * 16), v);
+                if (TS) {
+                    // the warp's 32 nodes x 16 directions through shared memory and one TMA store (nodes past
+                    // NENK and directions past NI lie outside the tensor and are not written)
+                    float* st = stage + sidx * 512;
+                    if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+                    __syncwarp();
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) st[k * 32 + lane] = v[k];
+                    fence_async_smem();
+                    __syncwarp();
+                    if (lane == 0) tma_store_2d(&q_map, st, (int)(tile * kTM) + (e & 3) * 32, half * NH + g * 16);
+                    sidx ^= 1;
+                    continue;
+                }
                 if (valid) {
                     const int i0 = half * NH + g * 16;
                     const size_t o0 = (size_t)i0 * (size_t)NENK + (size_t)n;
@@ -337,6 +367,8 @@ __global__ void __launch_bounds__(kM2dThreads, 1) m2d_tc_kernel(const int* __res
             tc_before_sync();
             bar_arrive(&empty[b]);
         }
+        // the staging buffers stay in use until the stores have read them
+        if (TS && lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
     } else if ((tid & 31) == 0) {
         // ---- MMA issue ----
         const uint32_t idesc = idesc_bf16(kTM, NH);
@@ -822,10 +854,10 @@ EncodeTiledFn encode_tiled() {
     return fn;
 }
 
-size_t m2d_tc_smem(int NH, int nmpad) {
+size_t m2d_tc_smem(int NH, int nmpad, bool ts = false) {
     const size_t b = ((3 * (size_t)NH * nmpad * 2 + 1023) / 1024) * 1024;
     const size_t a = ((3 * (size_t)kTM * nmpad * 2 + 1023) / 1024) * 1024;
-    return b + 2 * a + 64;
+    return b + 2 * a + (ts ? 1024 + (size_t)kM2dEpi * 2 * 2048 : 64);
 }
 
 size_t d2m_tc_smem(int NIpad, int nmpad) {
@@ -862,36 +894,69 @@ bool moments_tma_enabled() {
     return on == 1;
 }
 
+// M2D's output written by TMA stores (LB_M2D_TMA_STORE=0: per-thread stores).
+bool moments_tma_store_enabled() {
+    static int on = -1;
+    if (on < 0) {
+        const char* e = std::getenv("LB_M2D_TMA_STORE");
+        on = (e && *e == '0') ? 0 : 1;
+    }
+    return on == 1;
+}
+
 // Returns LB_ERR_ARG when the shape does not fit the tensor-core kernels (caller falls back).
 int launch_m2d_tc(Handle* h, const double* x, const float* sigl, const double* a, const float* qadd, float* q) {
     const int nhalves = h->NIpad > 256 ? 2 : 1;
     const int NH = ((h->NIpad + nhalves - 1) / nhalves + 15) / 16 * 16;
     if (NH > 256 || h->nmpad % 16 || h->nmpad > 64 || h->NIpad % 8) return LB_ERR_ARG;
     // one CTA per SM (it holds all 512 TMEM columns: two accumulators of up to 256)
-    const size_t smem = std::max<size_t>(m2d_tc_smem(NH, h->nmpad), 116 * 1024);
-    if (smem > 227 * 1024) return LB_ERR_ARG;
     int* err = tc_error_flag();
     if (!err) return LB_ERR_OOM;
+    // TMA stores of the output when there is no added source and a tensor map can be made
+    CUtensorMap map;
+    std::memset(&map, 0, sizeof(map));
+    bool ts = !qadd && moments_tma_store_enabled() && m2d_tc_smem(NH, h->nmpad, true) <= 227 * 1024 &&
+              !((uintptr_t)q & 15) && h->NENK < (1LL << 31);
+    if (ts) {
+        EncodeTiledFn enc = encode_tiled();
+        const cuuint64_t dims[2] = {(cuuint64_t)h->NENK, (cuuint64_t)h->NI};
+        const cuuint64_t strides[1] = {(cuuint64_t)h->NENK * 4};
+        const cuuint32_t box[2] = {32u, 16u};
+        const cuuint32_t estr[2] = {1, 1};
+        ts = enc && enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, q, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    }
+    const size_t smem = std::max<size_t>(m2d_tc_smem(NH, h->nmpad, ts), 116 * 1024);
+    if (smem > 227 * 1024) return LB_ERR_ARG;
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(m2d_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        cudaFuncSetAttribute(m2d_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        cudaFuncSetAttribute(m2d_tc_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        cudaFuncSetAttribute(m2d_tc_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(m2d_tc_kernel<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(m2d_tc_kernel<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(m2d_tc_kernel<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(m2d_tc_kernel<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(m2d_tc_kernel<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(m2d_tc_kernel<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(m2d_tc_kernel<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(m2d_tc_kernel<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
         attr = true;
     }
     const long long ntiles = (h->NENK + kTM - 1) / kTM;
     long long grid = std::min<long long>(ntiles * nhalves, (long long)h->sm_count);
     grid = std::max<long long>(nhalves, grid / nhalves * nhalves);
-#define LB_M2DTC(K)                                                                                                \
-    m2d_tc_kernel<K><<<(int)grid, kM2dThreads, smem, h->stream>>>(h->d_active, x, sigl, a, qadd, h->d_mat, h->d_Ym2d, q,   \
-                                                           h->NENK, h->NI, h->NIpad, h->nm, h->nmpad, NH, nhalves, \
-                                                           ntiles, err)
-    switch (h->nmpad / 16) {
-        case 1: LB_M2DTC(1); break;
-        case 2: LB_M2DTC(2); break;
-        case 3: LB_M2DTC(3); break;
-        default: LB_M2DTC(4); break;
+#define LB_M2DTC(K, T)                                                                                              \
+    m2d_tc_kernel<K, T><<<(int)grid, kM2dThreads, smem, h->stream>>>(map, h->d_active, x, sigl, a, qadd, h->d_mat,  \
+                                                                  h->d_Ym2d, q, h->NENK, h->NI, h->NIpad, h->nm,  \
+                                                                  h->nmpad, NH, nhalves, ntiles, err)
+    switch (h->nmpad / 16 + (ts ? 4 : 0)) {
+        case 1: LB_M2DTC(1, false); break;
+        case 2: LB_M2DTC(2, false); break;
+        case 3: LB_M2DTC(3, false); break;
+        case 4: LB_M2DTC(4, false); break;
+        case 5: LB_M2DTC(1, true); break;
+        case 6: LB_M2DTC(2, true); break;
+        case 7: LB_M2DTC(3, true); break;
+        default: LB_M2DTC(4, true); break;
     }
 #undef LB_M2DTC
     cudaError_t e = cudaGetLastError();
