@@ -213,9 +213,16 @@ __device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, const void*
 constexpr int kM2dEpi = 12;                          // epilogue warps (three per TMEM lane quarter)
 constexpr int kM2dMma = 8 + kM2dEpi;                 // the MMA warp
 constexpr int kM2dThreads = 32 * (kM2dMma + 1);
+constexpr int kM2dTma = kM2dMma + 1;                 // MODE 2: the warp whose lane 0 loads the moment tiles
+constexpr int kM2dThreadsTma = 32 * (kM2dTma + 1);
 
-template <int KT, bool TS>
-__global__ void __launch_bounds__(kM2dThreads, 1) m2d_tc_kernel(const __grid_constant__ CUtensorMap q_map,
+// MODE 0: per-thread output stores; 1: TMA output stores (two staging buffers per epilogue warp); 2: TMA
+// output stores (one buffer per warp) and the moment tiles x[0..nm)[128 nodes] brought into a two-stage
+// shared-memory ring by TMA, from which the producers read (nodes past NENK arrive as zeros).
+template <int KT, int MODE>
+__global__ void __launch_bounds__(MODE == 2 ? kM2dThreadsTma : kM2dThreads, 1) m2d_tc_kernel(
+                                                      const __grid_constant__ CUtensorMap q_map,
+                                                      const __grid_constant__ CUtensorMap x_map,
                                                       const int* __restrict__ active, const double* __restrict__ x,
                                                       const float* __restrict__ sigl, const double* __restrict__ add,
                                                       const float* __restrict__ qadd, const int* __restrict__ mat,
@@ -234,17 +241,28 @@ __global__ void __launch_bounds__(kM2dThreads, 1) m2d_tc_kernel(const __grid_con
     uint64_t* full = reinterpret_cast<uint64_t*>(sA + 2 * abuf);
     uint64_t* done = full + 2;
     uint64_t* empty = full + 4;
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(full + 6);
-    // TS: per epilogue warp two 2 KB staging buffers [16 directions][32 nodes] for the TMA stores
+    uint64_t* xfull = full + 6;     // MODE 2: [2] moment stages loaded
+    uint64_t* xempty = full + 8;    // MODE 2: [2] moment stages read
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(full + 10);
+    // MODE >= 1: per epilogue warp NB 2 KB staging buffers [16 directions][32 nodes] for the TMA stores
+    constexpr int NB = MODE == 2 ? 1 : 2;
     float* sS = reinterpret_cast<float*>(sA + 2 * abuf + 1024);
+    const size_t xbuf = (size_t)kTM * nm * 8;                                    // MODE 2: one moment stage
+    unsigned char* sX = sA + 2 * abuf + 1024 + (size_t)kM2dEpi * NB * 2048;       // MODE 2: [2] stages
     const int half = blockIdx.x % nhalves;
     stage_kmajor(Y, NIpad, nmpad, half * NH, NH, sB, bplane);
-    if (tid == 0)
+    if (tid == 0) {
         for (int k = 0; k < 2; ++k) {
             bar_init(&full[k], 256);
             bar_init(&done[k], 1);
             bar_init(&empty[k], 32 * kM2dEpi);
         }
+        if (MODE == 2)
+            for (int k = 0; k < 2; ++k) {
+                bar_init(&xfull[k], 1);
+                bar_init(&xempty[k], 256);
+            }
+    }
     if (warp == kM2dMma) tmem_alloc(tslot, 512);
     fence_async_smem();
     tc_before_sync();
@@ -264,7 +282,18 @@ __global__ void __launch_bounds__(kM2dThreads, 1) m2d_tc_kernel(const __grid_con
             const long long n = tile * kTM + r;
             const bool valid = n < NENK;
             double raw[HM];
-            {
+            if (MODE == 2) {
+                // the tile's moments from the stage, then the stage back to the TMA: the proxy fence orders
+                // these generic reads before its next (async-proxy) write into the stage
+                const int xs = it & 1;
+                if (!bar_wait(&xfull[xs], (uint32_t)(it >> 1) & 1u, err)) break;
+                const double* X = reinterpret_cast<const double*>(sX + xs * xbuf) + (size_t)(side * HM) * kTM + r;
+                const int jn = nm - side * HM;
+#pragma unroll
+                for (int k = 0; k < HM; ++k) raw[k] = k < jn ? X[(size_t)k * kTM] : 0.0;
+                fence_async_smem();
+                bar_arrive(&xempty[xs]);
+            } else {
                 // one pointer stepped by a row (NENK) per moment instead of a 64-bit index per load
                 const double* sp = src + (size_t)(side * HM) * (size_t)NENK + (valid ? n : 0);
                 const int jn = valid ? nm - side * HM : 0;   // moments of this half that exist
@@ -313,7 +342,7 @@ __global__ void __launch_bounds__(kM2dThreads, 1) m2d_tc_kernel(const __grid_con
         const int g0 = (e >> 2) * per, g1 = min(ngr, g0 + per);
         const uint32_t lane_base = tmem + ((uint32_t)((e & 3) * 32) << 16);
         const int lane = tid & 31;
-        float* stage = sS + (size_t)e * 1024;    // TS: this warp's two [16][32] buffers
+        float* stage = sS + (size_t)e * NB * 512;    // MODE >= 1: this warp's NB [16][32] buffers
         int sidx = 0;
         int it = 0;
         for (long long tile = t0; tile < ntiles; tile += tstep, ++it) {
@@ -326,18 +355,21 @@ __global__ void __launch_bounds__(kM2dThreads, 1) m2d_tc_kernel(const __grid_con
             for (int g = g0; g < g1; ++g) {
                 float v[16];
                 tmem_ld16(lane_base + (uint32_t)(b * 256 + g * 16), v);
-                if (TS) {
+                if (MODE >= 1) {
                     // the warp's 32 nodes x 16 directions through shared memory and one TMA store (nodes past
                     // NENK and directions past NI lie outside the tensor and are not written)
                     float* st = stage + sidx * 512;
-                    if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+                    if (lane == 0) {
+                        if (NB == 2) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+                        else asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+                    }
                     __syncwarp();
 #pragma unroll
                     for (int k = 0; k < 16; ++k) st[k * 32 + lane] = v[k];
                     fence_async_smem();
                     __syncwarp();
                     if (lane == 0) tma_store_2d(&q_map, st, (int)(tile * kTM) + (e & 3) * 32, half * NH + g * 16);
-                    sidx ^= 1;
+                    sidx = (sidx + 1) % NB;
                     continue;
                 }
                 if (valid) {
@@ -368,8 +400,8 @@ __global__ void __launch_bounds__(kM2dThreads, 1) m2d_tc_kernel(const __grid_con
             bar_arrive(&empty[b]);
         }
         // the staging buffers stay in use until the stores have read them
-        if (TS && lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
-    } else if ((tid & 31) == 0) {
+        if (MODE >= 1 && lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    } else if (warp == kM2dMma && (tid & 31) == 0) {
         // ---- MMA issue ----
         const uint32_t idesc = idesc_bf16(kTM, NH);
         const uint32_t lboA = kTM * 16, lboB = (uint32_t)NH * 16;
@@ -389,6 +421,15 @@ __global__ void __launch_bounds__(kM2dThreads, 1) m2d_tc_kernel(const __grid_con
                     mma_bf16_ss(tmem + b * 256, da, db, idesc, (ks | pr) ? 1u : 0u);
                 }
             mma_commit(&done[b]);
+        }
+    } else if (MODE == 2 && warp == kM2dTma && (tid & 31) == 0) {
+        // ---- moment tiles by TMA, up to two ahead of the producers ----
+        int it = 0;
+        for (long long tile = t0; tile < ntiles; tile += tstep, ++it) {
+            const int xs = it & 1;
+            if (it >= 2 && !bar_wait(&xempty[xs], (uint32_t)((it >> 1) - 1) & 1u, err)) break;
+            bar_expect_tx(&xfull[xs], (uint32_t)xbuf);
+            tma_load_2d(sX + xs * xbuf, &x_map, (int)(tile * kTM), 0, &xfull[xs]);
         }
     }
     tc_before_sync();
@@ -715,6 +756,8 @@ __global__ void __launch_bounds__(kD2tThreads, 1) d2m_tma_kernel(const __grid_co
             float v[16];
 #pragma unroll
             for (int k = 0; k < 16; ++k) v[k] = F[(size_t)k * kTM];
+            // the stage is refilled by the TMA (async proxy): order these generic reads before that write
+            fence_async_smem();
             bar_arrive(&tempty[s]);
             const uint32_t ua = (uint32_t)(c / kTA);
             if (ua > 0 && !bar_wait(&adone[sa], (ua - 1) & 1u, err)) break;
@@ -854,10 +897,12 @@ EncodeTiledFn encode_tiled() {
     return fn;
 }
 
-size_t m2d_tc_smem(int NH, int nmpad, bool ts = false) {
+size_t m2d_tc_smem(int NH, int nmpad, int mode = 0, int nm = 0) {
     const size_t b = ((3 * (size_t)NH * nmpad * 2 + 1023) / 1024) * 1024;
     const size_t a = ((3 * (size_t)kTM * nmpad * 2 + 1023) / 1024) * 1024;
-    return b + 2 * a + (ts ? 1024 + (size_t)kM2dEpi * 2 * 2048 : 64);
+    if (mode == 0) return b + 2 * a + 96;
+    if (mode == 1) return b + 2 * a + 1024 + (size_t)kM2dEpi * 2 * 2048;
+    return b + 2 * a + 1024 + (size_t)kM2dEpi * 2048 + 2 * (size_t)kTM * nm * 8;
 }
 
 size_t d2m_tc_smem(int NIpad, int nmpad) {
@@ -904,6 +949,16 @@ bool moments_tma_store_enabled() {
     return on == 1;
 }
 
+// M2D's moment tiles loaded by TMA (LB_M2D_TMA_LOAD=0: per-thread loads).
+bool moments_tma_load_enabled() {
+    static int on = -1;
+    if (on < 0) {
+        const char* e = std::getenv("LB_M2D_TMA_LOAD");
+        on = (e && *e == '0') ? 0 : 1;
+    }
+    return on == 1;
+}
+
 // Returns LB_ERR_ARG when the shape does not fit the tensor-core kernels (caller falls back).
 int launch_m2d_tc(Handle* h, const double* x, const float* sigl, const double* a, const float* qadd, float* q) {
     const int nhalves = h->NIpad > 256 ? 2 : 1;
@@ -915,49 +970,66 @@ int launch_m2d_tc(Handle* h, const double* x, const float* sigl, const double* a
     // TMA stores of the output when there is no added source and a tensor map can be made
     CUtensorMap map;
     std::memset(&map, 0, sizeof(map));
-    bool ts = !qadd && moments_tma_store_enabled() && m2d_tc_smem(NH, h->nmpad, true) <= 227 * 1024 &&
+    CUtensorMap xmap;
+    std::memset(&xmap, 0, sizeof(xmap));
+    EncodeTiledFn enc = encode_tiled();
+    bool ts = enc && !qadd && moments_tma_store_enabled() && m2d_tc_smem(NH, h->nmpad, 1) <= 227 * 1024 &&
               !((uintptr_t)q & 15) && h->NENK < (1LL << 31);
     if (ts) {
-        EncodeTiledFn enc = encode_tiled();
         const cuuint64_t dims[2] = {(cuuint64_t)h->NENK, (cuuint64_t)h->NI};
         const cuuint64_t strides[1] = {(cuuint64_t)h->NENK * 4};
         const cuuint32_t box[2] = {32u, 16u};
         const cuuint32_t estr[2] = {1, 1};
-        ts = enc && enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, q, dims, strides, box, estr,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
-                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+        ts = enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, q, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
     }
-    const size_t smem = std::max<size_t>(m2d_tc_smem(NH, h->nmpad, ts), 116 * 1024);
+    // the moment tiles by TMA as well (no add operand; the two stages fit)
+    bool tl = ts && x && !a && moments_tma_load_enabled() && h->nm <= 256 &&
+              m2d_tc_smem(NH, h->nmpad, 2, h->nm) <= 227 * 1024 && !((uintptr_t)x & 15);
+    if (tl) {
+        const cuuint64_t dims[2] = {(cuuint64_t)h->NENK, (cuuint64_t)h->nm};
+        const cuuint64_t strides[1] = {(cuuint64_t)h->NENK * 8};
+        const cuuint32_t box[2] = {(cuuint32_t)kTM, (cuuint32_t)h->nm};
+        const cuuint32_t estr[2] = {1, 1};
+        tl = enc(&xmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(x), dims, strides, box, estr,
+                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    }
+    const int mode = tl ? 2 : ts ? 1 : 0;
+    const size_t smem = std::max<size_t>(m2d_tc_smem(NH, h->nmpad, mode, h->nm), 116 * 1024);
     if (smem > 227 * 1024) return LB_ERR_ARG;
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(m2d_tc_kernel<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        cudaFuncSetAttribute(m2d_tc_kernel<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        cudaFuncSetAttribute(m2d_tc_kernel<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        cudaFuncSetAttribute(m2d_tc_kernel<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        cudaFuncSetAttribute(m2d_tc_kernel<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        cudaFuncSetAttribute(m2d_tc_kernel<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        cudaFuncSetAttribute(m2d_tc_kernel<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        cudaFuncSetAttribute(m2d_tc_kernel<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+#define LB_M2DATTR(K)                                                                                      \
+    cudaFuncSetAttribute(m2d_tc_kernel<K, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);   \
+    cudaFuncSetAttribute(m2d_tc_kernel<K, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);   \
+    cudaFuncSetAttribute(m2d_tc_kernel<K, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024)
+        LB_M2DATTR(1);
+        LB_M2DATTR(2);
+        LB_M2DATTR(3);
+        LB_M2DATTR(4);
+#undef LB_M2DATTR
         attr = true;
     }
     const long long ntiles = (h->NENK + kTM - 1) / kTM;
     long long grid = std::min<long long>(ntiles * nhalves, (long long)h->sm_count);
     grid = std::max<long long>(nhalves, grid / nhalves * nhalves);
-#define LB_M2DTC(K, T)                                                                                              \
-    m2d_tc_kernel<K, T><<<(int)grid, kM2dThreads, smem, h->stream>>>(map, h->d_active, x, sigl, a, qadd, h->d_mat,  \
-                                                                  h->d_Ym2d, q, h->NENK, h->NI, h->NIpad, h->nm,  \
-                                                                  h->nmpad, NH, nhalves, ntiles, err)
-    switch (h->nmpad / 16 + (ts ? 4 : 0)) {
-        case 1: LB_M2DTC(1, false); break;
-        case 2: LB_M2DTC(2, false); break;
-        case 3: LB_M2DTC(3, false); break;
-        case 4: LB_M2DTC(4, false); break;
-        case 5: LB_M2DTC(1, true); break;
-        case 6: LB_M2DTC(2, true); break;
-        case 7: LB_M2DTC(3, true); break;
-        default: LB_M2DTC(4, true); break;
+#define LB_M2DTC(K, M)                                                                                              \
+    m2d_tc_kernel<K, M><<<(int)grid, M == 2 ? kM2dThreadsTma : kM2dThreads, smem, h->stream>>>(                      \
+        map, xmap, h->d_active, x, sigl, a, qadd, h->d_mat, h->d_Ym2d, q, h->NENK, h->NI, h->NIpad, h->nm, h->nmpad, \
+        NH, nhalves, ntiles, err)
+#define LB_M2DK(K)                           \
+    if (mode == 2) LB_M2DTC(K, 2);           \
+    else if (mode == 1) LB_M2DTC(K, 1);      \
+    else LB_M2DTC(K, 0)
+    switch (h->nmpad / 16) {
+        case 1: LB_M2DK(1); break;
+        case 2: LB_M2DK(2); break;
+        case 3: LB_M2DK(3); break;
+        default: LB_M2DK(4); break;
     }
+#undef LB_M2DK
 #undef LB_M2DTC
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? LB_OK : cuda_fail(h, e, "m2d tensor-core kernel");
