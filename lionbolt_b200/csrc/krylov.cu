@@ -259,16 +259,31 @@ __global__ void __launch_bounds__(256) group_source_kernel(double* __restrict__ 
                                                           const double* __restrict__ unc,
                                                           const double* __restrict__ ybeam, const int* __restrict__ mat,
                                                           long long NENK, int Nm, int nm, int nmpad) {
+    // One element (its four DG nodes, one material) per thread: one table entry per (g', j) for four nodes,
+    // and 32-byte loads, so a warp reads 1 KB of one moment row at a time.  Each node sums g' = 0, 1, ...
+    // in the same order as a node-per-thread loop.
     const size_t nvec = (size_t)nm * NENK;
-    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < NENK; n += (long long)gridDim.x * blockDim.x) {
-        const int m = mat[n >> 2];
-        const double u = unc ? unc[n] : 0.0;
+    const size_t tstride = (size_t)G * Nm * nmpad;   // g' -> g' + 1 in the (g', g, m, j) table
+    const long long NE = NENK >> 2;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < NE; e += (long long)gridDim.x * blockDim.x) {
+        const long long n = e << 2;
+        const int m = mat[e];
+        const double4 u = unc ? *reinterpret_cast<const double4*>(unc + n) : make_double4(0.0, 0.0, 0.0, 0.0);
         const float* t0 = tab + ((size_t)g * Nm + m) * nmpad;   // (g' = 0, g)
         for (int j = 0; j < nm; ++j) {
-            double acc = (double)t0[j] * ybeam[j] * u;
-            for (int gp = 0; gp < g; ++gp)
-                acc += (double)tab[(((size_t)gp * G + g) * Nm + m) * nmpad + j] * phi_all[(size_t)gp * nvec + (size_t)j * NENK + n];
-            src[(size_t)j * NENK + n] = acc;
+            const double y = (double)t0[j] * ybeam[j];
+            double a0 = y * u.x, a1 = y * u.y, a2 = y * u.z, a3 = y * u.w;
+            const float* tp = t0 + j;
+            const double* pp = phi_all + (size_t)j * NENK + n;
+            for (int gp = 0; gp < g; ++gp) {
+                const double t = (double)tp[(size_t)gp * tstride];
+                const double4 p = *reinterpret_cast<const double4*>(pp + (size_t)gp * nvec);
+                a0 += t * p.x;
+                a1 += t * p.y;
+                a2 += t * p.z;
+                a3 += t * p.w;
+            }
+            *reinterpret_cast<double4*>(src + (size_t)j * NENK + n) = make_double4(a0, a1, a2, a3);
         }
     }
 }
@@ -597,7 +612,7 @@ int k_group_source(Handle* h, double* src, const double* phi_all, const float* t
                    const double* ybeam, const int* mat, long long NENK, int Nm, int nm, int nmpad) {
     Timer t;
     timer_begin(h, LB_T_TALLY, t);
-    group_source_kernel<<<grid_for(h, (size_t)NENK), 256, 0, h->stream>>>(src, phi_all, tab, G, g, unc, ybeam, mat, NENK,
+    group_source_kernel<<<grid_for(h, (size_t)NENK / 4), 256, 0, h->stream>>>(src, phi_all, tab, G, g, unc, ybeam, mat, NENK,
                                                                            Nm, nm, nmpad);
     timer_end(h, t);
     return LB_OK;
