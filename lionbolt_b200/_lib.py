@@ -211,8 +211,10 @@ class Handle:
             d["min_ctas_per_sm"] = d.pop("dirs_per_cta")
             if d["ilp"] >= 2:
                 d["schedule"] += "+element prefetch"
-            if d["ilp"] >= 3:
+            if d["ilp"] == 3:
                 d["schedule"] += "+previous in registers"
+            if d["ilp"] >= 4:
+                d["schedule"] += "+two previous in registers"
         return d
 
     def mesh_types(self):

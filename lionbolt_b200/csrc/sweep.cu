@@ -138,10 +138,11 @@ __device__ __forceinline__ Geom load_geom(const float4* __restrict__ geom, int e
     return g;
 }
 
-template <bool kCG, bool kHaveQ = false, bool kPrev = false>
+template <bool kCG, bool kHaveQ = false, int kPrev = 0>
 __device__ __forceinline__ void assemble_g(const float* base, float4 dir, int item, const Geom& G, const float* s_sigt,
                                            Update& u, float4 qpre, int prev_e = -1,
-                                           float4 prev_v = make_float4(0.f, 0.f, 0.f, 0.f));
+                                           float4 prev_v = make_float4(0.f, 0.f, 0.f, 0.f), int prev2_e = -1,
+                                           float4 prev2_v = make_float4(0.f, 0.f, 0.f, 0.f));
 
 // Element from its 16-byte record (one 128-bit load) and the type table in shared memory.  The type
 // index sits in the bits that otherwise carry the material, so the element update reads it as the
@@ -184,11 +185,12 @@ __device__ __forceinline__ void assemble(const SweepArgs& a, const float* base, 
     assemble_g<kCG, kHaveQ>(base, dir, item, G, s_sigt, u, qpre);
 }
 
-// kPrev: the solution of element prev_e (the thread's previous update) is passed in registers and used
-// instead of a load when it is an upstream neighbour.
-template <bool kCG, bool kHaveQ, bool kPrev>
+// kPrev >= 1: the solution of element prev_e (the thread's previous update) is passed in registers and used
+// instead of a load when it is an upstream neighbour; kPrev = 2 also the one before it (prev2_e).
+template <bool kCG, bool kHaveQ, int kPrev>
 __device__ __forceinline__ void assemble_g(const float* base, float4 dir, int item, const Geom& G, const float* s_sigt,
-                                           Update& u, float4 qpre, int prev_e, float4 prev_v) {
+                                           Update& u, float4 qpre, int prev_e, float4 prev_v, int prev2_e,
+                                           float4 prev2_v) {
     // gmsh face -> local nodes; the vertex opposite face f is 3 - f
     constexpr int F[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
     const int e = item & 0xFFFFFF;
@@ -212,7 +214,9 @@ __device__ __forceinline__ void assemble_g(const float* base, float4 dir, int it
         if ((upm >> f) & 1) {
             const unsigned wd = nw[f];
             const int ep = (int)(wd & 0xFFFFFFu);
-            const float4 u4 = (kPrev && ep == prev_e) ? prev_v : ld4<kCG>(base + 4 * (size_t)ep);
+            const float4 u4 = (kPrev >= 1 && ep == prev_e)   ? prev_v
+                              : (kPrev >= 2 && ep == prev2_e) ? prev2_v
+                                                              : ld4<kCG>(base + 4 * (size_t)ep);
             const float u0 = pick(u4, (wd >> 24) & 3);
             const float u1 = pick(u4, (wd >> 26) & 3);
             const float u2 = pick(u4, (wd >> 28) & 3);
@@ -579,8 +583,8 @@ __global__ void __launch_bounds__(NT, MINB) sweep_cluster_kernel(SweepArgs a) {
                     int e = mem ? __ldg(&mem[f & 7u]) : e0 + (int)(f & 7u);
                     int4 gn = __ldg(&a.rec[e]);
                     float4 q = ld4<false>(base + 4 * (size_t)e);
-                    int prev_e = -1;
-                    float4 prev_v = make_float4(0.f, 0.f, 0.f, 0.f);
+                    int prev_e = -1, prev2_e = -1;
+                    float4 prev_v = make_float4(0.f, 0.f, 0.f, 0.f), prev2_v = prev_v;
 #pragma unroll 1
                     for (int k = 0; k < kClusterSize; ++k) {
                         const unsigned fn = (unsigned)(pk & 0xFFFFu);
@@ -599,9 +603,13 @@ __global__ void __launch_bounds__(NT, MINB) sweep_cluster_kernel(SweepArgs a) {
                             update_tab_pre<false>(a, base, dir, item, gn, q, s_sigt, s_gtab, s_tab);
                         } else if (PF >= 2) {
                             Update up;
-                            assemble_g<false, true, true>(base, dir, item, geom_from_rec(gn, s_gtab), s_sigt, up, q,
-                                                          prev_e, prev_v);
+                            assemble_g<false, true, (PF >= 3 ? 2 : 1)>(base, dir, item, geom_from_rec(gn, s_gtab), s_sigt,
+                                                                       up, q, prev_e, prev_v, prev2_e, prev2_v);
                             finish<false>(base, item, up);
+                            if (PF >= 3) {
+                                prev2_e = prev_e;
+                                prev2_v = prev_v;
+                            }
                             prev_e = e;
                             prev_v = make_float4(up.r[0], up.r[1], up.r[2], up.r[3]);
                         } else {
@@ -987,14 +995,15 @@ struct Config {
     int threads;
     int dpc;       // directions per CTA (kind 0); minimum CTAs per SM (kinds 2, 5)
     int ilp;       // updates in flight per thread (kind 0); kinds 5, 6: 2 = next element's record and source
-                   // prefetched, 3 = the same and the previous element's solution kept in registers
+                   // prefetched, 3 = the same and the previous element's solution kept in registers, 4 = the
+                   // same with the two previous elements' solutions
 };
 
 const Config kConfigs[] = {
     {4, 1024, 2, 1}, {4, 512, 2, 1}, {4, 512, 3, 1}, {4, 1024, 3, 1}, {4, 512, 6, 1},
     {0, 1024, 1, 1}, {0, 512, 1, 1}, {2, 1024, 1, 1}, {3, 512, 0, 1}, {1, 256, 0, 0},
     {4, 768, 2, 1}, {0, 1024, 1, 2}, {0, 1024, 1, 3}, {0, 768, 1, 3}, {5, 1024, 1, 1}, {5, 512, 2, 1}, {5, 768, 2, 1}, {5, 1024, 2, 1},
-    {6, 512, 2, 1}, {6, 768, 2, 1}, {5, 512, 2, 2}, {6, 512, 2, 2}, {5, 512, 2, 3},
+    {6, 512, 2, 1}, {6, 768, 2, 1}, {5, 512, 2, 2}, {6, 512, 2, 2}, {5, 512, 2, 3}, {5, 512, 2, 4},
 };
 constexpr int kNumConfigs = sizeof(kConfigs) / sizeof(kConfigs[0]);
 constexpr int kFinalists = 3;   // candidates timed a second time before one is kept
@@ -1191,6 +1200,7 @@ int launch_sweep(Handle* h, float* psi) {
         cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2, false, 1>);
         cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2, true, 1>);
         cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2, false, 2>);
+        cudaFuncGetAttributes(&fa, sweep_cluster_kernel<512, 2, false, 3>);
     }
     Config cfg = kConfigs[cfg_idx];
     // the autotuner skips the block schedule where it has more barrier levels than the element schedule
@@ -1235,6 +1245,7 @@ int launch_sweep(Handle* h, float* psi) {
                                   : launch_flags<512>(a, h->sm_count, h->stream);
     } else if ((cfg.kind == 5 || cfg.kind == 6) && cfg.ilp >= 2) {
         e = cfg.kind == 6   ? launch_cluster<512, 2, true, 1>(a, h->sm_count, h->stream)
+            : cfg.ilp == 4 ? launch_cluster<512, 2, false, 3>(a, h->sm_count, h->stream)
             : cfg.ilp == 3 ? launch_cluster<512, 2, false, 2>(a, h->sm_count, h->stream)
                            : launch_cluster<512, 2, false, 1>(a, h->sm_count, h->stream);
     } else if (cfg.kind == 5) {

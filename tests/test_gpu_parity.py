@@ -58,7 +58,7 @@ def test_transport_inverse_matches_oracle(case):
     assert T.timers()["sweep"][1] >= 1
 
 
-@pytest.mark.parametrize("cfg", range(23))
+@pytest.mark.parametrize("cfg", range(24))
 def test_every_sweep_schedule_matches_oracle(cfg, monkeypatch):
     """Each launch candidate of the sweep autotuner (levels, prefetching levels, element flags,
     grouped directions, dataflow, cluster levels with and without element prefetch) reproduces the oracle's T^{-1} on a two-material mesh."""
@@ -73,7 +73,7 @@ def test_every_sweep_schedule_matches_oracle(cfg, monkeypatch):
     assert rel_l2(out, ref) < TOL
 
 
-CLUSTER_CONFIGS = range(14, 23)   # launch candidates of the cluster schedule (plain, type tables, prefetch)
+CLUSTER_CONFIGS = range(14, 24)   # launch candidates of the cluster schedule (plain, type tables, prefetch)
 
 
 def _sweep_case(m, k, w, sigt, seed):
