@@ -369,6 +369,7 @@ def real_sh(Ls, dirs):
 SWEEP_KERNELS = {"cluster levels": "sweep_cluster_kernel", "cluster levels+type tables": "sweep_cluster_kernel",
                  "cluster levels+element prefetch": "sweep_cluster_kernel",
                  "cluster levels+element prefetch+previous in registers": "sweep_cluster_kernel",
+                 "cluster levels+element prefetch+two previous in registers": "sweep_cluster_kernel",
                  "cluster levels+type tables+element prefetch": "sweep_cluster_kernel",
                  "levels": "sweep_levels_kernel",
                  "levels+prefetch": "sweep_levels_pf_kernel", "element flags": "sweep_flags_kernel",
