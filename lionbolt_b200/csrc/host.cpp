@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstring>
 #include <omp.h>
+#include <functional>
 #include <unordered_map>
 
 namespace lb {
@@ -601,6 +602,66 @@ static int build_cluster_schedule(Handle* h) {
         std::vector<unsigned long long> key;
         std::vector<int4> tmp;
         std::vector<std::vector<int>> umem;
+        // Walk order inside a block: of the orders that respect the block's internal dependencies, the one
+        // with the fewest upstream neighbours three or more updates back (the kernel holds the last two
+        // solutions in registers; earlier ones are read back through L1), ties broken towards the
+        // (element level, id) order.  The best order depends only on the block's dependency pattern
+        // (which member reads which), so it is memoised by that pattern.
+        std::unordered_map<unsigned long long, unsigned> best_order;
+        auto order_block = [&](std::vector<int>& mem, int c) {
+            const int nmem = (int)mem.size();
+            if (nmem <= 3) return;   // with three or fewer updates every upstream read is within two
+            int upmask[kClusterSize] = {0, 0, 0, 0, 0, 0};
+            unsigned long long sig = (unsigned long long)nmem;
+            for (int a = 0; a < nmem; ++a) {
+                const int x = mem[a];
+                const int upm = (fld[x] >> 3) & 0xF;
+                for (int f = 0; f < 4; ++f) {
+                    if (!((upm >> f) & 1)) continue;
+                    const int y = h->nbr[(size_t)x * 4 + f];
+                    if (y < 0 || unit[y] != c) continue;
+                    for (int b = 0; b < nmem; ++b)
+                        if (mem[b] == y) upmask[a] |= 1 << b;
+                }
+                sig |= (unsigned long long)upmask[a] << (4 + 6 * a);
+            }
+            unsigned code;
+            auto hit = best_order.find(sig);
+            if (hit != best_order.end()) {
+                code = hit->second;
+            } else {
+                // depth-first over the orders that respect the dependencies, members tried in their sorted order
+                int perm[kClusterSize], pos[kClusterSize], bperm[kClusterSize];
+                int bcost = 1 << 30;
+                for (int a = 0; a < nmem; ++a) pos[a] = -1;
+                std::function<void(int, int, int)> dfs = [&](int depth, int used, int cost) {
+                    if (cost >= bcost) return;
+                    if (depth == nmem) {
+                        bcost = cost;
+                        std::copy(perm, perm + nmem, bperm);
+                        return;
+                    }
+                    for (int a = 0; a < nmem; ++a) {
+                        if ((used >> a) & 1) continue;
+                        if ((upmask[a] & used) != upmask[a]) continue;
+                        int far = 0;
+                        for (int b = 0; b < nmem; ++b)
+                            if (((upmask[a] >> b) & 1) && depth - pos[b] > 2) ++far;
+                        perm[depth] = a;
+                        pos[a] = depth;
+                        dfs(depth + 1, used | (1 << a), cost + far);
+                        pos[a] = -1;
+                    }
+                };
+                dfs(0, 0, 0);
+                code = 0;
+                for (int k = 0; k < nmem; ++k) code |= (unsigned)bperm[k] << (3 * k);
+                best_order.emplace(sig, code);
+            }
+            int tmpm[kClusterSize];
+            for (int k = 0; k < nmem; ++k) tmpm[k] = mem[(code >> (3 * k)) & 7];
+            for (int k = 0; k < nmem; ++k) mem[k] = tmpm[k];
+        };
 #pragma omp for schedule(dynamic, 1)
         for (int i = 0; i < NI; ++i) {
             if (cyclic) continue;
@@ -685,6 +746,7 @@ static int build_cluster_schedule(Handle* h) {
                     members = umem[c];
                     std::sort(members.begin(), members.end(),
                               [&](int x, int y) { return lev[x] != lev[y] ? lev[x] < lev[y] : x < y; });
+                    order_block(members, c);
                     uint32_t sl[6];
                     for (int k = 0; k < 6; ++k) sl[k] = k < (int)members.size() ? fld[members[k]] : 7u;
                     tmp[q] = make_int4(ublk[c], (int)(sl[0] | (sl[1] << 16)), (int)(sl[2] | (sl[3] << 16)),
