@@ -657,7 +657,7 @@ __global__ void __launch_bounds__(NT, MINB) sweep_cluster_kernel(SweepArgs a) {
 // single-problem level kernel (same element update, bit-identical results).
 // ---------------------------------------------------------------------------------------------
 template <int NT>
-__global__ void __launch_bounds__(NT) sweep_batch_kernel(const BatchWork* __restrict__ work, int nwork, int* counter,
+__global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 2) sweep_batch_kernel(const BatchWork* __restrict__ work, int nwork, int* counter,
                                                         const int* __restrict__ active) {
     __shared__ float s_sigt[256];
     __shared__ float4 s_gt[3 * 256];   // the item's element types (face vectors), when it has a type table
@@ -705,6 +705,47 @@ __global__ void __launch_bounds__(NT) sweep_batch_kernel(const BatchWork* __rest
                     const int* mem = W->blk_elem ? W->blk_elem + e0 : nullptr;
                     unsigned long long pk = (unsigned long long)(unsigned)r.y | ((unsigned long long)(unsigned)r.z << 32);
                     unsigned pw = (unsigned)r.w;
+                    if (ngeom > 0) {
+                        // the cluster kernel's walk: next element's record and source loaded one element
+                        // ahead, the two previous solutions kept in registers for upstream reads in the block
+                        unsigned f = (unsigned)(pk & 0xFFFFu);
+                        pk = (pk >> 16) | ((unsigned long long)(pw & 0xFFFFu) << 48);
+                        pw >>= 16;
+                        int e = mem ? __ldg(&mem[f & 7u]) : e0 + (int)(f & 7u);
+                        int4 gn = __ldg(&rec[e]);
+                        float4 q = ld4<false>(base + 4 * (size_t)e);
+                        int prev_e = -1, prev2_e = -1;
+                        float4 prev_v = make_float4(0.f, 0.f, 0.f, 0.f), prev2_v = prev_v;
+#pragma unroll 1
+                        for (int k = 0; k < kClusterSize; ++k) {
+                            const unsigned fn = (unsigned)(pk & 0xFFFFu);
+                            pk = (pk >> 16) | ((unsigned long long)(pw & 0xFFFFu) << 48);
+                            pw >>= 16;
+                            const bool more = k + 1 < kClusterSize && (fn & 7u) != 7u;
+                            const int en = !more ? e : mem ? __ldg(&mem[fn & 7u]) : e0 + (int)(fn & 7u);
+                            int4 gn_n = gn;
+                            float4 q_n = q;
+                            if (more) {
+                                gn_n = __ldg(&rec[en]);
+                                q_n = ld4<false>(base + 4 * (size_t)en);
+                            }
+                            const int item = e | (int)(((f >> 3) & 0xFu) << 24) | (int)(((f >> 7) & 0xFu) << 28);
+                            Update up;
+                            assemble_g<false, true, 2>(base, dir, item, geom_from_rec(gn, s_gt), s_sigt, up, q, prev_e,
+                                                       prev_v, prev2_e, prev2_v);
+                            finish<false>(base, item, up);
+                            prev2_e = prev_e;
+                            prev2_v = prev_v;
+                            prev_e = e;
+                            prev_v = make_float4(up.r[0], up.r[1], up.r[2], up.r[3]);
+                            if (!more) break;
+                            f = fn;
+                            e = en;
+                            gn = gn_n;
+                            q = q_n;
+                        }
+                        continue;
+                    }
 #pragma unroll 1
                     for (int k = 0; k < kClusterSize; ++k) {
                         const unsigned f = (unsigned)(pk & 0xFFFFu);
@@ -713,7 +754,7 @@ __global__ void __launch_bounds__(NT) sweep_batch_kernel(const BatchWork* __rest
                         if ((f & 7u) == 7u) break;
                         const int e = mem ? __ldg(&mem[f & 7u]) : e0 + (int)(f & 7u);
                         const int item = e | (int)(((f >> 3) & 0xFu) << 24) | (int)(((f >> 7) & 0xFu) << 28);
-                        const Geom g = ngeom > 0 ? load_geom_tab(rec, s_gt, e) : load_geom(geom, e);
+                        const Geom g = load_geom(geom, e);
                         Update up;
                         assemble_g<false>(base, dir, item, g, s_sigt, up, make_float4(0.f, 0.f, 0.f, 0.f));
                         finish<false>(base, item, up);
