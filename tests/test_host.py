@@ -257,6 +257,7 @@ def _check_cluster_schedule(m, k, w):
     assert sorted(mem[mem >= 0].tolist()) == list(range(NE))
     nbr = m.neighbors
     split = 0
+    far = 0
     for i in range(NI):
         upm = np.zeros(NE, np.int64)
         upm[sl[i]] = up[i]
@@ -290,12 +291,16 @@ def _check_cluster_schedule(m, k, w):
             other = rec_of[ne] != rec_of[e]
             assert np.all(rec_level[rec_of[ne[other]]] < rec_level[rec_of[e[other]]])
             assert np.all(slot_of[ne[~other]] < slot_of[e[~other]])
+            # walk distance of every in-block upstream read (the kernels hold the last two solutions)
+            far += int(np.count_nonzero(slot_of[e[~other]] - slot_of[ne[~other]] > 2))
+    cs["far_reads"] = far
     return cs, split
 
 
 def test_cluster_schedule_respects_every_dependency():
     """The block schedule against the reference schedule.  A box mesh: blocks of 6 consecutive tets
-    (one hex), nx + ny + nz - 2 block levels in an oblique direction and no block split.  A jittered
+    (one hex), nx + ny + nz - 2 block levels in an oblique direction, no block split, and walk orders
+    that read every in-block upstream neighbour within two updates.  A jittered
     box: blocks on dependency cycles are split into single elements in the directions that need it.
     The reference's unstructured meshes: blocks grown from face neighbours."""
     m = P.config1_small(n=(6, 6, 12)).mesh
@@ -305,6 +310,8 @@ def test_cluster_schedule_respects_every_dependency():
     cs, split = _check_cluster_schedule(m, *P.quadrature(6, 12))
     assert cs["nb"] == m.NE // 6 and cs["max_levels"] == 6 + 6 + 12 - 2 and split == 0
     assert np.array_equal(cs["members"].ravel(), np.arange(m.NE))
+    # each block's walk order leaves every in-block upstream neighbour among the two previous updates
+    assert cs["far_reads"] == 0
     jit = jittered(M.box_mesh(6, 5, 4, (0, 0, 0), (3.0, 2.5, 2.0)), 0.07)
     cs, split = _check_cluster_schedule(jit, *P.quadrature(4, 8))
     assert split > 0
