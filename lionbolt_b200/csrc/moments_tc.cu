@@ -275,12 +275,19 @@ __global__ void __launch_bounds__(MODE == 2 ? kM2dThreadsTma : kM2dThreads, 1) m
         constexpr int HM = NMP / 2;
         const int r = tid & 127, side = tid >> 7;
         const double* src = x ? x : add;
+        // the node's material (it selects the sigma row) is loaded one tile ahead, off the tile's load chain
+        int m_next = (t0 * kTM + r < NENK) ? __ldg(&mat[(t0 * kTM + r) >> 2]) : 0;
         int it = 0;
         for (long long tile = t0; tile < ntiles; tile += tstep, ++it) {
             const int b = it & 1;
             const uint32_t u = (uint32_t)(it >> 1);
             const long long n = tile * kTM + r;
             const bool valid = n < NENK;
+            const int m = valid ? m_next : 0;
+            {
+                const long long nn = (tile + tstep) * kTM + r;
+                m_next = nn < NENK ? __ldg(&mat[nn >> 2]) : 0;
+            }
             double raw[HM];
             if (MODE == 2) {
                 // the tile's moments from the stage, then the stage back to the TMA: the proxy fence orders
@@ -303,7 +310,6 @@ __global__ void __launch_bounds__(MODE == 2 ? kM2dThreadsTma : kM2dThreads, 1) m
                     sp += NENK;
                 }
             }
-            const int m = valid ? __ldg(&mat[n >> 2]) : 0;
             if (u > 0 && !bar_wait(&done[b], (u - 1) & 1u, err)) break;
             unsigned char* A = sA + b * abuf;
             // this half's sigma_l(j) row of the node's material (the table is padded to nmpad with zeros, and
@@ -984,15 +990,17 @@ int launch_m2d_tc(Handle* h, const double* x, const float* sigl, const double* a
                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
     }
-    // the moment tiles by TMA as well (no add operand; the two stages fit)
-    bool tl = ts && x && !a && moments_tma_load_enabled() && h->nm <= 256 &&
-              m2d_tc_smem(NH, h->nmpad, 2, h->nm) <= 227 * 1024 && !((uintptr_t)x & 15);
+    // the moment tiles by TMA as well, from whichever operand holds them (x, or the add operand when x is
+    // null: the group sources), not when both are given; the two stages must fit
+    const double* src = x ? x : a;
+    bool tl = ts && src && !(x && a) && moments_tma_load_enabled() && h->nm <= 256 &&
+              m2d_tc_smem(NH, h->nmpad, 2, h->nm) <= 227 * 1024 && !((uintptr_t)src & 15);
     if (tl) {
         const cuuint64_t dims[2] = {(cuuint64_t)h->NENK, (cuuint64_t)h->nm};
         const cuuint64_t strides[1] = {(cuuint64_t)h->NENK * 8};
         const cuuint32_t box[2] = {(cuuint32_t)kTM, (cuuint32_t)h->nm};
         const cuuint32_t estr[2] = {1, 1};
-        tl = enc(&xmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(x), dims, strides, box, estr,
+        tl = enc(&xmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(src), dims, strides, box, estr,
                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
     }
