@@ -50,7 +50,9 @@ __device__ __forceinline__ void block_reduce_store(double (&acc)[NV + 1], double
 
 // partial[b][j] = V_j . w (j < NV) and partial[b][NV] = w . w over this block's elements.
 // Vectors are read as double2 (n is even: n = nm * NENK with NENK a multiple of 4).
-template <int NV>
+// ZM: the vector passed is z and w = V_{NV-1} - z (the Arnoldi step's A v = v - z formed here, from the basis
+// vector this pass reads anyway, instead of in the D2M epilogue).
+template <int NV, bool ZM = false>
 __global__ void __launch_bounds__(kRedThreads) dots_t(const double* __restrict__ V, size_t ldv,
                                                      const double* __restrict__ w, size_t n2, double* partial) {
     constexpr int U = unroll_for<NV>();
@@ -69,6 +71,7 @@ __global__ void __launch_bounds__(kRedThreads) dots_t(const double* __restrict__
 #pragma unroll
             for (int j = 0; j < NV; ++j)
                 v[u][j] = in ? __ldcs(reinterpret_cast<const double2*>(V + (size_t)j * ldv) + q) : make_double2(0.0, 0.0);
+            if constexpr (ZM) wq[u] = make_double2(v[u][NV - 1].x - wq[u].x, v[u][NV - 1].y - wq[u].y);
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -83,7 +86,8 @@ __global__ void __launch_bounds__(kRedThreads) dots_t(const double* __restrict__
 // w <- w - sum_j c_j V_j; partial[b][j] = V_j . w_new (j < NV, when DOTS) and partial[b][NV] =
 // w_new . w_new.  Up to 16 vectors stay in registers between the update and the dots; beyond that
 // the dots re-read the block's elements (L1/L2 hits).
-template <int NV, bool DOTS>
+// ZM: w holds z on entry and the vector updated is V_{NV-1} - z (see dots_t).
+template <int NV, bool DOTS, bool ZM = false>
 __global__ void __launch_bounds__(kRedThreads) axpy_dots_t(double* w, const double* __restrict__ V, size_t ldv, Coefs cf,
                                                           size_t n2, double* partial) {
     double acc[NV + 1];
@@ -97,6 +101,7 @@ __global__ void __launch_bounds__(kRedThreads) axpy_dots_t(double* w, const doub
             double2 v[NV > 0 ? NV : 1];
 #pragma unroll
             for (int j = 0; j < NV; ++j) v[j] = __ldg(reinterpret_cast<const double2*>(V + (size_t)j * ldv) + q);
+            if constexpr (ZM) x = make_double2(v[NV - 1].x - x.x, v[NV - 1].y - x.y);
 #pragma unroll
             for (int j = 0; j < NV; ++j) {
                 x.x = fma(-cf.c[j], v[j].x, x.x);
@@ -108,6 +113,10 @@ __global__ void __launch_bounds__(kRedThreads) axpy_dots_t(double* w, const doub
                 for (int j = 0; j < NV; ++j) acc[j] = fma(v[j].x, x.x, fma(v[j].y, x.y, acc[j]));
             }
         } else {
+            if constexpr (ZM) {
+                const double2 vl = __ldg(reinterpret_cast<const double2*>(V + (size_t)(NV - 1) * ldv) + q);
+                x = make_double2(vl.x - x.x, vl.y - x.y);
+            }
 #pragma unroll
             for (int j = 0; j < NV; ++j) {
                 const double2 v = __ldg(reinterpret_cast<const double2*>(V + (size_t)j * ldv) + q);
@@ -434,17 +443,27 @@ static bool check_args(Handle* h, int nv, size_t n, const char* what, int* rc) {
 }
 
 // out[j] = V_j . w for j < nv; *wnorm2 = w . w (either output may be null).
-int k_dots_norm(Handle* h, const double* V, size_t ldv, int nv, const double* w, size_t n, double* out, double* wnorm2) {
+int k_dots_norm(Handle* h, const double* V, size_t ldv, int nv, const double* w, size_t n, double* out, double* wnorm2,
+                bool zm) {
     int rc = 0;
     if (!check_args(h, nv, n, "dots", &rc)) return rc;
+    if (zm && nv < 1) return fail(h, LB_ERR_ARG, "dots: the z form needs a basis vector");
     int grid = 0;
     Timer t;
     timer_begin(h, LB_T_KRYLOV, t);
     NvDispatch<kMaxDots>::run(nv, [&](auto c) {
         constexpr int NV = decltype(c)::value;
-        static const int occ = blocks_per_sm(dots_t<NV>);
-        grid = h->sm_count * occ;
-        dots_t<NV><<<grid, kRedThreads, 0, h->stream>>>(V, ldv, w, n / 2, h->d_red);
+        if (zm) {
+            if constexpr (NV >= 1) {
+                static const int occ = blocks_per_sm(dots_t<NV, true>);
+                grid = h->sm_count * occ;
+                dots_t<NV, true><<<grid, kRedThreads, 0, h->stream>>>(V, ldv, w, n / 2, h->d_red);
+            }
+        } else {
+            static const int occ = blocks_per_sm(dots_t<NV>);
+            grid = h->sm_count * occ;
+            dots_t<NV><<<grid, kRedThreads, 0, h->stream>>>(V, ldv, w, n / 2, h->d_red);
+        }
     });
     timer_end(h, t);
     double tmp[kPartStride];
@@ -456,14 +475,15 @@ int k_dots_norm(Handle* h, const double* V, size_t ldv, int nv, const double* w,
 }
 
 int k_dots(Handle* h, const double* V, size_t ldv, int nv, const double* w, size_t n, double* out) {
-    return k_dots_norm(h, V, ldv, nv, w, n, out, nullptr);
+    return k_dots_norm(h, V, ldv, nv, w, n, out, nullptr, false);
 }
 
 // w -= sum_j coef[j] V_j; then dots[j] = V_j . w (if dots != null) and *nrm2 = w . w (if non-null).
 int k_axpy_dots(Handle* h, double* w, const double* V, size_t ldv, int nv, const double* coef, size_t n, double* dots,
-                double* nrm2) {
+                double* nrm2, bool zm) {
     int rc = 0;
     if (!check_args(h, nv, n, "axpy", &rc)) return rc;
+    if (zm && (nv < 1 || !dots)) return fail(h, LB_ERR_ARG, "axpy: the z form needs a basis vector and the dots");
     Coefs cf;
     for (int j = 0; j < kMaxDots; ++j) cf.c[j] = (j < nv) ? coef[j] : 0.0;
     int grid = 0;
@@ -471,7 +491,13 @@ int k_axpy_dots(Handle* h, double* w, const double* V, size_t ldv, int nv, const
     timer_begin(h, LB_T_KRYLOV, t);
     NvDispatch<kMaxDots>::run(nv, [&](auto c) {
         constexpr int NV = decltype(c)::value;
-        if (dots) {
+        if (zm) {
+            if constexpr (NV >= 1) {
+                static const int occ = blocks_per_sm(axpy_dots_t<NV, true, true>);
+                grid = h->sm_count * occ;
+                axpy_dots_t<NV, true, true><<<grid, kRedThreads, 0, h->stream>>>(w, V, ldv, cf, n / 2, h->d_red);
+            }
+        } else if (dots) {
             static const int occ = blocks_per_sm(axpy_dots_t<NV, true>);
             grid = h->sm_count * occ;
             axpy_dots_t<NV, true><<<grid, kRedThreads, 0, h->stream>>>(w, V, ldv, cf, n / 2, h->d_red);

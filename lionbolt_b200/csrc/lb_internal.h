@@ -323,10 +323,12 @@ int moments_tc_status(Handle* h);
 // FP64 BLAS-1 on device vectors of length n
 int k_dots(Handle* h, const double* V, size_t ldv, int nv, const double* w, size_t n, double* out_host);
 // out[j] = V_j . w (j < nv, nv may be 0) and *wnorm2 = w . w in one pass (outputs may be null)
-int k_dots_norm(Handle* h, const double* V, size_t ldv, int nv, const double* w, size_t n, double* out, double* wnorm2);
+// zm: w holds z and the vector dotted is V_{nv-1} - z (k_axpy_dots: updated and written back to w).
+int k_dots_norm(Handle* h, const double* V, size_t ldv, int nv, const double* w, size_t n, double* out, double* wnorm2,
+                bool zm = false);
 // w -= sum_j coef[j] V_j, then dots[j] = V_j . w and *nrm2 = w . w in the same pass (outputs may be null)
 int k_axpy_dots(Handle* h, double* w, const double* V, size_t ldv, int nv, const double* coef, size_t n, double* dots,
-                double* nrm2);
+                double* nrm2, bool zm = false);
 // w <- (w - sum_j coef[j] V_j) * scale
 int k_axpy_scale(Handle* h, double* w, const double* V, size_t ldv, int nv, const double* coef, double scale, size_t n);
 int k_multi_axpy_norm(Handle* h, double* w, const double* V, size_t ldv, int nv, const double* coef, size_t n, double* nrm2);

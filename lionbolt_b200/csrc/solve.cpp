@@ -66,6 +66,15 @@ static int apply_A(Handle* h, const double* x, double* y, const float* sigl) {
     return rc;
 }
 
+// z = D T^{-1} M Sigma x, so that A x = x - z: the Arnoldi step forms the difference in its projection passes,
+// which read x (the last basis vector) anyway, and the D2M epilogue skips reading x.
+static int apply_Z(Handle* h, const double* x, double* z, const float* sigl) {
+    int rc = launch_m2d(h, x, sigl, nullptr, nullptr, h->d_psi);
+    if (!rc) rc = launch_sweep(h, h->d_psi);
+    if (!rc) rc = launch_d2m(h, h->d_psi, nullptr, 0.0, 1.0, z);
+    return rc;
+}
+
 // y = D T^{-1} (M (Sigma x + a) + qext)   (any of x, a, qext may be null)
 static int apply_transport_moments(Handle* h, const double* x, const float* sigl, const double* a, const float* qext,
                                    double* y) {
@@ -101,8 +110,10 @@ using DevOp = std::function<int(const double* in, double* out)>;
 using PrecOp = std::function<int(const double* in, double scale, double* out)>;
 
 // Restarted GMRES(m) / FGMRES(m) (right preconditioner `prec`), SPARSKIT semantics.
+// matvec_z (plain GMRES only): z with A x = x - z, used by the Arnoldi steps (see apply_Z); the residual at a
+// (re)start still uses matvec.
 static KrylovResult gmres_device(Handle* h, size_t n, const double* rhs, double* sol, int m, double rtol, double atol,
-                                 int maxit, const DevOp& matvec, const PrecOp* prec) {
+                                 int maxit, const DevOp& matvec, const PrecOp* prec, const DevOp* matvec_z = nullptr) {
     KrylovResult res;
     int rc = 0;
     double* V = h->d_V;
@@ -161,7 +172,8 @@ static KrylovResult gmres_device(Handle* h, size_t n, const double* rhs, double*
                 vin = Z + (size_t)(k - 1) * n;
             }
             double* vk = V + (size_t)k * n;
-            if ((rc = matvec(vin, vk))) { res.status = rc; return res; }
+            const bool zm = matvec_z && !prec;   // vk holds z; A v = V_{k-1} - z is formed by the passes
+            if ((rc = zm ? (*matvec_z)(vin, vk) : matvec(vin, vk))) { res.status = rc; return res; }
             ++nmv;
             // Gram-corrected classical Gram-Schmidt in two passes over V[0..k-1]: (1) hh = V^T vk and
             // |vk|^2;  (2) vk -= V c with G c = hh (G = V^T V, kept up to date from the dots of pass 2),
@@ -173,12 +185,12 @@ static KrylovResult gmres_device(Handle* h, size_t n, const double* rhs, double*
             // (vk holds A W_{k-1} = A V_{k-1} / sc[k-1]; the dots below are of the stored vectors)
             const double s1 = sc[k - 1];
             double nrm0 = 0.0, nrm1 = 0.0;
-            if ((rc = k_dots_norm(h, V, n, k, vk, n, hh.data(), &nrm0))) { res.status = rc; return res; }
+            if ((rc = k_dots_norm(h, V, n, k, vk, n, hh.data(), &nrm0, zm))) { res.status = rc; return res; }
             for (int i = 0; i < k; ++i) hh[i] *= sc[i] * s1;
             if (!gram_solve(G, ldg, k, hh.data(), cc.data()))
                 for (int i = 0; i < k; ++i) cc[i] = hh[i];
             for (int i = 0; i < k; ++i) cw[i] = cc[i] * sc[i] / s1;
-            if ((rc = k_axpy_dots(h, vk, V, n, k, cw.data(), n, h2.data(), &nrm1))) { res.status = rc; return res; }
+            if ((rc = k_axpy_dots(h, vk, V, n, k, cw.data(), n, h2.data(), &nrm1, zm))) { res.status = rc; return res; }
             for (int i = 0; i < k; ++i) {
                 hh[i] = cc[i];
                 h2[i] *= sc[i] * s1;
@@ -256,6 +268,7 @@ static KrylovResult moment_solve(Handle* h, const double* b, double* phi, int so
     const size_t n = (size_t)h->nm * (size_t)h->NENK;
     if (solver == LB_SOLVER_SI) return si_device(h, n, b, phi, rtol, atol, maxit, sigl);
     DevOp mv = [h, sigl](const double* in, double* out) { return apply_A(h, in, out, sigl); };
+    DevOp mz = [h, sigl](const double* in, double* out) { return apply_Z(h, in, out, sigl); };
     if (solver == LB_SOLVER_FGMRES) {
         // FGMRES(m) (iters.f:2511-2795) with the caller's per-moment diagonal as right preconditioner
         if (!h->pdiag.empty() && (int)h->pdiag.size() != h->nm) {
@@ -273,7 +286,7 @@ static KrylovResult moment_solve(Handle* h, const double* b, double* phi, int so
     if (solver == LB_SOLVER_FGMRES_ML) {
         if (!mlp_ready(h)) {
             // plain GMRES is the fallback when no trained network is loaded
-            return gmres_device(h, n, b, phi, m, rtol, atol, maxit, mv, nullptr);
+            return gmres_device(h, n, b, phi, m, rtol, atol, maxit, mv, nullptr, &mz);
         }
         // Learned path: FGMRES(m) with the network as right preconditioner, capped at `budget` operator
         // applications (plain GMRES's count on this group in calibration), else 4m, and never beyond
@@ -309,11 +322,11 @@ static KrylovResult moment_solve(Handle* h, const double* b, double* phi, int so
         // Fallback: plain GMRES(m) from the learned iterate, under the caller's limit.
         h->err.clear();
         KrylovResult k2 = gmres_device(h, n, b, phi, m, rtol, atol, maxit > 0 ? std::max(1, maxit - nmv) : 0, mv,
-                                       nullptr);
+                                       nullptr, &mz);
         k2.nmv += nmv;
         return k2;
     }
-    return gmres_device(h, n, b, phi, m, rtol, atol, maxit, mv, nullptr);
+    return gmres_device(h, n, b, phi, m, rtol, atol, maxit, mv, nullptr, &mz);
 }
 
 // ---------------------------------------------------------------------------------------------
