@@ -98,6 +98,19 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
+def rank_max(x):
+    """Largest x over all ranks (replicas finish when the slowest one does); x itself on one rank.
+    The reduction runs on the process group's device: the current GPU under NCCL, the host under gloo."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    dev = "cpu" if dist.get_backend() == "gloo" else f"cuda:{torch.cuda.current_device()}"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -307,7 +320,7 @@ def learned_comparison(args, mg, device, barrier, gmres_ms, gmres_dose, gmres_it
     for _ in range(args.steps):
         it = mg.solve("FGMRES_ML", m=args.m, rtol=args.rtol, atol=0.0)
     h.mark(3)
-    ml_ms = h.elapsed_ms(2, 3) / args.steps
+    ml_ms = rank_max(h.elapsed_ms(2, 3)) / args.steps
     _, dose = mg.results()
     mg.lp_enable(False)
     mg.lp_set_groups(None)
@@ -732,12 +745,7 @@ def run_ours(args):
     barrier()
     tm = h.timers()
     launches = int(sum(v[1] for v in tm.values()))
-    t_max = dev_ms
-    if world > 1:
-        t = torch.tensor([dev_ms], device=f"cuda:{local}", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        t_max = float(t.item())
-    ms_per_step = t_max / args.steps
+    ms_per_step = rank_max(dev_ms) / args.steps
 
     # sweep roofline
     by, up, nz = np.zeros(1), np.zeros(1), np.zeros(1, dtype=np.int64)
@@ -775,11 +783,7 @@ def run_ours(args):
         h.call("lb_mg_update_inputs", dp(h_sigt), dp(h_sigs), dp(h_dd), dp(h_unc), dp(h_dir))
         step()
         h.call("lb_mg_get_results", None, dp(h_dose))
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = rank_max(time.perf_counter() - t0)
     e2e_value = world * updates_per_step * args.steps / e2e_s
     gmres_dose = h_dose.numpy().copy()
 

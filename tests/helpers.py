@@ -100,3 +100,30 @@ def layered_beam_reference(mesh, center, width, layers):
     phi = np.where(inside, np.exp(-tau), 0.0)
     c = np.sqrt(5) * phi + 0.25 * (1 - np.sqrt(5)) * phi.sum(axis=1, keepdims=True)
     return c.ravel()
+
+
+def replica_rank(rank, world, port, out):
+    """One gloo rank of the replicas path of bench.py: the max-over-ranks reduction its timings go
+    through, and the reference arm, which runs on rank 0 only (the other ranks exit 0 without work)."""
+    import contextlib
+    import datetime
+    import io
+    import sys as _sys
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    import torch.distributed as dist
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    if root not in _sys.path:
+        _sys.path.insert(0, root)
+    import bench
+    res = {"env": bench.dist_env(), "max": bench.rank_max(10.0 + 2.5 * rank),
+           "max_neg": bench.rank_max(-1.0 - rank)}
+    if rank != 0:
+        buf = io.StringIO()
+        with contextlib.redirect_stdout(buf):
+            res["ref_rc"] = bench.run_reference(None)
+        res["ref_out"] = buf.getvalue()
+    dist.barrier()
+    dist.destroy_process_group()
+    out.put((rank, res))
