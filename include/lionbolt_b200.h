@@ -35,7 +35,8 @@ enum lb_status {
     LB_ERR_CUDA = 2,     /* CUDA runtime error                                                */
     LB_ERR_OOM = 3,      /* device allocation failed                                          */
     LB_ERR_CYCLE = 4,    /* sweep ordering stagnated: cyclic dependency (SweepOrder.f90:178)  */
-    LB_ERR_TIMEOUT = 5,  /* a bounded device-side dependency wait gave up                     */
+    LB_ERR_TIMEOUT = 5,  /* a bounded device-side wait gave up (sweep dependency or tensor-core
+                            contraction pipeline); the call's results are invalid             */
     LB_ERR_NOCONV = 6,   /* Krylov iteration limit reached (SPARSKIT.f90:159-162, ipar(1)=-1) */
     LB_ERR_NAN = 7,      /* residual norm is NaN (SPARSKIT.f90:123-124)                       */
     LB_ERR_STATE = 8,    /* operator not ready (TransportOperator.f90:87-88)                  */
@@ -126,7 +127,9 @@ int lb_transport_inv_noalloc(lb_handle* h, float* psi);
  *                  psi FP32 [NI][NENK]; moment-to-discrete with the current cross sections)
  *   lb_d2m_device: phi[j][n] = sum_i w_i Y_j(k_i) psi[i][n]                  (discrete-to-moment)
  * Both are split-BF16 tensor-core contractions (six BF16 products per term, FP32 accumulation).
- * With sigma_l = 1 they are the plain GEMMs Y phi and (wY)^T psi of ScatteringAlgebra.f90:13-55. */
+ * With sigma_l = 1 they are the plain GEMMs Y phi and (wY)^T psi of ScatteringAlgebra.f90:13-55.
+ * A contraction whose bounded pipeline wait gave up is reported by the next lb_synchronize (or the
+ * next synchronous call of the handle) as LB_ERR_TIMEOUT. */
 int lb_m2d_device(lb_handle* h, const double* phi, float* psi);
 int lb_d2m_device(lb_handle* h, const float* psi, double* phi);
 
@@ -192,6 +195,7 @@ int lb_reset_timers(lb_handle* h);
  * solution write per update, 12 B per upstream face, and the element record (16 B with the type
  * table, 64 B without) once per sweep; schedule records are not counted. */
 int lb_sweep_stats(lb_handle* h, double* bytes_per_sweep, double* updates_per_sweep, long long* upstream_faces);
+/* Waits for the handle's stream; LB_ERR_TIMEOUT if a contraction queued since the last check timed out. */
 int lb_synchronize(lb_handle* h);
 /* Sweep launch shape picked by the autotuner: cfg[0] schedule (0 levels, 1 dataflow, 2 levels with
  * next-level prefetch, 3 element flags, 4 grouped directions, 5 blocks of 6 elements swept as

@@ -681,6 +681,8 @@ int lb_batch_solve(lb_batch* b, int m, double rtol, double atol, int maxit, int*
     float ms = 0.f;
     cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]);
     b->last_ms = ms;
+    for (int p = 0; p < P; ++p)
+        if ((rc = moments_tc_status(b->probs[p]))) return prop_error(b, b->probs[p], rc, p);
     return first_err;
 }
 

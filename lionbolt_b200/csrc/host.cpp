@@ -125,7 +125,7 @@ static int dev_upload(Handle* h, T** p, const T* src, size_t count, const char* 
 
 static void free_all(Handle* h) {
     void* ptrs[] = {h->d_geom, h->d_rec, h->d_crec, h->d_crec_base, h->d_blk_elem, h->d_beam_plane, h->d_beam_xyz,
-                    h->d_beam_node, h->d_beam_nbr, h->d_cl_start, h->d_cl_base, h->d_ncl, h->d_gtab, h->d_tmat, h->d_mat, h->d_items, h->d_groups, h->d_pitems, h->d_pbase, h->d_chunks, h->d_lvl_start, h->d_lvl_base, h->d_nlev, h->d_done, h->d_status, h->d_dirs, h->d_sigt,
+                    h->d_beam_node, h->d_beam_nbr, h->d_cl_start, h->d_cl_base, h->d_ncl, h->d_gtab, h->d_tmat, h->d_mat, h->d_items, h->d_groups, h->d_pitems, h->d_pbase, h->d_chunks, h->d_lvl_start, h->d_lvl_base, h->d_nlev, h->d_done, h->d_status, h->d_tc_err, h->d_dirs, h->d_sigt,
                     h->d_psi, h->d_qext, h->d_Ym2d, h->d_Yd2m, h->d_sigl, h->d_lofj, h->d_V, h->d_Z, h->d_x,
                     h->d_b, h->d_t, h->d_red, h->d_unc, h->d_phi_all, h->d_src, h->d_dose, h->d_flux,
                     h->d_sigl_mg, h->d_yb, h->d_dd};
@@ -235,6 +235,10 @@ int lb_create(int device, lb_handle** out) {
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) { delete h; return LB_ERR_CUDA; }
     cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device);
     if (cudaMalloc(&h->d_status, sizeof(SweepStatus)) != cudaSuccess) { delete h; return LB_ERR_OOM; }
+    if (cudaMalloc(&h->d_tc_err, sizeof(int)) != cudaSuccess || cudaMemset(h->d_tc_err, 0, sizeof(int)) != cudaSuccess) {
+        delete h;
+        return LB_ERR_OOM;
+    }
     if (cudaMallocHost(&h->h_red, sizeof(double) * 65536) != cudaSuccess) { delete h; return LB_ERR_OOM; }
     if (cudaMalloc(&h->d_red, sizeof(double) * 65536) != cudaSuccess) { delete h; return LB_ERR_OOM; }
     *out = h;
@@ -1186,7 +1190,7 @@ int lb_synchronize(lb_handle* h) {
     cudaSetDevice(h->device);
     cudaError_t e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "synchronize");
-    return LB_OK;
+    return moments_tc_status(h);
 }
 
 }  // extern "C"

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 #include <cstdint>
+#include <mutex>
 #include <string>
 #include <vector>
 #include "../../include/lionbolt_b200.h"
@@ -131,6 +132,7 @@ struct Handle {
     int* d_nlev = nullptr;         // [NI]
     int* d_done = nullptr;         // [total_levels]
     SweepStatus* d_status = nullptr;
+    int* d_tc_err = nullptr;      // set to LB_ERR_TIMEOUT by a contraction kernel whose pipeline wait gave up
     float4* d_dirs = nullptr;      // [NI] (kx, ky, kz, w)
     float* d_sigt = nullptr;       // [Nm]
     float* d_psi = nullptr;        // [NI][NENK] FP32 angular work vector
@@ -220,6 +222,27 @@ bool mlp_ready(Handle* h);
 int mlp_apply_precond(Handle* h, const double* v, double* z, double vscale);
 // Appends `count` training samples drawn from the residual r and error err (device moment vectors).
 int mlp_sample(Handle* h, const double* r, const double* err, long long count, unsigned long long seed);
+
+// A value computed once per device at one call site (kernel attributes and occupancies are per
+// device, and one process may drive several GPUs from several threads); the caller keeps it as a
+// function-local static.
+struct PerDevice {
+    std::mutex m;
+    unsigned long long done = 0;
+    int value[64] = {};
+    template <class F>
+    int get(F&& f) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        dev &= 63;
+        std::lock_guard<std::mutex> g(m);
+        if (!(done >> dev & 1ull)) {
+            value[dev] = f();
+            done |= 1ull << dev;
+        }
+        return value[dev];
+    }
+};
 
 // Allow a kernel the largest dynamic shared memory the device permits next to its static
 // shared memory (227 KB per CTA on sm_100 in total).  Clears the error state it may leave.

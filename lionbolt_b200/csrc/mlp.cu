@@ -653,12 +653,12 @@ static int ensure_grad_bufs(Handle* h, MlpState* s, int parts, int hist) {
         if (e != cudaSuccess) return cuda_fail(h, e, "loss history");
         s->hist_cap = hist;
     }
-    static bool attr = false;
-    if (!attr) {
+    static PerDevice attr;
+    attr.get([&] {
         cudaFuncSetAttribute(lp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGradSmem);
         cudaGetLastError();
-        attr = true;
-    }
+        return 1;
+    });
     return LB_OK;
 }
 

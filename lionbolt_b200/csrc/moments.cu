@@ -415,11 +415,11 @@ __global__ void __launch_bounds__(NW * 32, 1) d2m_stream_kernel(const int* __res
 template <int MT>
 int run_d2m(Handle* h, const float* psi, const double* xin, double alpha, double beta, double* out, long long ntiles,
             int grid, size_t smem) {
-    static bool attr = false;
-    if (!attr) {
+    static PerDevice attr;
+    attr.get([&] {
         allow_max_dynamic_smem(d2m_kernel<MT>);
-        attr = true;
-    }
+        return 1;
+    });
     d2m_kernel<MT><<<grid, kThreads, smem, h->stream>>>(h->d_active, psi, h->d_Yd2m, xin, alpha, beta, out, h->NENK, h->NI,
                                                         h->NIpad, h->nm, h->nmpad, ntiles);
     return LB_OK;
@@ -429,12 +429,15 @@ int run_d2m(Handle* h, const float* psi, const double* xin, double alpha, double
 template <int KT, int NW>
 cudaError_t run_m2d_stream(Handle* h, const double* x, const float* sigl, const double* a, const float* qadd, float* q,
                            size_t smem) {
-    static int per_sm = -1;
-    if (per_sm < 0) {
+    static PerDevice attr;
+    attr.get([&] {
         allow_max_dynamic_smem(m2d_stream_kernel<KT, NW>);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, m2d_stream_kernel<KT, NW>, NW * 32, smem);
-        if (per_sm < 1) per_sm = 1;
-    }
+        return 1;
+    });
+    // the occupancy depends on this handle's tile size (smem)
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, m2d_stream_kernel<KT, NW>, NW * 32, smem);
+    if (per_sm < 1) per_sm = 1;
     const long long ntiles = (h->NENK + NW * 8 - 1) / (NW * 8);
     long long grid = std::min<long long>(ntiles, (long long)h->sm_count * per_sm);
     m2d_stream_kernel<KT, NW><<<(int)grid, NW * 32, smem, h->stream>>>(h->d_active, x, sigl, a, qadd, h->d_mat, h->d_Ym2d, q,
@@ -445,12 +448,15 @@ cudaError_t run_m2d_stream(Handle* h, const double* x, const float* sigl, const 
 template <int MT, int NW>
 cudaError_t run_d2m_stream(Handle* h, const float* psi, const double* xin, double alpha, double beta, double* out,
                            size_t smem) {
-    static int per_sm = -1;
-    if (per_sm < 0) {
+    static PerDevice attr;
+    attr.get([&] {
         allow_max_dynamic_smem(d2m_stream_kernel<MT, NW>);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, d2m_stream_kernel<MT, NW>, NW * 32, smem);
-        if (per_sm < 1) per_sm = 1;
-    }
+        return 1;
+    });
+    // the occupancy depends on this handle's tile size (smem)
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, d2m_stream_kernel<MT, NW>, NW * 32, smem);
+    if (per_sm < 1) per_sm = 1;
     const long long ntiles = (h->NENK + NW * 8 - 1) / (NW * 8);
     long long grid = std::min<long long>(ntiles, (long long)h->sm_count * per_sm);
     d2m_stream_kernel<MT, NW><<<(int)grid, NW * 32, smem, h->stream>>>(h->d_active, psi, h->d_Yd2m, xin, alpha, beta, out,
@@ -504,11 +510,11 @@ int launch_m2d(Handle* h, const double* x, const float* sigl, const double* a, c
         }
 #undef LB_M2D
     } else {
-        static bool attr = false;
-        if (!attr) {
+        static PerDevice attr;
+        attr.get([&] {
             allow_max_dynamic_smem(m2d_kernel);
-            attr = true;
-        }
+            return 1;
+        });
         const size_t smem = (size_t)3 * kTileN * smem_stride_words(h->nmpad) * 4;
         if (smem > 227 * 1024) { timer_end(h, t); return fail(h, LB_ERR_ARG, "m2d: too many moments for the shared-memory tile"); }
         int per_sm = 0;

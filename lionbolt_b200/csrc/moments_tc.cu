@@ -110,18 +110,6 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
     for (int k = 0; k < 8; ++k) v[k] = __uint_as_float(r[k]);
 }
 
-__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float (&v)[16]) {
-    asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};"
-        ::"r"(taddr), "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
-          "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])), "r"(__float_as_uint(v[6])),
-          "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])), "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])),
-          "r"(__float_as_uint(v[11])), "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])),
-          "r"(__float_as_uint(v[14])), "r"(__float_as_uint(v[15]))
-        : "memory");
-    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-}
-
 // The warp calling this allocates ncols TMEM columns (power of two >= 32) and publishes the base.
 __device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)), "r"(ncols)
@@ -918,12 +906,6 @@ size_t d2m_tc_smem(int NIpad, int nmpad) {
     return b + kStages * a + 128;
 }
 
-int* tc_error_flag() {
-    static int* flag = nullptr;
-    if (!flag && cudaMalloc(&flag, sizeof(int)) == cudaSuccess) cudaMemset(flag, 0, sizeof(int));
-    return flag;
-}
-
 }  // namespace
 
 bool moments_tc_enabled() {
@@ -971,8 +953,8 @@ int launch_m2d_tc(Handle* h, const double* x, const float* sigl, const double* a
     const int NH = ((h->NIpad + nhalves - 1) / nhalves + 15) / 16 * 16;
     if (NH > 256 || h->nmpad % 16 || h->nmpad > 64 || h->NIpad % 8) return LB_ERR_ARG;
     // one CTA per SM (it holds all 512 TMEM columns: two accumulators of up to 256)
-    int* err = tc_error_flag();
-    if (!err) return LB_ERR_OOM;
+    int* err = h->d_tc_err;
+    if (!err) return LB_ERR_STATE;
     // TMA stores of the output when there is no added source and a tensor map can be made
     CUtensorMap map;
     std::memset(&map, 0, sizeof(map));
@@ -1007,8 +989,8 @@ int launch_m2d_tc(Handle* h, const double* x, const float* sigl, const double* a
     const int mode = tl ? 2 : ts ? 1 : 0;
     const size_t smem = std::max<size_t>(m2d_tc_smem(NH, h->nmpad, mode, h->nm), 116 * 1024);
     if (smem > 227 * 1024) return LB_ERR_ARG;
-    static bool attr = false;
-    if (!attr) {
+    static PerDevice attr;
+    attr.get([&] {
 #define LB_M2DATTR(K)                                                                                      \
     cudaFuncSetAttribute(m2d_tc_kernel<K, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);   \
     cudaFuncSetAttribute(m2d_tc_kernel<K, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);   \
@@ -1018,8 +1000,8 @@ int launch_m2d_tc(Handle* h, const double* x, const float* sigl, const double* a
         LB_M2DATTR(3);
         LB_M2DATTR(4);
 #undef LB_M2DATTR
-        attr = true;
-    }
+        return 1;
+    });
     const long long ntiles = (h->NENK + kTM - 1) / kTM;
     long long grid = std::min<long long>(ntiles * nhalves, (long long)h->sm_count);
     grid = std::max<long long>(nhalves, grid / nhalves * nhalves);
@@ -1052,8 +1034,8 @@ int launch_d2m_tma(Handle* h, const float* psi, const double* xin, double alpha,
         return LB_ERR_ARG;
     const size_t smem = std::max<size_t>(d2m_tma_smem(h->NIpad, h->nmpad), 116 * 1024);
     if (smem > 227 * 1024) return LB_ERR_ARG;
-    int* err = tc_error_flag();
-    if (!err) return LB_ERR_OOM;
+    int* err = h->d_tc_err;
+    if (!err) return LB_ERR_STATE;
     // tensor map over psi[NI][NENK] (FP32): box 128 nodes x kKT directions, zero fill outside
     CUtensorMap map;
     const cuuint64_t dims[2] = {(cuuint64_t)h->NENK, (cuuint64_t)h->NI};
@@ -1064,14 +1046,14 @@ int launch_d2m_tma(Handle* h, const float* psi, const double* xin, double alpha,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return LB_ERR_ARG;
-    static bool attr = false;
-    if (!attr) {
+    static PerDevice attr;
+    attr.get([&] {
         cudaFuncSetAttribute(d2m_tma_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
         cudaFuncSetAttribute(d2m_tma_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
         cudaFuncSetAttribute(d2m_tma_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
         cudaFuncSetAttribute(d2m_tma_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        attr = true;
-    }
+        return 1;
+    });
     const long long ntiles = (h->NENK + kTM - 1) / kTM;
     const long long grid = std::min<long long>(ntiles, (long long)h->sm_count);
 #define LB_D2MTMA(K)                                                                                                \
@@ -1097,16 +1079,16 @@ int launch_d2m_tc(Handle* h, const float* psi, const double* xin, double alpha, 
     // one CTA per SM (two accumulators of up to 64 columns in a 128-column allocation)
     const size_t smem = std::max<size_t>(d2m_tc_smem(h->NIpad, h->nmpad), 116 * 1024);
     if (smem > 227 * 1024) return LB_ERR_ARG;
-    int* err = tc_error_flag();
-    if (!err) return LB_ERR_OOM;
-    static bool attr = false;
-    if (!attr) {
+    int* err = h->d_tc_err;
+    if (!err) return LB_ERR_STATE;
+    static PerDevice attr;
+    attr.get([&] {
         cudaFuncSetAttribute(d2m_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
         cudaFuncSetAttribute(d2m_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
         cudaFuncSetAttribute(d2m_tc_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
         cudaFuncSetAttribute(d2m_tc_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        attr = true;
-    }
+        return 1;
+    });
     const long long ntiles = (h->NENK + kTM - 1) / kTM;
     const long long grid = std::min<long long>(ntiles, (long long)h->sm_count);
 #define LB_D2MTC(K)                                                                                         \
@@ -1123,18 +1105,19 @@ int launch_d2m_tc(Handle* h, const float* psi, const double* xin, double alpha, 
     return e == cudaSuccess ? LB_OK : cuda_fail(h, e, "d2m tensor-core kernel");
 }
 
-// Reads and clears the tensor-core kernels' timeout flag (synchronises the handle's stream).
+// Reads and clears the handle's contraction timeout flag (synchronises the handle's stream): LB_ERR_TIMEOUT
+// when a tensor-core contraction gave up on a pipeline wait since the last check.
 int moments_tc_status(Handle* h) {
-    int* err = tc_error_flag();
-    if (!err) return LB_OK;
+    if (!h->d_tc_err) return LB_OK;
     int v = 0;
-    cudaStreamSynchronize(h->stream);
-    cudaMemcpy(&v, err, sizeof(int), cudaMemcpyDeviceToHost);
-    if (v) {
-        cudaMemset(err, 0, sizeof(int));
-        return fail(h, LB_ERR_TIMEOUT, "tensor-core moment kernel: MMA completion wait timed out");
-    }
-    return LB_OK;
+    cudaError_t e = cudaMemcpyAsync(&v, h->d_tc_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "contraction status");
+    if (!v) return LB_OK;
+    e = cudaMemsetAsync(h->d_tc_err, 0, sizeof(int), h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "contraction status");
+    return fail(h, LB_ERR_TIMEOUT, "tensor-core moment kernel: pipeline wait timed out (results invalid)");
 }
 
 }  // namespace lb

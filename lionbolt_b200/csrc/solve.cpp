@@ -454,7 +454,8 @@ int lb_scatter_apply(lb_handle* h, double* x) {
     if ((rc = upload_angular(h, x, h->d_psi))) return rc;
     if ((rc = launch_d2m(h, h->d_psi, nullptr, 0.0, 1.0, h->d_t))) return rc;
     if ((rc = launch_m2d(h, h->d_t, h->d_sigl, nullptr, nullptr, h->d_psi))) return rc;
-    return download_angular(h, h->d_psi, x);
+    if ((rc = download_angular(h, h->d_psi, x))) return rc;
+    return moments_tc_status(h);
 }
 
 int lb_boltzmann_matvec(lb_handle* h, double* x) {
@@ -469,6 +470,7 @@ int lb_boltzmann_matvec(lb_handle* h, double* x) {
     if ((rc = launch_sweep(h, h->d_psi))) return rc;
     std::vector<double> y(h->psi_elems);
     if ((rc = download_angular(h, h->d_psi, y.data()))) return rc;
+    if ((rc = moments_tc_status(h))) return rc;
 #pragma omp parallel for schedule(static)
     for (size_t q = 0; q < y.size(); ++q) x[q] = x[q] - y[q];
     return LB_OK;
@@ -500,7 +502,8 @@ int lb_boltzmann_solve(lb_handle* h, double* s, int solver, int m, double rtol, 
     // psi = T^{-1} (M Sigma phi + q)
     if ((rc = launch_m2d(h, h->d_x, h->d_sigl, nullptr, h->d_qext, h->d_psi))) return rc;
     if ((rc = launch_sweep(h, h->d_psi))) return rc;
-    return download_angular(h, h->d_psi, s);
+    if ((rc = download_angular(h, h->d_psi, s))) return rc;
+    return moments_tc_status(h);
 }
 
 int lb_set_right_precond_diag(lb_handle* h, int nm, const double* d) {
@@ -602,6 +605,7 @@ int lb_mg_solve(lb_handle* h, int solver, int m, double rtol, double atol, int m
     }
     cudaError_t e = cudaStreamSynchronize(h->stream);
     if (!rc && e != cudaSuccess) rc = cuda_fail(h, e, "multigroup solve");
+    if (!rc) rc = moments_tc_status(h);
     return rc;
 }
 
@@ -642,7 +646,7 @@ int lb_lp_calibrate(lb_handle* h, int m, double rtol, int* plain_iters, int* lea
         if (learned_iters) learned_iters[g] = kl.nmv;
     }
     cudaError_t e = cudaStreamSynchronize(h->stream);
-    return e == cudaSuccess ? LB_OK : cuda_fail(h, e, "lb_lp_calibrate");
+    return e == cudaSuccess ? moments_tc_status(h) : cuda_fail(h, e, "lb_lp_calibrate");
 }
 
 int lb_mg_get_results(lb_handle* h, double* flux, double* dose) {
@@ -694,6 +698,7 @@ int lb_lp_generate(lb_handle* h, int samples_per_group, int iters, unsigned long
     }
     cudaError_t e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "lb_lp_generate");
+    if ((rc = moments_tc_status(h))) return rc;
     if (total) lb_lp_num_samples(h, total);
     return LB_OK;
 }

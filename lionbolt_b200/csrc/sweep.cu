@@ -1063,11 +1063,12 @@ cudaError_t launch_levels(const SweepArgs& a, int threads, int sm_count, cudaStr
 
 template <int G, int NT>
 cudaError_t launch_group(const SweepArgs& a, const int* groups, int ngroups, int sm_count, cudaStream_t s) {
-    static int per_sm = -1;
-    if (per_sm < 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_group_kernel<G, NT>, NT, 0);
-        if (per_sm < 1) per_sm = 1;
-    }
+    static PerDevice per_sm_cache;
+    const int per_sm = per_sm_cache.get([&] {
+        int n = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_group_kernel<G, NT>, NT, 0);
+        return n < 1 ? 1 : n;
+    });
     int grid = std::min(ngroups, sm_count * per_sm);
     sweep_group_kernel<G, NT><<<grid, NT, 0, s>>>(a, groups, ngroups);
     return cudaGetLastError();
@@ -1105,14 +1106,14 @@ template <int NT>
 cudaError_t launch_flags(const SweepArgs& a, int sm_count, cudaStream_t s) {
     const size_t smem = sizeof(uint32_t) * (size_t)((a.NE + 31) / 32);
     if (smem > 200 * 1024) return cudaErrorInvalidConfiguration;
-    static int per_sm = -1;
-    static size_t last_smem = 0;
-    if (per_sm < 0 || last_smem != smem) {
+    static PerDevice attr;
+    attr.get([&] {
         allow_max_dynamic_smem(sweep_flags_kernel<NT>);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_flags_kernel<NT>, NT, smem);
-        if (per_sm < 1) per_sm = 1;
-        last_smem = smem;
-    }
+        return 1;
+    });
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_flags_kernel<NT>, NT, smem);
+    if (per_sm < 1) per_sm = 1;
     int grid = std::min(a.NI, sm_count * per_sm);
     sweep_flags_kernel<NT><<<grid, NT, smem, s>>>(a);
     return cudaGetLastError();
@@ -1147,18 +1148,20 @@ int launch_sweep_batch(cudaStream_t st, const BatchWork* work, int nwork, int* c
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
     if (e != cudaSuccess) return LB_ERR_CUDA;
     if (threads == 512) {
-        static int per_sm = -1;
-        if (per_sm < 0) {
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_batch_kernel<512>, 512, 0);
-            if (per_sm < 1) per_sm = 1;
-        }
+        static PerDevice per_sm_cache;
+        const int per_sm = per_sm_cache.get([&] {
+            int n = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_batch_kernel<512>, 512, 0);
+            return n < 1 ? 1 : n;
+        });
         sweep_batch_kernel<512><<<std::min(nwork, sm_count * per_sm), 512, 0, st>>>(work, nwork, counter, active);
     } else {
-        static int per_sm = -1;
-        if (per_sm < 0) {
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_batch_kernel<1024>, 1024, 0);
-            if (per_sm < 1) per_sm = 1;
-        }
+        static PerDevice per_sm_cache;
+        const int per_sm = per_sm_cache.get([&] {
+            int n = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_batch_kernel<1024>, 1024, 0);
+            return n < 1 ? 1 : n;
+        });
         sweep_batch_kernel<1024><<<std::min(nwork, sm_count * per_sm), 1024, 0, st>>>(work, nwork, counter, active);
     }
     return cudaGetLastError() == cudaSuccess ? LB_OK : LB_ERR_CUDA;
@@ -1301,11 +1304,12 @@ int launch_sweep(Handle* h, float* psi) {
         e = (cfg.dpc == 2) ? launch_levels_pf<2>(a, cfg.threads, h->sm_count, h->stream)
                            : launch_levels_pf<1>(a, cfg.threads, h->sm_count, h->stream);
     } else if (cfg.kind == 1) {
-        static int df_per_sm = -1;
-        if (df_per_sm < 0) {
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&df_per_sm, sweep_dataflow_kernel, 256, 0);
-            if (df_per_sm < 1) df_per_sm = 1;
-        }
+        static PerDevice df_per_sm_cache;
+        const int df_per_sm = df_per_sm_cache.get([&] {
+            int n = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_dataflow_kernel, 256, 0);
+            return n < 1 ? 1 : n;
+        });
         sweep_dataflow_kernel<<<h->sm_count * df_per_sm, 256, 0, h->stream>>>(a);
         e = cudaGetLastError();
     } else if (cfg.dpc == 1 && cfg.ilp == 1) e = launch_levels<1, 1>(a, cfg.threads, h->sm_count, h->stream);
