@@ -40,6 +40,9 @@ SWEEP_CASES = {
                          np.array([1.3]), np.zeros((1, 1))),
     "thin_air": lambda: (M.box_mesh(4, 4, 4, (0, 0, 0), (2, 2, 2)), P.quadrature(4, 8), np.array([1e-6]),
                          np.zeros((1, 1))),
+    # a void material (sigma_t = 0) next to an absorber: pure streaming through half of the elements
+    "void_region": lambda: (P.config1_small(n=(6, 6, 12)).mesh, P.quadrature(6, 12), np.array([0.0, 0.9]),
+                            np.zeros((2, 1))),
 }
 
 
@@ -153,6 +156,36 @@ def test_scattering_matches_oracle(nmat):
     out = x.copy()
     ScatteringOp().Build(m, ang, xs).MatVec(out)
     assert rel_l2(out, ref) < TOL
+
+
+@pytest.mark.parametrize("nmat", [1, 2])
+def test_device_contractions_compose_to_scattering(nmat):
+    """lb_d2m_device then lb_m2d_device on caller-owned device arrays (asynchronous on the handle's
+    stream; lb_synchronize reports their status) give K psi of the oracle."""
+    torch = pytest.importorskip("torch")
+    import ctypes
+    if nmat == 1:
+        m = M.box_mesh(3, 3, 3, (0, 0, 0), (1, 1, 1))
+        sigt, sigs = np.array([0.5]), np.array([[0.45 * 0.8 ** l for l in range(6)]])
+    else:
+        m = P.config1_small(n=(3, 3, 6)).mesh
+        sigt = np.array([0.3, 0.81])
+        sigs = np.array([[0.27 * 0.7 ** l for l in range(6)], [0.6 * 0.9 ** l for l in range(6)]])
+    k, w = P.quadrature(6, 12)
+    o, ang, xs = _pair(m, k, w, sigt, sigs, L=5)
+    x = np.random.default_rng(15).normal(size=m.NENK * k.shape[0]).astype(np.float32).astype(np.float64)
+    ref = o.scatter_apply(x)
+    K = ScatteringOp().Build(m, ang, xs)
+    lib, h = K._h.lib, K._h.h
+    psi = torch.from_numpy(x.astype(np.float32)).to("cuda:0")
+    phi = torch.zeros(36 * m.NENK, dtype=torch.float64, device="cuda:0")
+    out = torch.zeros_like(psi)
+    torch.cuda.synchronize()
+    assert lib.lb_d2m_device(h, ctypes.c_void_p(psi.data_ptr()), ctypes.c_void_p(phi.data_ptr())) == 0
+    assert lib.lb_m2d_device(h, ctypes.c_void_p(phi.data_ptr()), ctypes.c_void_p(out.data_ptr())) == 0
+    assert lib.lb_synchronize(h) == 0
+    assert rel_l2(out.cpu().numpy(), ref) < TOL
+    assert K.timers()["m2d"][1] >= 1 and K.timers()["d2m"][1] >= 1
 
 
 def test_scatter_mms_known_answer_on_gpu():
