@@ -666,7 +666,11 @@ constexpr int kD2tEpi = kD2tConv + 8 * kD2tSets;   // first epilogue warp
 constexpr int kD2tMma = kD2tEpi + 4;               // the MMA warp
 constexpr int kD2tThreads = 32 * (kD2tMma + 1);
 
-template <int KT>
+// STACK: the three B planes are interleaved along N ([hi; mid; lo] rows per K column), so that one MMA of
+// N = 3 nmpad takes hi x {hi, mid, lo}, one of N = 2 nmpad mid x {hi, mid} and one of N = nmpad lo x hi: each A
+// plane is read from shared memory once per K step instead of once per product.  The accumulator of a tile
+// holds three column groups (the hi x hi product, the 2^-8 products, the 2^-16 products), summed by the epilogue.
+template <int KT, bool STACK>
 __global__ void __launch_bounds__(kD2tThreads, 1) d2m_tma_kernel(const __grid_constant__ CUtensorMap psi_map,
                                                       const int* __restrict__ active,
                                                       const __nv_bfloat16* __restrict__ Dw, const double* xin,
@@ -699,9 +703,14 @@ __global__ void __launch_bounds__(kD2tThreads, 1) d2m_tma_kernel(const __grid_co
             const int r = rem / cc, c = rem % cc;
             uint4 v = make_uint4(0u, 0u, 0u, 0u);
             if (c * 8 < NIpad) v = __ldg(reinterpret_cast<const uint4*>(Dw + ((size_t)p * nmpad + r) * NIpad) + c);
-            *reinterpret_cast<uint4*>(sB + p * bplane + (size_t)c * nmpad * 16 + (size_t)r * 16) = v;
+            if (STACK)
+                *reinterpret_cast<uint4*>(sB + (size_t)c * 3 * nmpad * 16 + (size_t)(p * nmpad + r) * 16) = v;
+            else
+                *reinterpret_cast<uint4*>(sB + p * bplane + (size_t)c * nmpad * 16 + (size_t)r * 16) = v;
         }
     }
+    // TMEM columns per tile buffer: two groups of up to 64 (leading, corrections), or three of nmpad (STACK)
+    constexpr uint32_t kBufCols = STACK ? 256u : 128u;
     if (tid == 0) {
         for (int k = 0; k < kT32; ++k) {
             bar_init(&tfull[k], 1);
@@ -716,7 +725,7 @@ __global__ void __launch_bounds__(kD2tThreads, 1) d2m_tma_kernel(const __grid_co
             bar_init(&dempty[k], 128);
         }
     }
-    if (warp == kD2tMma) tmem_alloc(tslot, 256);   // per tile buffer: leading-product and correction accumulators
+    if (warp == kD2tMma) tmem_alloc(tslot, 2 * kBufCols);   // two tile buffers
     fence_async_smem();
     tc_before_sync();
     __syncthreads();
@@ -797,10 +806,18 @@ __global__ void __launch_bounds__(kD2tThreads, 1) d2m_tma_kernel(const __grid_co
             tc_after_sync();
 #pragma unroll
             for (int g = 0; g < KT; ++g) {
-                // the leading product's accumulator plus the correction products' accumulator (IEEE FP32)
+                // the leading product's accumulator plus the correction products' accumulator(s) (IEEE FP32)
                 float v[16], w[16];
-                tmem_ld16(lane_base + (uint32_t)(b * 128 + g * 16), v);
-                tmem_ld16(lane_base + (uint32_t)(b * 128 + 64 + g * 16), w);
+                if (STACK) {
+                    tmem_ld16(lane_base + (uint32_t)(b * kBufCols + nmpad + g * 16), w);
+                    tmem_ld16(lane_base + (uint32_t)(b * kBufCols + 2 * nmpad + g * 16), v);
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) w[k] += v[k];
+                    tmem_ld16(lane_base + (uint32_t)(b * kBufCols + g * 16), v);
+                } else {
+                    tmem_ld16(lane_base + (uint32_t)(b * kBufCols + g * 16), v);
+                    tmem_ld16(lane_base + (uint32_t)(b * kBufCols + 64 + g * 16), w);
+                }
 #pragma unroll
                 for (int k = 0; k < 16; ++k) v[k] += w[k];
                 if (valid) {
@@ -828,7 +845,7 @@ __global__ void __launch_bounds__(kD2tThreads, 1) d2m_tma_kernel(const __grid_co
     } else if ((tid & 31) == 0) {
         // ---- MMA issue ----
         const uint32_t idesc = idesc_bf16(kTM, nmpad);
-        const uint32_t lboA = kTM * 16, lboB = (uint32_t)nmpad * 16;
+        const uint32_t lboA = kTM * 16, lboB = (uint32_t)nmpad * 16 * (STACK ? 3u : 1u);
         const uint32_t aBase = smem_u32(sA), bBase = smem_u32(sB);
         long long c = 0;
         int it = 0;
@@ -845,16 +862,29 @@ __global__ void __launch_bounds__(kD2tThreads, 1) d2m_tma_kernel(const __grid_co
                 }
                 tc_after_sync();
                 const uint32_t a0 = aBase + sa * (uint32_t)abuf;
-                for (int ks = 0; ks < kKT / 16; ++ks)
-                    for (int pr = 0; pr < 6; ++pr) {
-                        const uint64_t da = sdesc(a0 + kProdA[pr] * (uint32_t)aplane + ks * 2 * lboA, lboA, 128);
-                        const uint64_t db = sdesc(bBase + kProdB[pr] * (uint32_t)bplane +
-                                                      (uint32_t)(ch * (kKT / 8) + ks * 2) * lboB, lboB, 128);
-                        // product 5 (hi x hi) alone in columns b*128.., the five smaller ones in b*128 + 64..
-                        const bool lead = pr == 5;
-                        const uint32_t acc = lead ? (uint32_t)(ch | ks) : (uint32_t)(ch | ks | pr);
-                        mma_bf16_ss(tmem + b * 128 + (lead ? 0u : 64u), da, db, idesc, acc ? 1u : 0u);
+                if (STACK) {
+                    // hi x [hi; mid; lo] -> groups 0, 1, 2; mid x [hi; mid] -> groups 1, 2; lo x hi -> group 2
+                    const uint32_t d0 = tmem + (uint32_t)b * kBufCols;
+                    for (int ks = 0; ks < kKT / 16; ++ks) {
+                        const uint64_t db = sdesc(bBase + (uint32_t)(ch * (kKT / 8) + ks * 2) * lboB, lboB, 128);
+                        const uint32_t ka = a0 + ks * 2 * lboA;
+                        mma_bf16_ss(d0, sdesc(ka, lboA, 128), db, idesc_bf16(kTM, 3 * nmpad), (ch | ks) ? 1u : 0u);
+                        mma_bf16_ss(d0 + nmpad, sdesc(ka + (uint32_t)aplane, lboA, 128), db, idesc_bf16(kTM, 2 * nmpad),
+                                    1u);
+                        mma_bf16_ss(d0 + 2 * nmpad, sdesc(ka + 2 * (uint32_t)aplane, lboA, 128), db, idesc, 1u);
                     }
+                } else {
+                    for (int ks = 0; ks < kKT / 16; ++ks)
+                        for (int pr = 0; pr < 6; ++pr) {
+                            const uint64_t da = sdesc(a0 + kProdA[pr] * (uint32_t)aplane + ks * 2 * lboA, lboA, 128);
+                            const uint64_t db = sdesc(bBase + kProdB[pr] * (uint32_t)bplane +
+                                                          (uint32_t)(ch * (kKT / 8) + ks * 2) * lboB, lboB, 128);
+                            // product 5 (hi x hi) alone in columns b*128.., the five smaller ones in b*128 + 64..
+                            const bool lead = pr == 5;
+                            const uint32_t acc = lead ? (uint32_t)(ch | ks) : (uint32_t)(ch | ks | pr);
+                            mma_bf16_ss(tmem + b * kBufCols + (lead ? 0u : 64u), da, db, idesc, acc ? 1u : 0u);
+                        }
+                }
                 mma_commit(&adone[sa]);
                 if (ch == nchunks - 1) mma_commit(&dfull[b]);
             }
@@ -862,7 +892,7 @@ __global__ void __launch_bounds__(kD2tThreads, 1) d2m_tma_kernel(const __grid_co
     }
     tc_before_sync();
     __syncthreads();
-    if (warp == kD2tMma) tmem_free(tmem, 256);
+    if (warp == kD2tMma) tmem_free(tmem, 2 * kBufCols);
 }
 
 size_t d2m_tma_smem(int NIpad, int nmpad) {
@@ -925,6 +955,15 @@ bool moments_tma_enabled() {
         on = (e && *e == '0') ? 0 : 1;
     }
     return on == 1;
+}
+
+// D2M's B planes stacked along N, three MMAs per K step (LB_D2M_STACK=0: six MMAs, one per product).
+bool d2m_stack_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("LB_D2M_STACK");
+        return !(e && *e == '0');
+    }();
+    return on;
 }
 
 // M2D's output written by TMA stores (LB_M2D_TMA_STORE=0: per-thread stores).
@@ -1048,17 +1087,24 @@ int launch_d2m_tma(Handle* h, const float* psi, const double* xin, double alpha,
         return LB_ERR_ARG;
     static PerDevice attr;
     attr.get([&] {
-        cudaFuncSetAttribute(d2m_tma_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        cudaFuncSetAttribute(d2m_tma_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        cudaFuncSetAttribute(d2m_tma_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        cudaFuncSetAttribute(d2m_tma_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+#define LB_D2MATTR(K, S) cudaFuncSetAttribute(d2m_tma_kernel<K, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024)
+        LB_D2MATTR(1, false); LB_D2MATTR(2, false); LB_D2MATTR(3, false); LB_D2MATTR(4, false);
+        LB_D2MATTR(1, true); LB_D2MATTR(2, true); LB_D2MATTR(3, true); LB_D2MATTR(4, true);
+#undef LB_D2MATTR
         return 1;
     });
     const long long ntiles = (h->NENK + kTM - 1) / kTM;
     const long long grid = std::min<long long>(ntiles, (long long)h->sm_count);
-#define LB_D2MTMA(K)                                                                                                \
-    d2m_tma_kernel<K><<<(int)grid, kD2tThreads, smem, h->stream>>>(map, h->d_active, h->d_Yd2m, xin, alpha, beta, out, \
-                                                                h->NENK, h->NI, h->NIpad, h->nm, h->nmpad, ntiles, err)
+    const bool stack = d2m_stack_enabled();
+#define LB_D2MTMA(K)                                                                                                    \
+    if (stack)                                                                                                          \
+        d2m_tma_kernel<K, true><<<(int)grid, kD2tThreads, smem, h->stream>>>(map, h->d_active, h->d_Yd2m, xin, alpha,   \
+                                                                           beta, out, h->NENK, h->NI, h->NIpad, h->nm, \
+                                                                           h->nmpad, ntiles, err);                     \
+    else                                                                                                                \
+        d2m_tma_kernel<K, false><<<(int)grid, kD2tThreads, smem, h->stream>>>(map, h->d_active, h->d_Yd2m, xin, alpha,  \
+                                                                            beta, out, h->NENK, h->NI, h->NIpad, h->nm, \
+                                                                            h->nmpad, ntiles, err)
     switch (h->nmpad / 16) {
         case 1: LB_D2MTMA(1); break;
         case 2: LB_D2MTMA(2); break;
