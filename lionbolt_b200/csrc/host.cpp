@@ -564,6 +564,14 @@ static void form_blocks(Handle* h, std::vector<int>& blk_elem, std::vector<int>&
     }
 }
 
+// Units per group of the block schedule: the sweep's CTA size (512 threads), LB_CLUSTER_GROUP=<n> for
+// another cap, 0 for uncapped groups (Kahn's levels).
+static int cluster_group_cap() {
+    const char* e = std::getenv("LB_CLUSTER_GROUP");
+    if (e && *e) return std::max(0, std::atoi(e));
+    return 512;
+}
+
 // Block schedule of every direction: units on levels.  A unit is a block, or part of one: Kahn's
 // algorithm runs over the units of the direction, and whenever no unit is ready while elements remain
 // (the direction's block graph has a cycle), every element whose upstream neighbours are all done
@@ -597,10 +605,14 @@ static int build_cluster_schedule(Handle* h) {
     std::vector<std::vector<int4>> crec(NI);
     std::vector<std::vector<int>> cstart(NI);
     bool cyclic = false;
+    // Units per group.  A group is one pass of the sweep CTA's threads between two barriers, so a group of
+    // Kahn's levels (all ready units) with more units than threads takes several passes, the last one part
+    // empty; capped groups pack every pass (list scheduling: ready units wait at most until a pass has room).
+    const int cap = cluster_group_cap();
 #pragma omp parallel reduction(|| : cyclic)
     {
         std::vector<int> lev(NE), unit(NE), ublk, pend, epend, dstart(NE + 1), ddst, cur, nxt, members, ord, waiting;
-        std::vector<int> usize, newunit;
+        std::vector<int> usize, newunit, rest;
         std::vector<char> done(NE);
         std::vector<uint16_t> fld(NE);
         std::vector<unsigned long long> key;
@@ -715,6 +727,14 @@ static int build_cluster_schedule(Handle* h) {
             cstart[i].clear();
             int ndone = 0;
             while (ndone < NE) {
+                // at most `cap` units per group (one per thread of the sweep CTA): the ready units past it wait
+                // for the next group, ahead of the units that become ready now
+                rest.clear();
+                if (cap > 0 && (int)cur.size() > cap) {
+                    // the units ready longest go first (the leftovers of the previous group lead `cur`)
+                    rest.assign(cur.begin() + cap, cur.end());
+                    cur.resize(cap);
+                }
                 if (cur.empty()) {
                     // stalled on a cycle of units: the ready elements of every blocked unit form new units
                     newunit.clear();
@@ -780,7 +800,8 @@ static int build_cluster_schedule(Handle* h) {
                 // elements whose units became ready do not wait
                 waiting.erase(std::remove_if(waiting.begin(), waiting.end(), [&](int x) { return pend[unit[x]] == 0; }),
                               waiting.end());
-                cur.swap(nxt);
+                rest.insert(rest.end(), nxt.begin(), nxt.end());
+                cur.swap(rest);
             }
             cstart[i].push_back((int)out.size());
             if (ndone != NE) cyclic = true;   // an element-level cycle: no block schedule

@@ -323,6 +323,28 @@ def test_cluster_schedule_respects_every_dependency():
         assert split > 0                                        # block graphs of unstructured meshes have cycles
 
 
+def test_cluster_groups_are_capped_and_packed(monkeypatch):
+    """Groups of the block schedule hold at most one unit per sweep thread (the cap, here 16 instead of
+    512): a level with more ready units spills into the next group, which the units that became ready
+    meanwhile fill up, so the groups take fewer passes of the CTA than Kahn's levels do, and every
+    dependency still points to an earlier group (checked by _check_cluster_schedule)."""
+    m = M.box_mesh(8, 8, 8, (0, 0, 0), (1, 1, 1))
+    k, w = P.quadrature(4, 8)
+    monkeypatch.setenv("LB_CLUSTER_GROUP", "0")
+    levels, _ = _check_cluster_schedule(m, k, w)
+    monkeypatch.setenv("LB_CLUSTER_GROUP", "16")
+    groups, split = _check_cluster_schedule(m, k, w)
+    assert split == 0
+    passes_levels = passes_groups = 0
+    for i in range(k.shape[0]):
+        nl = np.diff(levels["starts"][i][: levels["nlevels"][i] + 1])
+        ng = np.diff(groups["starts"][i][: groups["nlevels"][i] + 1])
+        assert ng.max() <= 16 and nl.max() > 16
+        passes_levels += int(np.sum((nl + 15) // 16))
+        passes_groups += len(ng)
+    assert passes_groups < passes_levels
+
+
 def test_cluster_queries_need_a_block_schedule():
     hj = HostHandle()
     assert hj.mesh(M.box_mesh(1, 1, 1)) == 0 and hj.quad(*P.quadrature(2, 4)) == 0
