@@ -778,10 +778,13 @@ static int build_cluster_schedule(Handle* h) {
                     key[q] = ((unsigned long long)(uint32_t)tmp[q].y * 0x9E3779B97F4A7C15ull) ^
                              ((unsigned long long)(uint32_t)tmp[q].z << 21) ^ (uint32_t)tmp[q].w;
                 }
-                // units with equal patterns next to each other (a warp then runs one element sequence)
+                // units with equal patterns next to each other (a warp then runs one element sequence), and
+                // among them by block index, so that a warp's blocks lie close together in memory
                 ord.resize(n);
                 for (int q = 0; q < n; ++q) ord[q] = q;
-                std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return key[x] < key[y]; });
+                std::sort(ord.begin(), ord.end(), [&](int x, int y) {
+                    return key[x] != key[y] ? key[x] < key[y] : tmp[x].x != tmp[y].x ? tmp[x].x < tmp[y].x : x < y;
+                });
                 for (int q = 0; q < n; ++q) out.push_back(tmp[ord[q]]);
                 nxt.clear();
                 for (int c : cur)
