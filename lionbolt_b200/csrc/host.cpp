@@ -572,7 +572,8 @@ static int cluster_group_cap() {
     return 512;
 }
 
-// Block schedule of every direction: units on levels.  A unit is a block, or part of one: Kahn's
+// Block schedule of every direction: units in groups (a group's units depend only on units of earlier
+// groups; the sweep runs a group between two CTA barriers).  A unit is a block, or part of one: Kahn's
 // algorithm runs over the units of the direction, and whenever no unit is ready while elements remain
 // (the direction's block graph has a cycle), every element whose upstream neighbours are all done
 // leaves its unit for a new unit with the other such elements of its block.  Those elements are
