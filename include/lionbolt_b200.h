@@ -197,6 +197,12 @@ int lb_reset_timers(lb_handle* h);
 int lb_sweep_stats(lb_handle* h, double* bytes_per_sweep, double* updates_per_sweep, long long* upstream_faces);
 /* Waits for the handle's stream; LB_ERR_TIMEOUT if a contraction queued since the last check timed out. */
 int lb_synchronize(lb_handle* h);
+/* Failure-path check (no counterpart in the reference): launches one thread that waits, with the
+ * contraction kernels' bounded wait cut to `polls` polls, on a pipeline barrier that nothing arrives
+ * at.  The wait gives up and raises the handle's timeout flag; the call returns what the following
+ * synchronisation reports, LB_ERR_TIMEOUT (message in lb_last_error), and clears the flag, so the
+ * handle stays usable. */
+int lb_probe_pipeline_timeout(lb_handle* h, long long polls);
 /* Sweep launch shape picked by the autotuner: cfg[0] schedule (0 levels, 1 dataflow, 2 levels with
  * next-level prefetch, 3 element flags, 4 grouped directions, 5 blocks of 6 elements swept as
  * units, 6 the same with per-type element tables), cfg[1] threads per CTA, cfg[2] directions per CTA

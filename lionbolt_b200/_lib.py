@@ -63,6 +63,7 @@ SIGNATURES = {
     "lb_reset_timers": (ctypes.c_int, [_vp]),
     "lb_sweep_stats": (ctypes.c_int, [_vp, _c_double_p, _c_double_p, _c_ll_p]),
     "lb_synchronize": (ctypes.c_int, [_vp]),
+    "lb_probe_pipeline_timeout": (ctypes.c_int, [_vp, ctypes.c_longlong]),
     "lb_get_sweep_config": (ctypes.c_int, [_vp, _c_int_p]),
     "lb_mesh_types": (ctypes.c_int, [_vp, _c_int_p]),
     "lb_set_right_precond_diag": (ctypes.c_int, [_vp, ctypes.c_int, _c_double_p]),

@@ -1218,4 +1218,11 @@ int lb_synchronize(lb_handle* h) {
     return moments_tc_status(h);
 }
 
+int lb_probe_pipeline_timeout(lb_handle* h, long long polls) {
+    if (!h || polls < 1) return LB_ERR_ARG;
+    if (h->device < 0) return fail(h, LB_ERR_STATE, "host-only handle: no device attached");
+    cudaSetDevice(h->device);
+    return tc_wait_probe(h, polls);
+}
+
 }  // extern "C"

@@ -342,6 +342,9 @@ int launch_m2d_tc(Handle* h, const double* x, const float* sigl, const double* a
 int launch_d2m_tc(Handle* h, const float* psi, const double* xin, double alpha, double beta, double* out);
 // Reads and clears the tensor-core kernels' bounded-wait timeout flag.
 int moments_tc_status(Handle* h);
+// Runs the bounded pipeline wait against a barrier nothing arrives at (polls polls); returns what
+// moments_tc_status reports afterwards.
+int tc_wait_probe(Handle* h, long long polls);
 
 // FP64 BLAS-1 on device vectors of length n
 int k_dots(Handle* h, const double* V, size_t ldv, int nv, const double* w, size_t n, double* out_host);

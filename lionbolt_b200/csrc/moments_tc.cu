@@ -79,8 +79,8 @@ __device__ __forceinline__ bool bar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Bounded wait for the MMA commit of the given phase.  Returns false (and raises *err) on timeout.
-__device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t parity, int* err) {
-    for (long long it = 0; it < kSpinLimit; ++it) {
+__device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t parity, int* err, long long limit = kSpinLimit) {
+    for (long long it = 0; it < limit; ++it) {
         if (bar_try_wait(bar, parity)) return true;
         if ((it & 1023) == 1023 && *(volatile int*)err) return false;
     }
@@ -1149,6 +1149,26 @@ int launch_d2m_tc(Handle* h, const float* psi, const double* xin, double alpha, 
 #undef LB_D2MTC
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? LB_OK : cuda_fail(h, e, "d2m tensor-core kernel");
+}
+
+namespace {
+// One thread waits on a pipeline barrier that nothing arrives at, with the contraction kernels' bounded wait
+// cut to `limit` polls: it gives up, raises the handle's error flag and returns, as a stuck stage would.
+__global__ void tc_wait_probe_kernel(int* err, long long limit) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        bar_init(&bar, 1);
+        bar_wait(&bar, 0u, err, limit);
+    }
+}
+}  // namespace
+
+int tc_wait_probe(Handle* h, long long polls) {
+    if (!h->d_tc_err) return LB_ERR_STATE;
+    tc_wait_probe_kernel<<<1, 32, 0, h->stream>>>(h->d_tc_err, polls);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(h, e, "wait probe launch");
+    return moments_tc_status(h);
 }
 
 // Reads and clears the handle's contraction timeout flag (synchronises the handle's stream): LB_ERR_TIMEOUT

@@ -345,6 +345,12 @@ def test_cluster_groups_are_capped_and_packed(monkeypatch):
     assert passes_groups < passes_levels
 
 
+def test_pipeline_timeout_probe_needs_a_device_and_a_bound():
+    hh = HostHandle()
+    assert hh.lib.lb_probe_pipeline_timeout(hh.h, 0) == _lib.LB_ERR_ARG
+    assert hh.lib.lb_probe_pipeline_timeout(hh.h, 4096) == _lib.LB_ERR_STATE   # host-only handle
+
+
 def test_cluster_queries_need_a_block_schedule():
     hj = HostHandle()
     assert hj.mesh(M.box_mesh(1, 1, 1)) == 0 and hj.quad(*P.quadrature(2, 4)) == 0
